@@ -1,0 +1,359 @@
+"""Benchmark: kNN sources/s, 4M points, k = 32, one B200.
+
+Workload: the bimodal triclinic configuration (4,000,000 seeded synthetic
+points in the sheared cell a=(L,0,0), b=(0.3L,0.95L,0), c=(0.1L,0.2L,0.97L),
+density 0.1 on one half and 0.005 on the other, 1 % of points on bin
+faces, 0.5 % exact duplicates; k = 32; cell_hint = 3.0; no mask).
+
+One step = one full search of that frame (fold, bin, scan, placement, walk,
+replay) with inputs resident in HBM. The L2 (126 MB) is flushed between
+timed steps by writing a 256 MB buffer; each step also writes 1.5 GB of
+output rows.
+
+--impl reference times the reference CPU walk (the C++ restatement of
+src/knearest.rs in oracle/, on every host thread) on a bounded sample of
+sources of the same workload.
+
+Under torchrun each rank runs its own frame on its own GPU (no collective on
+the data path; weak scaling); timings are the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "kNN sources/s, 4M pts k=32, 1 B200: FP32+learned vs plain walk, exact indices"
+MODE_NAMES = {0: "plain_f64", 1: "fast_f32", 2: "learned", 3: "replay"}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--mode", type=int, default=-1, help="walk mode; -1 = best available")
+    p.add_argument("--n", type=int, default=4_000_000)
+    p.add_argument("--k", type=int, default=32)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def workload(n, k, seed):
+    from linkcell_b200 import workloads as W
+    return W.bimodal_triclinic(n=n, seed=seed, k=k)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap,utilization.gpu")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        load = [r for r in self.rows if (num(r[7]) or 0) > 0] or self.rows
+        sm = [num(r[0]) for r in load if num(r[0]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for name, v in zip(names, r[3:7]):
+                if v.strip().lower() in ("active", "1"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": num(self.rows[0][1]), "reasons": sorted(reasons),
+                "samples": len(self.rows), "power_w_max": max(num(r[2]) or 0 for r in self.rows)}
+
+
+def cpu_baseline(w, seconds_target=15.0):
+    """The reference walk restated in oracle/ on all host threads, on a bounded
+    sample of sources; extrapolated to sources/s of the whole frame."""
+    from oracle import oracle as O
+    O.build()
+    n = w["xyz"].shape[0]
+    threads = os.cpu_count() or 1
+    probe = O.time_sample(w["xyz"], w["cell"], w["k"], cell_hint=w["cell_hint"], first=0,
+                          stride=max(1, n // 20000), count=20000, threads=threads)
+    per_src = probe["walk_s"] / max(1, probe["walked"])
+    count = int(max(20000, min(n, seconds_target / max(per_src, 1e-9))))
+    stride = max(1, n // count)
+    r = O.time_sample(w["xyz"], w["cell"], w["k"], cell_hint=w["cell_hint"], first=0,
+                      stride=stride, count=count, threads=threads)
+    est_total = r["prep_s"] + r["walk_s"] * (n / max(1, r["walked"]))
+    return {"value": n / est_total, "unit": "sources/s", "cores": threads, "kind": "port",
+            "sample": (f"fold+bin+lists over all {n} points ({r['prep_s']:.2f} s) plus the walk of "
+                       f"{r['walked']} sources (every {stride}-th, {r['walk_s']:.2f} s), "
+                       f"extrapolated to all sources")}
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    w = workload(args.n, args.k, seed=2)
+    from oracle import oracle as O
+    O.build()
+    n = w["xyz"].shape[0]
+    threads = os.cpu_count() or 1
+    # bounded sample per step so the whole run stays within minutes
+    count = int(os.environ.get("LINKCELL_REF_SAMPLE", "60000"))
+    stride = max(1, n // count)
+    vals = []
+    for step in range(args.warmup + args.steps):
+        r = O.time_sample(w["xyz"], w["cell"], w["k"], cell_hint=w["cell_hint"], first=step % stride,
+                          stride=stride, count=count, threads=threads)
+        if step >= args.warmup:
+            vals.append(n / (r["prep_s"] + r["walk_s"] * (n / max(1, r["walked"]))))
+    v = statistics.median(vals)
+    ms = 1000.0 * n / v
+    out = {"metric": METRIC, "value": v, "unit": "sources/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "bimodal_triclinic_4M_k32", "n": n, "k": args.k,
+                      "cell_hint": 3.0, "l2": "n/a (CPU)"},
+           "impl": "reference",
+           "cpu_baseline": {"value": v, "unit": "sources/s", "cores": threads, "kind": "port",
+                            "sample": f"fold+bin over all {n} points plus the walk of every "
+                                      f"{stride}-th source ({count} sources) per step, "
+                                      "extrapolated to the whole frame"},
+           "e2e": {"value": v, "unit": "sources/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    from linkcell_b200 import _capi
+    from linkcell_b200 import build as B
+    from linkcell_b200 import _cell_struct
+    B.build()
+    L = _capi.load()
+    w = workload(args.n, args.k, seed=2 + rank)
+    n, k = w["xyz"].shape[0], w["k"]
+    cell = _cell_struct(np.asarray(w["cell"], dtype=np.float64))
+    x = torch.as_tensor(w["xyz"], device="cuda")
+    nn = torch.empty((n, k), dtype=torch.int32, device="cuda")
+    d2 = torch.empty((n, k), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    ws = L.lc_gpu_workspace_new()
+    assert ws, _capi.gpu_error()
+    stream = ctypes.c_void_p(L.lc_gpu_queue(ws))
+    tstream = torch.cuda.ExternalStream(stream.value)
+
+    def step():
+        rc = L.lc_gpu_knearest_many(ws, x.data_ptr(), n, 1, ctypes.byref(cell), k, None, 3.0,
+                                    nn.data_ptr(), d2.data_ptr(), 0)
+        assert rc == 0, _capi.gpu_error()
+
+    def time_mode(mode, steps, warmup):
+        assert L.lc_gpu_set_mode(ws, mode) == 0
+        for _ in range(warmup):
+            step()
+            L.lc_gpu_wait(ws)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        walk_ms = []
+        counters = None
+        for s in range(steps):
+            with torch.cuda.stream(tstream):
+                flush.fill_(s & 0xFF)  # L2 flush between timed steps, outside the events
+                ev[s][0].record(tstream)
+            step()
+            with torch.cuda.stream(tstream):
+                ev[s][1].record(tstream)
+            L.lc_gpu_wait(ws)
+            pw = ctypes.c_double()
+            L.lc_gpu_phase_times(ws, None, ctypes.byref(pw), None)
+            walk_ms.append(pw.value)
+        torch.cuda.synchronize()
+        buf = (ctypes.c_longlong * 16)()
+        L.lc_gpu_stats(ws, buf, 16, None)
+        counters = list(buf)
+        total = sum(a.elapsed_time(b) for a, b in ev)
+        if world > 1:
+            t = torch.tensor([total], dtype=torch.float64, device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            total = float(t.item())
+        return total, walk_ms, counters
+
+    best_mode = args.mode if args.mode >= 0 else 2
+    # plain FP64 walk (the 2x denominator), then the headline mode
+    plain_total, plain_walk, plain_cnt = time_mode(0, max(3, args.steps // 2), args.warmup)
+    sampler = ClockSampler(dev)
+    sampler.start()
+    total, walk_ms, cnt = time_mode(best_mode, args.steps, args.warmup)
+    sampler.stop()
+    ms_per_step = total / args.steps
+    value = world * n * args.steps / (total / 1000.0)
+    plain_value = world * n * max(3, args.steps // 2) / (plain_total / 1000.0)
+
+    # roofline of the dominant kernel (the walk): algorithmic bytes per launch
+    peak, peak_kind = measured_peaks()
+    walk_bytes = n * (32 + 12 * k)
+    walk_avg_ms = statistics.mean(walk_ms)
+    achieved = walk_bytes / (walk_avg_ms / 1000.0) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "walk_bimodal_4M_k32_traffic.txt")
+    if os.path.exists(tpath):
+        for line in open(tpath):
+            if line.startswith("traffic_bytes_per_launch:"):
+                traffic = float(line.split(":")[1])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "peak_source": f"{peak_kind} hbm_gbs", "kernel": "walk",
+                "algorithmic_bytes_per_source": 32 + 12 * k}
+
+    # end to end through the host C ABI with pinned buffers
+    e2e = None
+    if not args.no_e2e:
+        hx = torch.as_tensor(w["xyz"]).pin_memory()
+        hnn = torch.empty((n, k), dtype=torch.int32).pin_memory()
+        hd2 = torch.empty((n, k), dtype=torch.float64).pin_memory()
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        # the host ABI walks with the library's default mode; select the headline mode
+        os.environ["LINKCELL_MODE"] = str(best_mode)
+
+        def host_step():
+            rc = L.lc_knearest_d2(ctypes.cast(hx.data_ptr(), dp), n, ctypes.byref(cell), k, None, 3.0,
+                                  ctypes.cast(hnn.data_ptr(), ip), ctypes.cast(hd2.data_ptr(), dp))
+            assert rc == 0, _capi.cpu_error()
+        for _ in range(args.warmup):
+            host_step()
+        times = []
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            host_step()
+            times.append(time.perf_counter() - t0)
+        tot = sum(times)
+        if world > 1:
+            t = torch.tensor([tot], dtype=torch.float64, device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            tot = float(t.item())
+        e2e = {"value": world * n * args.steps / tot, "unit": "sources/s",
+               "h2d_bytes_per_step": n * 24, "d2h_bytes_per_step": n * k * 12,
+               "ms_per_step": 1000.0 * tot / args.steps, "timer": "host wall clock around the call"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(w, args.cpu_seconds)
+
+    names = ["pairs", "inserts", "replays", "shells", "pruned", "reranks", "prop_under",
+             "prop_over", "prop_exact", "revisited"]
+    walk_stats = {nm: cnt[i] // args.steps for i, nm in enumerate(names)}
+    launches_per_step = 6
+    out = {"metric": METRIC, "value": value, "unit": "sources/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic",
+           "config": {"workload": "bimodal_triclinic_4M_k32", "n": n, "k": k, "cell_hint": 3.0,
+                      "mode": MODE_NAMES[best_mode], "parallelism": f"replicas x{world}",
+                      "l2": "flushed between timed steps (256 MB write)"},
+           "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+           "gpu_launches": launches_per_step * args.steps, "clocks": sampler.summary(),
+           "plain_fp64": {"value": plain_value, "unit": "sources/s",
+                          "walk_ms": statistics.mean(plain_walk)},
+           "speedup_vs_plain": value / plain_value, "walk_ms": walk_avg_ms,
+           "walk_stats_per_step": walk_stats}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    L.lc_gpu_workspace_free(ws)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

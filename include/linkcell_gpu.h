@@ -1,0 +1,125 @@
+/*
+ * linkcell device C API, served by the B200 implementation
+ * (liblinkcell_b200.so, sm_100a kernels built ahead of time with nvcc).
+ *
+ * Drop-in for the reference device C ABI (HaoZeke/linkcell v0.3.3,
+ * include/linkcell_gpu.h, src/gpu/capi.cpp): same 13 symbols, same
+ * arguments. xyz, mask, out_nn and out_d2 are CUDA device pointers; the
+ * cell is a host lc_cell (or, for _dcell, device doubles).
+ *
+ * Differences from the reference gpulite path, all toward the reference CPU
+ * walk (src/knearest.rs), whose results this library reproduces exactly:
+ *   - any k >= 1 (the reference device path stops at k <= 16);
+ *   - meshes up to 16,777,216 cells (the reference device path stops at
+ *     262,144);
+ *   - exact duplicates (dist2 == 0) are kept, as on the CPU;
+ *   - a mask has n entries shared by all frames, as on the CPU;
+ *   - cell_hint = +inf selects the default edge 3.0, as on the CPU;
+ *   - tie order follows the CPU heap exactly.
+ *
+ * Distinct workspaces may run concurrently. A workspace enqueues all work
+ * on one CUDA stream (lc_gpu_queue); call lc_gpu_wait before reading
+ * results of a search issued with wait == 0.
+ */
+#ifndef LINKCELL_GPU_H
+#define LINKCELL_GPU_H
+
+#include <stddef.h>
+
+#include "linkcell.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lc_gpu_workspace lc_gpu_workspace;
+
+/* 1 when a CUDA device is usable, else 0 (src/gpu/capi.cpp:21-27). */
+int lc_gpu_available(void);
+/* This thread's last lc_gpu_* error, NULL after success (src/gpu/capi.cpp:29-31). */
+const char *lc_gpu_last_error(void);
+
+/* Workspace: grow-only device buffers and one CUDA stream
+ * (src/gpu/capi.cpp:39-57). */
+lc_gpu_workspace *lc_gpu_workspace_new(void);
+void lc_gpu_workspace_free(lc_gpu_workspace *ws);
+
+/* One frame, waits for completion (src/gpu/capi.cpp:65-70). */
+int lc_gpu_knearest(lc_gpu_workspace *ws, const double *xyz, size_t n,
+                    const struct lc_cell *simbox, size_t k, const int *mask, double cell_hint,
+                    int *out_nn, double *out_d2);
+
+/* n_frames frames sharing one cell; wait == 0 returns after enqueueing
+ * (src/gpu/capi.cpp:72-108). */
+int lc_gpu_knearest_many(lc_gpu_workspace *ws, const double *xyz, size_t n, size_t n_frames,
+                         const struct lc_cell *simbox, size_t k, const int *mask,
+                         double cell_hint, int *out_nn, double *out_d2, int wait);
+
+/* Cell given as device doubles: 3 (ortho lengths), 9 (rows a, b, c) or 12
+ * (rows plus origin) (src/gpu/capi.cpp:110-148). */
+int lc_gpu_knearest_many_dcell(lc_gpu_workspace *ws, const double *xyz, size_t n,
+                               size_t n_frames, const double *cell, int cell_n, size_t k,
+                               const int *mask, double cell_hint, int *out_nn, double *out_d2,
+                               int wait);
+
+/* The workspace's cudaStream_t (src/gpu/capi.cpp:150-157). */
+void *lc_gpu_queue(lc_gpu_workspace *ws);
+/* Stream barrier (src/gpu/capi.cpp:159-167). */
+void lc_gpu_wait(lc_gpu_workspace *ws);
+
+/* Helpers used by language bindings (src/gpu/capi.cpp:169-282). kind is a
+ * cudaMemcpyKind; fill supports the values 0 and -1 only. */
+int lc_gpu_alloc(void **ptr, size_t bytes);
+void lc_gpu_free(void *ptr);
+int lc_gpu_fill_i32(void *ptr, int value, size_t n);
+int lc_gpu_memcpy(void *dst, const void *src, size_t bytes, int kind);
+
+/* ------------------------------------------------------------------
+ * Extensions (no counterpart in the reference). Defaults keep the
+ * reference's exact results; every mode returns identical indices.
+ */
+
+/* Walk selection. */
+#define LC_GPU_MODE_PLAIN_F64 0 /* shell-by-shell FP64 walk */
+#define LC_GPU_MODE_FAST_F32 1  /* FP32 candidates, FP64 rerank of the boundary band */
+#define LC_GPU_MODE_LEARNED 2   /* FP32 walk that opens a learned shell proposal at once */
+#define LC_GPU_MODE_REPLAY 3    /* every source through the literal sequential heap */
+int lc_gpu_set_mode(lc_gpu_workspace *ws, int mode);
+int lc_gpu_get_mode(lc_gpu_workspace *ws);
+
+/* Enqueue on the caller's stream instead of the workspace's own one
+ * (NULL restores the workspace stream). */
+int lc_gpu_set_stream(lc_gpu_workspace *ws, void *stream);
+
+/* Walk counters of the last search issued with wait != 0: pairs evaluated,
+ * heap insertions, exact replays, shells, pruned cells, FP64 reranks,
+ * proposal under / over / exact, revisited shells. device_ms is the device
+ * time of the whole search. Returns the number of counters written. */
+int lc_gpu_stats(lc_gpu_workspace *ws, long long *counters, int n_counters, double *device_ms);
+
+/* Device time of the last search's phases, from CUDA events on the
+ * workspace stream: fold + bin + scan + placement, the walk kernel, and the
+ * exact replay of tied sources. Waits for the search to finish. */
+int lc_gpu_phase_times(lc_gpu_workspace *ws, double *prep_ms, double *walk_ms, double *replay_ms);
+
+/* One frame of a heterogeneous batch: its own point count, cell, k and
+ * hint. Frames are packed back to back in xyz (3 doubles per point) and in
+ * the outputs (frame f starts at sum over g < f of n_g * k_g). mask_offset
+ * is the frame's first entry in mask, or -1 for an unmasked frame. */
+typedef struct lc_frame {
+  size_t n;
+  size_t k;
+  struct lc_cell cell;
+  double cell_hint;
+  long long mask_offset;
+} lc_frame;
+
+int lc_gpu_knearest_batch(lc_gpu_workspace *ws, const double *xyz, const lc_frame *frames,
+                          size_t n_frames, const int *mask, int *out_nn, double *out_d2,
+                          int wait);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LINKCELL_GPU_H */

@@ -1,0 +1,321 @@
+// Fold, bin, histogram, scan and stable cell-sorted placement (sm_100a).
+//
+// These are the HBM-bound stages in front of the walk. They replace the
+// fold/bin and linked-list build of the reference search
+// (src/knearest.rs:399-428). The reference keeps a per-cell linked list
+// that it traverses in descending point index. Here the points are stored
+// cell-major in SoA arrays, ascending by point index inside each cell, so a
+// cell is one contiguous range of the sorted arrays.
+#include <cuda/atomic>
+
+#include "lc_kernels.h"
+
+namespace lc {
+
+namespace {
+
+__device__ __forceinline__ int frame_of_point(const FrameDesc *__restrict__ fr, int nf,
+                                              long long g) {
+  int lo = 0, hi = nf - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (fr[mid].pt_base <= g)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// fold + bin + histogram: one thread per point, grid-stride.
+__global__ void __launch_bounds__(256)
+    k_fold_bin(const double *__restrict__ xyz, const int *__restrict__ mask,
+               const FrameDesc *__restrict__ frames, int nframes, long long npts,
+               uint32_t *__restrict__ cell_of, uint32_t *__restrict__ arank,
+               uint32_t *__restrict__ count, int *__restrict__ frame_flags) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += stride) {
+    const int f = nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
+    const FrameDesc &fr = frames[f];
+    const long long i = g - fr.pt_base;
+    if (fr.has_mask && mask[fr.mask_base + i] == 0) {
+      cell_of[g] = kInactive;
+      continue;
+    }
+    double s0, s1, s2;
+    fractional(fr, xyz[3 * g + 0], xyz[3 * g + 1], xyz[3 * g + 2], s0, s1, s2);
+    if (s0 != s0 || s1 != s1 || s2 != s2) atomicOr(&frame_flags[f], kFrameNaN);
+    const int cx = bin_of(s0, fr.nx);
+    const int cy = bin_of(s1, fr.ny);
+    const int cz = bin_of(s2, fr.nz);
+    const uint32_t c =
+        uint32_t(fr.cell_base + ((long long)cz * fr.ny + cy) * (long long)fr.nx + cx);
+    cell_of[g] = c;
+    arank[g] = atomicAdd(&count[c], 1u);
+  }
+}
+
+// ---------------------------------------------------------------- scan
+// Single-pass exclusive scan with decoupled look-back (Merrill & Garland).
+// Tile ids come from an atomic counter in launch order, so a tile only ever
+// waits on tiles that have already started; every wait is still bounded
+// and reports kStatusScanTimeout instead of hanging.
+constexpr unsigned long long kFlagA = 1ull << 62;  // aggregate published
+constexpr unsigned long long kFlagP = 2ull << 62;  // inclusive prefix published
+constexpr unsigned long long kValMask = (1ull << 62) - 1;
+constexpr int kSpinLimit = 1 << 22;
+
+__device__ __forceinline__ unsigned long long load_acquire(unsigned long long *p) {
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*p);
+  return r.load(cuda::memory_order_acquire);
+}
+__device__ __forceinline__ void store_release(unsigned long long *p, unsigned long long v) {
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*p);
+  r.store(v, cuda::memory_order_release);
+}
+
+__global__ void __launch_bounds__(kScanBlock)
+    k_scan_cells(const uint32_t *__restrict__ count, uint32_t *__restrict__ off, long long ncells,
+                 unsigned long long *__restrict__ tile_state, uint32_t *__restrict__ tile_counter,
+                 int *__restrict__ status) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp[kScanBlock / 32];
+  __shared__ unsigned long long s_excl;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+  __syncthreads();
+  const long long tile = s_tile;
+  const long long base = tile * kScanTile + (long long)tid * kScanItems;
+  uint32_t v[kScanItems];
+  if (base + kScanItems <= ncells) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(count + base);
+    const uint4 a = src[0], b = src[1];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int m = 0; m < kScanItems; ++m) v[m] = (base + m < ncells) ? count[base + m] : 0u;
+  }
+  uint32_t tsum = 0;
+#pragma unroll
+  for (int m = 0; m < kScanItems; ++m) tsum += v[m];
+  // inclusive warp scan of thread sums
+  uint32_t x = tsum;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < kScanBlock / 32 ? s_warp[lane] : 0u;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
+      if (lane >= d) w += y;
+    }
+    if (lane < kScanBlock / 32) s_warp[lane] = w;  // inclusive warp totals
+  }
+  __syncthreads();
+  const uint32_t agg = s_warp[kScanBlock / 32 - 1];
+  const uint32_t texcl = (warp ? s_warp[warp - 1] : 0u) + x - tsum;
+
+  if (warp == 0) {
+    // publish this tile's aggregate, then look back 32 predecessors at a time
+    if (lane == 0) store_release(&tile_state[tile], (tile == 0 ? kFlagP : kFlagA) | agg);
+    unsigned long long excl = 0;
+    if (tile > 0) {
+      long long end = tile;  // predecessors [end-32, end)
+      bool done = false, timeout = false;
+      while (!done && !timeout) {
+        const long long t = end - 1 - lane;
+        unsigned long long w = kFlagP;  // before tile 0: an empty prefix
+        if (t >= 0) {
+          int spins = 0;
+          w = load_acquire(&tile_state[t]);
+          while ((w >> 62) == 0 && spins < kSpinLimit) {
+            ++spins;
+            w = load_acquire(&tile_state[t]);
+          }
+        }
+        const unsigned invalid = __ballot_sync(0xffffffffu, (w >> 62) == 0);
+        if (invalid) {
+          timeout = true;
+          break;
+        }
+        const unsigned pm = __ballot_sync(0xffffffffu, (w >> 62) == 2);
+        const int stop = pm ? (__ffs(pm) - 1) : 31;
+        unsigned long long val = (lane <= stop) ? (w & kValMask) : 0ull;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) val += __shfl_xor_sync(0xffffffffu, val, d);
+        excl += val;
+        if (pm) done = true;
+        end -= 32;
+      }
+      if (timeout && lane == 0) atomicOr(status, kStatusScanTimeout);
+      if (lane == 0) store_release(&tile_state[tile], kFlagP | ((excl + agg) & kValMask));
+    }
+    if (lane == 0) s_excl = excl;
+  }
+  __syncthreads();
+  uint32_t run = uint32_t(s_excl) + texcl;
+  if (base + kScanItems <= ncells) {
+    uint32_t o[kScanItems];
+#pragma unroll
+    for (int m = 0; m < kScanItems; ++m) {
+      o[m] = run;
+      run += v[m];
+    }
+    uint4 *dst = reinterpret_cast<uint4 *>(off + base);
+    dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+    dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+  } else {
+#pragma unroll
+    for (int m = 0; m < kScanItems; ++m) {
+      if (base + m < ncells) off[base + m] = run;
+      run += v[m];
+    }
+  }
+  // the thread that owns the last cell also writes off[ncells]
+  if (base <= ncells - 1 && ncells - 1 < base + kScanItems) off[ncells] = run;
+}
+
+// Arrival slots: tmp[off[c] + arank[g]] = g.
+__global__ void __launch_bounds__(256)
+    k_place_slots(const uint32_t *__restrict__ cell_of, const uint32_t *__restrict__ arank,
+                  const uint32_t *__restrict__ off, uint32_t *__restrict__ tmp, long long npts,
+                  long long ncells, int *__restrict__ status) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long total = off[ncells];
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += stride) {
+    const uint32_t c = cell_of[g];
+    if (c == kInactive) continue;
+    const long long pos = (long long)off[c] + arank[g];
+    if (pos >= total || c >= ncells) {
+      atomicOr(status, kStatusBadIndex);
+      continue;
+    }
+    tmp[pos] = uint32_t(g);
+  }
+}
+
+// Stable placement: a point's slot in its cell is the number of points of
+// the same cell with a smaller id. Writes the sorted SoA records and fills
+// the output rows of masked points with -1 / NaN (src/knearest.rs:293-296).
+__global__ void __launch_bounds__(256)
+    k_place_records(const double *__restrict__ xyz, const FrameDesc *__restrict__ frames,
+                    int nframes, long long npts, long long ncells,
+                    const uint32_t *__restrict__ cell_of, const uint32_t *__restrict__ off,
+                    const uint32_t *__restrict__ tmp, double *__restrict__ sx,
+                    double *__restrict__ sy, double *__restrict__ sz, int *__restrict__ sidx,
+                    uint32_t *__restrict__ scell, float4 *__restrict__ rec,
+                    int *__restrict__ out_nn, double *__restrict__ out_d2,
+                    int *__restrict__ status) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long total = off[ncells];
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += stride) {
+    const int f = nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
+    const FrameDesc &fr = frames[f];
+    const long long i = g - fr.pt_base;
+    const uint32_t c = cell_of[g];
+    if (c == kInactive) {
+      int *row = out_nn + fr.out_base + i * fr.k;
+      for (int s = 0; s < fr.k; ++s) row[s] = -1;
+      if (out_d2) {
+        double *drow = out_d2 + fr.out_base + i * fr.k;
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        for (int s = 0; s < fr.k; ++s) drow[s] = nan;
+      }
+      continue;
+    }
+    if (c >= ncells) {
+      atomicOr(status, kStatusBadIndex);
+      continue;
+    }
+    const uint32_t a = off[c], b = off[c + 1];
+    uint32_t r = 0;
+    for (uint32_t q = a; q < b; ++q) r += tmp[q] < uint32_t(g) ? 1u : 0u;
+    const long long pos = (long long)a + r;
+    if (pos >= total) {
+      atomicOr(status, kStatusBadIndex);
+      continue;
+    }
+    double s0, s1, s2, q0, q1, q2;
+    fractional(fr, xyz[3 * g + 0], xyz[3 * g + 1], xyz[3 * g + 2], s0, s1, s2);
+    cartesian(fr, s0, s1, s2, q0, q1, q2);
+    sx[pos] = q0;
+    sy[pos] = q1;
+    sz[pos] = q2;
+    sidx[pos] = int(i);
+    const uint32_t lc = uint32_t(c - fr.cell_base);
+    scell[pos] = lc;
+    // FP32 offset from the lower cell corner H (c / n) + origin.
+    const int cx = int(lc % uint32_t(fr.nx));
+    const int cy = int((lc / uint32_t(fr.nx)) % uint32_t(fr.ny));
+    const int cz = int(lc / (uint32_t(fr.nx) * uint32_t(fr.ny)));
+    const double f0 = double(cx) / fr.nx, f1 = double(cy) / fr.ny, f2 = double(cz) / fr.nz;
+    const double c0 = fr.h[0] * f0 + fr.h[3] * f1 + fr.h[6] * f2 + fr.origin[0];
+    const double c1 = fr.h[1] * f0 + fr.h[4] * f1 + fr.h[7] * f2 + fr.origin[1];
+    const double c2 = fr.h[2] * f0 + fr.h[5] * f1 + fr.h[8] * f2 + fr.origin[2];
+    rec[pos] = make_float4(float(q0 - c0), float(q1 - c1), float(q2 - c2), __int_as_float(int(i)));
+  }
+}
+
+__global__ void k_count_active(const int *__restrict__ mask, long long n,
+                               unsigned long long *__restrict__ out) {
+  unsigned long long local = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    local += mask[i] != 0;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) local += __shfl_xor_sync(0xffffffffu, local, d);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, local);
+}
+
+int grid_for(long long n, int block) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long want = (n + block - 1) / block;
+  const long long cap = (long long)sms * 16;
+  return int(want < 1 ? 1 : (want < cap ? want : cap));
+}
+
+}  // namespace
+
+long long scan_tiles(long long ncells) { return (ncells + kScanTile - 1) / kScanTile; }
+
+cudaError_t launch_fold_bin(const BatchBuffers &b, cudaStream_t s) {
+  if (b.npts <= 0) return cudaSuccess;
+  k_fold_bin<<<grid_for(b.npts, 256), 256, 0, s>>>(b.xyz, b.mask, b.frames, b.nframes, b.npts,
+                                                     b.cell_of, b.arank, b.count, b.frame_flags);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scan(const BatchBuffers &b, cudaStream_t s) {
+  const long long tiles = scan_tiles(b.ncells);
+  k_scan_cells<<<unsigned(tiles), kScanBlock, 0, s>>>(b.count, b.off, b.ncells, b.tile_state,
+                                                       b.tile_counter, b.status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_place(const BatchBuffers &b, cudaStream_t s) {
+  if (b.npts <= 0) return cudaSuccess;
+  const int g = grid_for(b.npts, 256);
+  k_place_slots<<<g, 256, 0, s>>>(b.cell_of, b.arank, b.off, b.tmp, b.npts, b.ncells, b.status);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_place_records<<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.npts, b.ncells, b.cell_of, b.off,
+                                    b.tmp, b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec, b.out_nn,
+                                    b.out_d2, b.status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_active(const int *mask, long long n, unsigned long long *out,
+                                cudaStream_t s) {
+  k_count_active<<<grid_for(n, 256), 256, 0, s>>>(mask, n, out);
+  return cudaGetLastError();
+}
+
+}  // namespace lc

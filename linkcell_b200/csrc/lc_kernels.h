@@ -1,0 +1,106 @@
+// Launch wrappers of the sm_100a kernels of the linked-cell k-nearest
+// search. Host code (workspace.cu) calls only these; every pointer is a
+// device pointer and every launch goes on the given stream.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lc_types.h"
+
+namespace lc {
+
+// Device buffers of one batch. Sizes: P = points in the batch, C = cells
+// in the batch, F = frames.
+struct BatchBuffers {
+  const double *xyz = nullptr;   // P*3, frame-major, caller's
+  const int *mask = nullptr;     // caller's; frames index it with mask_base
+  const FrameDesc *frames = nullptr;  // F
+  int nframes = 0;
+  long long npts = 0;            // P
+  long long ncells = 0;          // C
+  uint32_t *cell_of = nullptr;   // P: batch cell id or kInactive
+  uint32_t *arank = nullptr;     // P: arrival rank inside the cell (atomics)
+  uint32_t *tmp = nullptr;       // P: point id at its arrival slot
+  uint32_t *count = nullptr;     // C
+  uint32_t *off = nullptr;       // C+1: exclusive scan of count
+  unsigned long long *tile_state = nullptr;  // scan tiles
+  uint32_t *tile_counter = nullptr;
+  int *status = nullptr;         // StatusBits
+  int *frame_flags = nullptr;    // F
+  // cell-sorted (stable: ascending point id inside a cell) source arrays
+  double *sx = nullptr, *sy = nullptr, *sz = nullptr;  // folded FP64 SoA
+  int *sidx = nullptr;           // index of the point inside its frame
+  uint32_t *scell = nullptr;     // cell id inside the frame
+  float4 *rec = nullptr;         // FP32 offset from the cell corner, idx bits in w
+  // outputs (caller's)
+  int *out_nn = nullptr;
+  double *out_d2 = nullptr;
+  // walk bookkeeping
+  uint32_t *work = nullptr;      // work-queue cursor
+  int *replay_list = nullptr;    // sorted positions that need the exact replay
+  uint32_t *replay_count = nullptr;
+  long long replay_cap = 0;
+  double *replay_d = nullptr;    // replay heap scratch: replay_threads * kmax
+  int *replay_i = nullptr;
+  int replay_threads = 0;
+  int kmax = 0;
+  long long *counters = nullptr; // walk statistics (see WalkCounters)
+};
+
+// Walk statistics accumulated on the device (counters[...]).
+enum WalkCounters : int {
+  kCntPairs = 0,      // candidate distances evaluated
+  kCntInserts = 1,    // heap insertions
+  kCntReplays = 2,    // sources sent to the exact replay
+  kCntShells = 3,     // shells walked (sum over sources)
+  kCntPruned = 4,     // stencil cells skipped by the distance bound
+  kCntRerank = 5,     // FP64 recomputations in the FP32 walk
+  kCntPropUnder = 6,  // learned proposal too short
+  kCntPropOver = 7,   // learned proposal too long
+  kCntPropExact = 8,  // learned proposal equal to the settled shell
+  kCntRevisit = 9,    // shells walked again after a short proposal
+  kNumCounters = 16
+};
+
+constexpr int kScanBlock = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+long long scan_tiles(long long ncells);
+
+// fold + bin + cell histogram (one pass over the points).
+cudaError_t launch_fold_bin(const BatchBuffers &b, cudaStream_t s);
+// exclusive scan of the histogram (single-pass decoupled look-back).
+cudaError_t launch_scan(const BatchBuffers &b, cudaStream_t s);
+// stable cell-sorted placement: arrival slots, then in-cell rank by point id.
+cudaError_t launch_place(const BatchBuffers &b, cudaStream_t s);
+
+// Walk modes.
+enum WalkMode : int {
+  kModePlainF64 = 0,   // shell-by-shell FP64 walk
+  kModeFastF32 = 1,    // FP32 candidates + FP64 rerank, shell-by-shell
+  kModeLearned = 2,    // FP32 + learned shell proposal (cube opened at once)
+  kModeReplayAll = 3,  // every source through the exact sequential replay
+};
+
+struct WalkLaunch {
+  int mode = kModePlainF64;
+  int block = 128;
+  int grid = 0;
+  int kmax = 32;
+  int prune = 1;
+  const int8_t *proposal = nullptr;  // per sorted source proposed shell (learned mode)
+};
+
+cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s);
+cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s);
+size_t walk_smem_bytes(int mode, int block, int kmax);
+int walk_max_block(int mode, int kmax);
+cudaError_t walk_prepare(int mode, int kmax, int block);  // sets the dynamic smem attribute
+
+// Counts active points (used to tell an all-masked batch from a bad mesh).
+cudaError_t launch_count_active(const int *mask, long long n, unsigned long long *out,
+                                cudaStream_t s);
+
+}  // namespace lc

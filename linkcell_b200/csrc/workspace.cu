@@ -1,0 +1,426 @@
+// Host planning and launch sequence of one batch.
+//
+// Host code in this file is compiled with -ffp-contract=off: plan_frame
+// reproduces the reference's FP64 cell set-up bit for bit
+// (src/cell.rs:97-124,322-388 and src/knearest.rs:42-48,377-397,430).
+#include "workspace.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+
+namespace lc {
+
+const char *cpu_message(Code c) {
+  switch (c) {
+    case Code::Ok: return "";
+    case Code::NoPoints: return "no points";
+    case Code::ZeroK: return "k must be at least 1";
+    case Code::NullPointer: return "null pointer";
+    case Code::Overflow: return "n * k overflows";
+    case Code::BadCell: return "singular or non-positive cell";
+    case Code::TooFine: return "linked-cell mesh is too fine";
+    case Code::BadCellN: return "device cell must have 3, 9, or 12 doubles";
+    case Code::NoDevice: return "no CUDA device available";
+    case Code::Cuda: return "CUDA error";
+    case Code::DeviceStatus: return "device search failed";
+    case Code::TooLarge: return "batch too large for 32-bit indexing";
+  }
+  return "unknown error";
+}
+
+const char *gpu_message(Code c) {
+  switch (c) {
+    case Code::BadCell: return "bad cell";          // src/gpu/knearest.cpp:731
+    case Code::TooFine: return "too many cells";    // src/gpu/knearest.cpp:756
+    case Code::NoDevice: return "CUDA driver or nvrtc not loaded";
+    default: return cpu_message(c);
+  }
+}
+
+namespace {
+
+// src/cell.rs:343-353
+void cross3(const double u[3], const double v[3], double o[3]) {
+  o[0] = u[1] * v[2] - u[2] * v[1];
+  o[1] = u[2] * v[0] - u[0] * v[2];
+  o[2] = u[0] * v[1] - u[1] * v[0];
+}
+double norm3(const double v[3]) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+
+// Smallest eigenvalue of a symmetric 3x3 matrix (closed form), used only
+// for the conservative cell-pruning bound of the walk.
+double min_eig_sym3(const double m[3][3]) {
+  const double p1 = m[0][1] * m[0][1] + m[0][2] * m[0][2] + m[1][2] * m[1][2];
+  const double q = (m[0][0] + m[1][1] + m[2][2]) / 3.0;
+  if (p1 == 0.0) return std::min(m[0][0], std::min(m[1][1], m[2][2]));
+  const double p2 = (m[0][0] - q) * (m[0][0] - q) + (m[1][1] - q) * (m[1][1] - q) +
+                    (m[2][2] - q) * (m[2][2] - q) + 2.0 * p1;
+  const double p = std::sqrt(p2 / 6.0);
+  double bm[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) bm[i][j] = (m[i][j] - (i == j ? q : 0.0)) / p;
+  const double detb = bm[0][0] * (bm[1][1] * bm[2][2] - bm[1][2] * bm[2][1]) -
+                      bm[0][1] * (bm[1][0] * bm[2][2] - bm[1][2] * bm[2][0]) +
+                      bm[0][2] * (bm[1][0] * bm[2][1] - bm[1][1] * bm[2][0]);
+  double r = detb / 2.0;
+  r = std::max(-1.0, std::min(1.0, r));
+  const double phi = std::acos(r) / 3.0;
+  const double e1 = q + 2.0 * p * std::cos(phi);
+  const double e3 = q + 2.0 * p * std::cos(phi + 2.0943951023931953);
+  const double e2 = 3.0 * q - e1 - e3;
+  return std::min(e1, std::min(e2, e3));
+}
+
+}  // namespace
+
+Code plan_frame(const double *rows, const double *origin, double cell_hint, int k, FrameDesc &fd) {
+  std::memset(&fd, 0, sizeof(fd));
+  const double a[3] = {rows[0], rows[1], rows[2]};
+  const double b[3] = {rows[3], rows[4], rows[5]};
+  const double c[3] = {rows[6], rows[7], rows[8]};
+  // H by columns (src/cell.rs:103)
+  for (int r = 0; r < 3; ++r) {
+    fd.h[0 * 3 + r] = a[r];
+    fd.h[1 * 3 + r] = b[r];
+    fd.h[2 * 3 + r] = c[r];
+  }
+  // invert_columns (src/cell.rs:355-388)
+  const double det = a[0] * (b[1] * c[2] - b[2] * c[1]) - a[1] * (b[0] * c[2] - b[2] * c[0]) +
+                     a[2] * (b[0] * c[1] - b[1] * c[0]);
+  if (!std::isfinite(det) || std::fabs(det) < 1e-18) return Code::BadCell;
+  const double invdet = 1.0 / det;
+  fd.hinv[0] = (b[1] * c[2] - b[2] * c[1]) * invdet;
+  fd.hinv[1] = (a[2] * c[1] - a[1] * c[2]) * invdet;
+  fd.hinv[2] = (a[1] * b[2] - a[2] * b[1]) * invdet;
+  fd.hinv[3] = (b[2] * c[0] - b[0] * c[2]) * invdet;
+  fd.hinv[4] = (a[0] * c[2] - a[2] * c[0]) * invdet;
+  fd.hinv[5] = (a[2] * b[0] - a[0] * b[2]) * invdet;
+  fd.hinv[6] = (b[0] * c[1] - b[1] * c[0]) * invdet;
+  fd.hinv[7] = (a[1] * c[0] - a[0] * c[1]) * invdet;
+  fd.hinv[8] = (a[0] * b[1] - a[1] * b[0]) * invdet;
+  // perpendicular widths (src/cell.rs:108-116)
+  double bc[3], ca[3], ab[3];
+  cross3(b, c, bc);
+  cross3(c, a, ca);
+  cross3(a, b, ab);
+  const double wa = std::fabs(det) / norm3(bc);
+  const double wb = std::fabs(det) / norm3(ca);
+  const double wc = std::fabs(det) / norm3(ab);
+  if (!(wa > 0.0 && wb > 0.0 && wc > 0.0)) return Code::BadCell;
+  fd.widths[0] = wa;
+  fd.widths[1] = wb;
+  fd.widths[2] = wc;
+  fd.origin[0] = origin[0];
+  fd.origin[1] = origin[1];
+  fd.origin[2] = origin[2];
+  // is_axis_aligned (src/cell.rs:322-331)
+  {
+    const double scale = std::fmax(norm3(a) + norm3(b) + norm3(c), 1.0);
+    const double tol = 1e-12 * scale;
+    fd.ortho = std::fabs(a[1]) <= tol && std::fabs(a[2]) <= tol && std::fabs(b[0]) <= tol &&
+               std::fabs(b[2]) <= tol && std::fabs(c[0]) <= tol && std::fabs(c[1]) <= tol;
+  }
+  // edge and bins (src/knearest.rs:42-48,377-397). The C ABI passes
+  // Some(hint) only for hint > 0 (src/capi.rs:235-239).
+  double edge = cell_hint > 0.0 ? cell_hint : 3.0;
+  if (!std::isfinite(edge) || edge <= 0.0) edge = 3.0;
+  edge = std::fmin(std::fmin(std::fmin(edge, wa), wb), wc);
+  int nb[3];
+  const double w[3] = {wa, wb, wc};
+  for (int d = 0; d < 3; ++d) {
+    const double nn = std::fmax(std::floor(w[d] / edge), 1.0);
+    if (!std::isfinite(nn) || nn > 1000000.0) return Code::TooFine;
+    nb[d] = int(nn);
+  }
+  const long long ncell = (long long)nb[0] * nb[1] * nb[2];
+  if (!(ncell > 0 && ncell <= 16777216LL)) return Code::TooFine;
+  fd.nx = nb[0];
+  fd.ny = nb[1];
+  fd.nz = nb[2];
+  fd.cell_min = std::fmin(std::fmin(wa / double(nb[0]), wb / double(nb[1])), wc / double(nb[2]));
+  fd.max_reach = std::max(nb[0], std::max(nb[1], nb[2])) / 2 + 1;
+  fd.k = k;
+  // FP32 cell edge vectors and the bin-unit metric (pruning only)
+  double ev[3][3];
+  for (int ax = 0; ax < 3; ++ax)
+    for (int r = 0; r < 3; ++r) {
+      ev[ax][r] = fd.h[ax * 3 + r] / double(nb[ax]);
+      fd.ev[ax * 3 + r] = float(ev[ax][r]);
+    }
+  double g[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) g[i][j] = ev[i][0] * ev[j][0] + ev[i][1] * ev[j][1] + ev[i][2] * ev[j][2];
+  fd.lam_min = std::max(0.0, min_eig_sym3(g));
+  return Code::Ok;
+}
+
+// ------------------------------------------------------------ workspace
+WorkspaceImpl::WorkspaceImpl() {
+  // Environment overrides: LINKCELL_MODE (walk mode), LINKCELL_BLOCK
+  // (threads per block of the walk), as the reference honours LINKCELL_TPP /
+  // LINKCELL_BLOCK (src/gpu/knearest.cpp:948-960).
+  if (const char *m = std::getenv("LINKCELL_MODE")) {
+    const int v = std::atoi(m);
+    if (v >= 0 && v <= 3) opts.mode = v;
+  }
+  if (const char *b = std::getenv("LINKCELL_BLOCK")) {
+    const int v = std::atoi(b);
+    if (v == 32 || v == 64 || v == 128 || v == 256) opts.block = v;
+  }
+  cudaGetDevice(&device_);
+  cudaStreamCreateWithFlags(&own_, cudaStreamNonBlocking);
+  for (auto &e : ev_) cudaEventCreate(&e);
+}
+
+WorkspaceImpl::~WorkspaceImpl() {
+  if (own_) cudaStreamSynchronize(own_);
+  if (user_set_ && user_) cudaStreamSynchronize(user_);
+  release_all();
+  for (auto &e : ev_)
+    if (e) cudaEventDestroy(e);
+  if (own_) cudaStreamDestroy(own_);
+}
+
+cudaStream_t WorkspaceImpl::stream() { return user_set_ ? user_ : own_; }
+
+void WorkspaceImpl::set_stream(cudaStream_t s) {
+  user_ = s;
+  user_set_ = s != nullptr;
+}
+
+Code WorkspaceImpl::wait(std::string &detail) {
+  const cudaError_t e = cudaStreamSynchronize(stream());
+  if (e != cudaSuccess) {
+    detail = cudaGetErrorString(e);
+    return Code::Cuda;
+  }
+  return Code::Ok;
+}
+
+template <class T>
+cudaError_t WorkspaceImpl::grow(Buf<T> &b, size_t n) {
+  if (n <= b.cap && b.p) return cudaSuccess;
+  size_t want = std::max<size_t>(n, 16);
+  want = want + want / 8;  // headroom against small repeated growth
+  if (b.p) {
+    // the previous batch may still read the old buffer on another stream
+    if (last_stream_ && last_stream_ != stream()) {
+      cudaError_t se = cudaStreamSynchronize(last_stream_);
+      if (se != cudaSuccess) return se;
+    }
+    cudaError_t e = cudaFreeAsync(b.p, stream());
+    if (e != cudaSuccess) return e;
+    b.p = nullptr;
+    b.cap = 0;
+  }
+  void *p = nullptr;
+  cudaError_t e = cudaMallocAsync(&p, want * sizeof(T), stream());
+  if (e != cudaSuccess) return e;
+  b.p = static_cast<T *>(p);
+  b.cap = want;
+  return cudaSuccess;
+}
+
+void WorkspaceImpl::release_all() {
+  auto rel = [&](auto &b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+  };
+  rel(cell_of_); rel(arank_); rel(tmp_); rel(count_); rel(off_); rel(tile_counter_);
+  rel(work_); rel(replay_count_); rel(tile_state_); rel(status_); rel(frame_flags_);
+  rel(sidx_); rel(replay_list_); rel(replay_i_); rel(scell_); rel(sx_); rel(sy_); rel(sz_);
+  rel(replay_d_); rel(rec_); rel(frames_); rel(counters_); rel(h_xyz_); rel(h_d2_);
+  rel(h_mask_); rel(h_nn_); rel(active_);
+}
+
+#define LC_TRY(expr)                        \
+  do {                                      \
+    const cudaError_t e_ = (expr);          \
+    if (e_ != cudaSuccess) {                \
+      detail = cudaGetErrorString(e_);      \
+      return Code::Cuda;                    \
+    }                                       \
+  } while (0)
+
+Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const int *mask,
+                        int *out_nn, double *out_d2, bool wait, std::string &detail) {
+  const int nf = int(frames.size());
+  long long npts = 0, ncells = 0;
+  int kmax = 1;
+  for (auto &fd : frames) {
+    fd.pt_base = npts;
+    fd.cell_base = ncells;
+    npts += fd.n;
+    ncells += (long long)fd.nx * fd.ny * fd.nz;
+    kmax = std::max(kmax, fd.k);
+  }
+  // 32-bit point ids and cell ids (kInactive is reserved)
+  if (npts >= 0xFFFFFFF0LL || ncells >= 0xFFFFFFF0LL) return Code::TooLarge;
+  const cudaStream_t s = stream();
+  const size_t P = size_t(npts), C = size_t(ncells);
+  struct LastStream {
+    cudaStream_t &slot, s;
+    ~LastStream() { slot = s; }
+  } last_guard{last_stream_, s};
+  const long long tiles = scan_tiles(ncells);
+  LC_TRY(grow(cell_of_, P));
+  LC_TRY(grow(arank_, P));
+  LC_TRY(grow(tmp_, P));
+  LC_TRY(grow(count_, C));
+  LC_TRY(grow(off_, C + 1));
+  LC_TRY(grow(tile_state_, size_t(tiles)));
+  LC_TRY(grow(tile_counter_, 1));
+  LC_TRY(grow(work_, 1));
+  LC_TRY(grow(replay_count_, 1));
+  LC_TRY(grow(status_, 1));
+  LC_TRY(grow(frame_flags_, size_t(nf)));
+  LC_TRY(grow(sidx_, P));
+  LC_TRY(grow(scell_, P));
+  LC_TRY(grow(sx_, P));
+  LC_TRY(grow(sy_, P));
+  LC_TRY(grow(sz_, P));
+  LC_TRY(grow(rec_, P));
+  LC_TRY(grow(replay_list_, P));
+  LC_TRY(grow(frames_, size_t(nf)));
+  LC_TRY(grow(counters_, size_t(kNumCounters)));
+
+  WalkLaunch wl;
+  wl.mode = opts.mode;
+  wl.prune = opts.prune;
+  wl.kmax = kmax;
+  // The shared-memory heap walk covers k <= 256; larger k runs the exact
+  // sequential replay for every source.
+  if (kmax > 256) wl.mode = kModeReplayAll;
+  wl.block = opts.block > 0 ? std::min(opts.block, walk_max_block(wl.mode, kmax))
+                            : walk_max_block(wl.mode, kmax);
+
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_);
+  const int replay_threads = int(std::min<long long>(
+      std::max<long long>(1, npts), std::max<long long>(sms * 32, std::min<long long>(
+                                                                     sms * 256,
+                                                                     (256LL << 20) / (kmax * 12)))));
+  LC_TRY(grow(replay_d_, size_t(replay_threads) * kmax));
+  LC_TRY(grow(replay_i_, size_t(replay_threads) * kmax));
+
+  LC_TRY(cudaMemcpyAsync(frames_.p, frames.data(), sizeof(FrameDesc) * nf, cudaMemcpyHostToDevice,
+                         s));
+  LC_TRY(cudaMemsetAsync(count_.p, 0, C * sizeof(uint32_t), s));
+  LC_TRY(cudaMemsetAsync(tile_state_.p, 0, size_t(tiles) * sizeof(unsigned long long), s));
+  LC_TRY(cudaMemsetAsync(tile_counter_.p, 0, sizeof(uint32_t), s));
+  LC_TRY(cudaMemsetAsync(work_.p, 0, sizeof(uint32_t), s));
+  LC_TRY(cudaMemsetAsync(replay_count_.p, 0, sizeof(uint32_t), s));
+  LC_TRY(cudaMemsetAsync(status_.p, 0, sizeof(int), s));
+  LC_TRY(cudaMemsetAsync(frame_flags_.p, 0, sizeof(int) * nf, s));
+  LC_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(long long) * kNumCounters, s));
+
+  BatchBuffers &b = bb_;
+  b = BatchBuffers();
+  b.xyz = xyz;
+  b.mask = mask;
+  b.frames = frames_.p;
+  b.nframes = nf;
+  b.npts = npts;
+  b.ncells = ncells;
+  b.cell_of = cell_of_.p;
+  b.arank = arank_.p;
+  b.tmp = tmp_.p;
+  b.count = count_.p;
+  b.off = off_.p;
+  b.tile_state = tile_state_.p;
+  b.tile_counter = tile_counter_.p;
+  b.status = status_.p;
+  b.frame_flags = frame_flags_.p;
+  b.sx = sx_.p;
+  b.sy = sy_.p;
+  b.sz = sz_.p;
+  b.sidx = sidx_.p;
+  b.scell = scell_.p;
+  b.rec = rec_.p;
+  b.out_nn = out_nn;
+  b.out_d2 = out_d2;
+  b.work = work_.p;
+  b.replay_list = replay_list_.p;
+  b.replay_count = replay_count_.p;
+  b.replay_cap = npts;
+  b.replay_d = replay_d_.p;
+  b.replay_i = replay_i_.p;
+  b.replay_threads = replay_threads;
+  b.kmax = kmax;
+  b.counters = counters_.p;
+
+  if (collect_stats) LC_TRY(cudaEventRecord(ev_[0], s));
+  LC_TRY(launch_fold_bin(b, s));
+  LC_TRY(launch_scan(b, s));
+  LC_TRY(launch_place(b, s));
+  if (collect_stats) LC_TRY(cudaEventRecord(ev_[1], s));
+  LC_TRY(launch_walk(b, wl, s));
+  if (collect_stats) LC_TRY(cudaEventRecord(ev_[2], s));
+  LC_TRY(launch_replay(b, s));
+  if (collect_stats) LC_TRY(cudaEventRecord(ev_[3], s));
+  timed_ = collect_stats;
+  if (!wait) return Code::Ok;
+  LC_TRY(cudaStreamSynchronize(s));
+  int st = 0;
+  LC_TRY(cudaMemcpy(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st != 0) {
+    detail = "device status " + std::to_string(st);
+    return Code::DeviceStatus;
+  }
+  return Code::Ok;
+}
+
+Code WorkspaceImpl::fetch_stats(Stats &out, std::string &detail) {
+  out = Stats();
+  if (!counters_.p) return Code::Ok;
+  if (timed_) {
+    LC_TRY(cudaEventSynchronize(ev_[3]));
+    float a = 0.f, b = 0.f, c = 0.f, t = 0.f;
+    LC_TRY(cudaEventElapsedTime(&a, ev_[0], ev_[1]));
+    LC_TRY(cudaEventElapsedTime(&b, ev_[1], ev_[2]));
+    LC_TRY(cudaEventElapsedTime(&c, ev_[2], ev_[3]));
+    LC_TRY(cudaEventElapsedTime(&t, ev_[0], ev_[3]));
+    out.ms_prep = a;
+    out.ms_walk = b;
+    out.ms_replay = c;
+    out.ms_total = t;
+  } else {
+    LC_TRY(cudaStreamSynchronize(stream()));
+  }
+  LC_TRY(cudaMemcpy(out.counters, counters_.p, sizeof(long long) * kNumCounters,
+                    cudaMemcpyDeviceToHost));
+  return Code::Ok;
+}
+
+Code WorkspaceImpl::run_host(std::vector<FrameDesc> &frames, const double *xyz, size_t xyz_n,
+                             const int *mask, size_t mask_n, int *out_nn, double *out_d2,
+                             size_t out_n, std::string &detail) {
+  const cudaStream_t s = stream();
+  LC_TRY(grow(h_xyz_, xyz_n));
+  LC_TRY(grow(h_nn_, out_n));
+  if (out_d2) LC_TRY(grow(h_d2_, out_n));
+  if (mask) LC_TRY(grow(h_mask_, mask_n));
+  LC_TRY(cudaMemcpyAsync(h_xyz_.p, xyz, xyz_n * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (mask)
+    LC_TRY(cudaMemcpyAsync(h_mask_.p, mask, mask_n * sizeof(int), cudaMemcpyHostToDevice, s));
+  const Code c = run(frames, h_xyz_.p, mask ? h_mask_.p : nullptr, h_nn_.p,
+                     out_d2 ? h_d2_.p : nullptr, false, detail);
+  if (c != Code::Ok) return c;
+  LC_TRY(cudaMemcpyAsync(out_nn, h_nn_.p, out_n * sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (out_d2)
+    LC_TRY(cudaMemcpyAsync(out_d2, h_d2_.p, out_n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  LC_TRY(cudaStreamSynchronize(s));
+  int st = 0;
+  LC_TRY(cudaMemcpy(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st != 0) {
+    detail = "device status " + std::to_string(st);
+    return Code::DeviceStatus;
+  }
+  return Code::Ok;
+}
+
+}  // namespace lc

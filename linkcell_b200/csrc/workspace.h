@@ -1,0 +1,122 @@
+// Host-side planning and the device workspace of the linked-cell k-nearest
+// search. The C ABI (capi.cpp) and the C++ class linkcell::gpu::Workspace
+// are thin layers over WorkspaceImpl.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "lc_kernels.h"
+#include "lc_types.h"
+
+namespace lc {
+
+// Why a call failed. Each public API family maps these to its own strings.
+enum class Code {
+  Ok = 0,
+  NoPoints,      // n == 0 or n_frames == 0
+  ZeroK,         // k == 0
+  NullPointer,
+  Overflow,      // n * k does not fit
+  BadCell,       // singular or non-positive cell
+  TooFine,       // linked-cell mesh exceeds the bin caps
+  BadCellN,      // device cell is not 3, 9 or 12 doubles
+  NoDevice,      // no CUDA device
+  Cuda,          // a CUDA runtime call failed (message in detail)
+  DeviceStatus,  // a kernel reported a status bit
+  TooLarge,      // batch exceeds the 32-bit point / cell indexing
+};
+
+// The reference's messages for the CPU C ABI (src/error.rs:24-36,
+// src/capi.rs:201-203).
+const char *cpu_message(Code c);
+// The reference's messages for the device C ABI (src/gpu/knearest.cpp,
+// src/gpu/capi.cpp).
+const char *gpu_message(Code c);
+
+// Cell::from_vectors + the mesh of search() (src/cell.rs:97-124,
+// src/knearest.rs:377-397,430) into a FrameDesc. rows = a, b, c (9 doubles)
+// and origin (3 doubles). hint <= 0 or NaN selects the default edge 3.0.
+Code plan_frame(const double *rows, const double *origin, double cell_hint, int k, FrameDesc &fd);
+
+// Options that pick the walk.
+struct WalkOptions {
+  int mode = kModePlainF64;
+  int block = 0;   // 0: autotune / default
+  int prune = 1;
+};
+
+struct Stats {
+  long long counters[kNumCounters] = {};
+  double ms_total = 0.0;   // fold .. replay, device time
+  double ms_prep = 0.0;    // fold + bin + scan + placement
+  double ms_walk = 0.0;    // the walk kernel(s)
+  double ms_replay = 0.0;  // exact replay of tied sources
+};
+
+class WorkspaceImpl {
+ public:
+  WorkspaceImpl();
+  ~WorkspaceImpl();
+  WorkspaceImpl(const WorkspaceImpl &) = delete;
+  WorkspaceImpl &operator=(const WorkspaceImpl &) = delete;
+
+  cudaStream_t stream();
+  void set_stream(cudaStream_t s);  // nullptr: back to the workspace's own stream
+  Code wait(std::string &detail);
+
+  // Runs one batch. frames[f] carries the plan (plan_frame) plus pt_base,
+  // cell_base (filled here), out_base and mask_base. xyz, mask, outputs are
+  // device pointers.
+  Code run(std::vector<FrameDesc> &frames, const double *xyz, const int *mask, int *out_nn,
+           double *out_d2, bool wait, std::string &detail);
+
+  WalkOptions opts;
+  bool collect_stats = true;
+  // Counters and phase times of the last run (waits for it to finish).
+  Code fetch_stats(Stats &out, std::string &detail);
+
+  // Host-pointer convenience used by the CPU-compatible C ABI: copies in,
+  // runs, copies out, waits.
+  Code run_host(std::vector<FrameDesc> &frames, const double *xyz, size_t xyz_n, const int *mask,
+                size_t mask_n, int *out_nn, double *out_d2, size_t out_n, std::string &detail);
+
+  // Device-side view of the last batch (diagnostics and tests).
+  const BatchBuffers &buffers() const { return bb_; }
+
+ private:
+  template <class T>
+  struct Buf {
+    T *p = nullptr;
+    size_t cap = 0;
+  };
+  template <class T>
+  cudaError_t grow(Buf<T> &b, size_t n);
+  void release_all();
+
+  int device_ = -1;
+  cudaStream_t own_ = nullptr;
+  cudaStream_t user_ = nullptr;
+  bool user_set_ = false;
+  cudaStream_t last_stream_ = nullptr;  // stream of the last batch
+
+  Buf<uint32_t> cell_of_, arank_, tmp_, count_, off_, tile_counter_, work_, replay_count_;
+  Buf<unsigned long long> tile_state_;
+  Buf<int> status_, frame_flags_, sidx_, replay_list_, replay_i_;
+  Buf<uint32_t> scell_;
+  Buf<double> sx_, sy_, sz_, replay_d_;
+  Buf<float4> rec_;
+  Buf<FrameDesc> frames_;
+  Buf<long long> counters_;
+  // host-pointer staging
+  Buf<double> h_xyz_, h_d2_;
+  Buf<int> h_mask_, h_nn_;
+  Buf<unsigned long long> active_;
+  BatchBuffers bb_;
+  cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool timed_ = false;
+};
+
+}  // namespace lc
