@@ -235,7 +235,7 @@ def run_ours(args):
             torch.distributed.barrier()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(steps)]
-        walk_ms = []
+        walk_ms, prep_ms, replay_ms = [], [], []
         counters = None
         for s in range(steps):
             with torch.cuda.stream(tstream):
@@ -245,9 +245,11 @@ def run_ours(args):
             with torch.cuda.stream(tstream):
                 ev[s][1].record(tstream)
             L.lc_gpu_wait(ws)
-            pw = ctypes.c_double()
-            L.lc_gpu_phase_times(ws, None, ctypes.byref(pw), None)
+            pp, pw, pr = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+            L.lc_gpu_phase_times(ws, ctypes.byref(pp), ctypes.byref(pw), ctypes.byref(pr))
             walk_ms.append(pw.value)
+            prep_ms.append(pp.value)
+            replay_ms.append(pr.value)
         torch.cuda.synchronize()
         buf = (ctypes.c_longlong * 16)()
         L.lc_gpu_stats(ws, buf, 16, None)
@@ -257,14 +259,14 @@ def run_ours(args):
             t = torch.tensor([total], dtype=torch.float64, device="cuda")
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             total = float(t.item())
-        return total, walk_ms, counters
+        return total, walk_ms, counters, prep_ms, replay_ms
 
     best_mode = args.mode if args.mode >= 0 else 2
     # plain FP64 walk (the 2x denominator), then the headline mode
-    plain_total, plain_walk, plain_cnt = time_mode(0, max(3, args.steps // 2), args.warmup)
+    plain_total, plain_walk, plain_cnt, _, _ = time_mode(0, max(3, args.steps // 2), args.warmup)
     sampler = ClockSampler(dev)
     sampler.start()
-    total, walk_ms, cnt = time_mode(best_mode, args.steps, args.warmup)
+    total, walk_ms, cnt, prep_ms, replay_ms = time_mode(best_mode, args.steps, args.warmup)
     sampler.stop()
     ms_per_step = total / args.steps
     value = world * n * args.steps / (total / 1000.0)
@@ -325,7 +327,7 @@ def run_ours(args):
 
     names = ["pairs", "inserts", "replays", "shells", "pruned", "reranks", "prop_under",
              "prop_over", "prop_exact", "revisited"]
-    walk_stats = {nm: cnt[i] // args.steps for i, nm in enumerate(names)}
+    walk_stats = {nm: cnt[i] for i, nm in enumerate(names)}  # counters of the last step
     launches_per_step = 6
     out = {"metric": METRIC, "value": value, "unit": "sources/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -339,7 +341,9 @@ def run_ours(args):
            "plain_fp64": {"value": plain_value, "unit": "sources/s",
                           "walk_ms": statistics.mean(plain_walk)},
            "speedup_vs_plain": value / plain_value, "walk_ms": walk_avg_ms,
-           "walk_stats_per_step": walk_stats}
+           "prep_ms": statistics.mean(prep_ms), "replay_ms": statistics.mean(replay_ms),
+           "walk_stats_last_step": walk_stats,
+           "plain_walk_stats_last_step": {nm: plain_cnt[i] for i, nm in enumerate(names)}}
     if rank == 0:
         print(json.dumps(out), flush=True)
     L.lc_gpu_workspace_free(ws)

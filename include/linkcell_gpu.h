@@ -87,6 +87,11 @@ int lc_gpu_memcpy(void *dst, const void *src, size_t bytes, int kind);
 int lc_gpu_set_mode(lc_gpu_workspace *ws, int mode);
 int lc_gpu_get_mode(lc_gpu_workspace *ws);
 
+/* Learned walk: propose this shell for every source instead of the
+ * network's proposal (0 restores the network). Results stay exact for any
+ * proposal; only the work changes. */
+int lc_gpu_set_proposal(lc_gpu_workspace *ws, int shell);
+
 /* Enqueue on the caller's stream instead of the workspace's own one
  * (NULL restores the workspace stream). */
 int lc_gpu_set_stream(lc_gpu_workspace *ws, void *stream);

@@ -287,9 +287,10 @@ def _knearest_cuda(L, xyz, cell, k, mask, hint, dev, workspace, sync):
             cs = _cell_struct(_host_array(cell, np.float64))
             rc = L.lc_gpu_knearest_many(ws.handle, x.data_ptr(), n, frames, ctypes.byref(cs), k,
                                         mptr, hint, nn.data_ptr(), d2.data_ptr(), 1 if sync else 0)
+        msg = _capi.gpu_error() if rc != 0 else None
         ws.use_stream(None)
     if rc != 0:
-        _raise_from_lib(_capi.gpu_error())
+        _raise_from_lib(msg)
     return nn, d2
 
 
@@ -328,7 +329,8 @@ def knearest_batch(xyz, frames, mask=None, *, workspace: Workspace | None = None
             mptr = mask.data_ptr()
         rc = L.lc_gpu_knearest_batch(ws.handle, x.data_ptr(), arr, len(frames), mptr,
                                      nn.data_ptr(), d2.data_ptr(), 1 if sync else 0)
+        msg = _capi.gpu_error() if rc != 0 else None
         ws.use_stream(None)
     if rc != 0:
-        _raise_from_lib(_capi.gpu_error())
+        _raise_from_lib(msg)
     return nn, d2

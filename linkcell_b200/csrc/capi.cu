@@ -458,20 +458,27 @@ int lc_gpu_fill_i32(void *ptr, int value, size_t n) {
   return 0;
 }
 
+// The extension setters below leave the error slot alone on success, so a
+// caller can still read the message of the search that failed before them.
 int lc_gpu_set_mode(lc_gpu_workspace *ws, int mode) {
   if (!ws) return gpu_fail(Code::NullPointer);
   if (mode < 0 || mode > 3) return gpu_fail_msg("unknown walk mode");
   ws->ws.opts.mode = mode;
-  gpu_ok();
   return 0;
 }
 
 int lc_gpu_get_mode(lc_gpu_workspace *ws) { return ws ? ws->ws.opts.mode : -1; }
 
+int lc_gpu_set_proposal(lc_gpu_workspace *ws, int shell) {
+  if (!ws) return gpu_fail(Code::NullPointer);
+  if (shell < 0 || shell > 127) return gpu_fail_msg("proposal shell must be 0..127");
+  ws->ws.opts.fixed_proposal = shell;
+  return 0;
+}
+
 int lc_gpu_set_stream(lc_gpu_workspace *ws, void *stream) {
   if (!ws) return gpu_fail(Code::NullPointer);
   ws->ws.set_stream(static_cast<cudaStream_t>(stream));
-  gpu_ok();
   return 0;
 }
 

@@ -16,10 +16,23 @@
 // therefore {j : m_j < v} plus the indices with m_j == v (v = k-th value),
 // sorted by (d2, index) -- unless more indices tie at v than slots remain,
 // in which case which of them survive depends on the exact push history.
-// The walk below detects that case (a rejected or evicted value equal to
-// the final k-th value) and sends the source to k_replay, which re-runs the
-// reference push sequence literally: shells ascending, offsets in
-// lexicographic order, occupants in descending point index.
+// The walk detects that case (a rejected or evicted value equal to the
+// final k-th value) and re-runs the reference push sequence literally for
+// that source: shells ascending, offsets in lexicographic order, occupants
+// in descending point index.
+//
+// Three walks share this skeleton:
+//  - plain FP64: every candidate distance in exact FP64;
+//  - FP32: candidate distances from FP32 cell-local offsets; a candidate is
+//    dropped without FP64 work only when d32 > theta (1 + alpha) + beta,
+//    which proves the exact distance exceeds the heap's worst value theta,
+//    so the reference would reject it too; whole cells are skipped by an
+//    FP32 lower bound under the same test; everything else is recomputed
+//    in exact FP64 and pushed into the same exact heap;
+//  - learned: the FP32 walk whose filter starts at the proposed shell's
+//    stop bound (R_p cell_min)^2 instead of +inf. For every reach up to R_p
+//    the stop decision is unchanged by that filter; a source whose walk
+//    passes R_p without stopping restarts without it.
 #include <cuda/atomic>
 
 #include "lc_kernels.h"
@@ -29,6 +42,7 @@ namespace lc {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr float kU32 = 5.9604645e-08f;  // 2^-24, FP32 unit roundoff
 
 __device__ __forceinline__ int frame_of_sorted(const BatchBuffers &b, long long p) {
   int lo = 0, hi = b.nframes - 1;
@@ -81,7 +95,7 @@ __device__ __forceinline__ bool key_gt(double d1, int i1, double d2, int i2) {
   return d1 > d2 || (d1 == d2 && i1 > i2);
 }
 
-// Max-heap of (d, idx) in shared memory, one slot every S words.
+// Max-heap of (d, idx), one slot every S words.
 __device__ __forceinline__ void heap_sift_down(double *hd, int *hi, int S, int pos, int n) {
   const double d = hd[pos * S];
   const int id = hi[pos * S];
@@ -126,6 +140,7 @@ __device__ __forceinline__ void heap_sort(double *hd, int *hi, int S, int n) {
 }
 
 __device__ __forceinline__ double qnan() { return __longlong_as_double(0x7ff8000000000000ll); }
+__device__ __forceinline__ double pinf() { return __longlong_as_double(0x7ff0000000000000ll); }
 
 __device__ __forceinline__ void write_row(const BatchBuffers &b, const FrameDesc &fr, int i,
                                           const double *hd, const int *hi, int S, int n) {
@@ -139,131 +154,29 @@ __device__ __forceinline__ void write_row(const BatchBuffers &b, const FrameDesc
 }
 
 struct LocalCounters {
-  long long pairs = 0, inserts = 0, shells = 0, replays = 0, pruned = 0;
+  long long v[kNumCounters] = {};
 };
 
 __device__ __forceinline__ void flush_counters(const BatchBuffers &b, LocalCounters &c) {
-  long long v[5] = {c.pairs, c.inserts, c.shells, c.replays, c.pruned};
-  const int slot[5] = {kCntPairs, kCntInserts, kCntShells, kCntReplays, kCntPruned};
 #pragma unroll
-  for (int t = 0; t < 5; ++t) {
-    long long x = v[t];
+  for (int t = 0; t < 10; ++t) {
+    long long x = c.v[t];
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(kFull, x, d);
-    if ((threadIdx.x & 31) == 0 && x) atomicAdd((unsigned long long *)&b.counters[slot[t]],
-                                                 (unsigned long long)x);
+    if ((threadIdx.x & 31) == 0 && x)
+      atomicAdd((unsigned long long *)&b.counters[t], (unsigned long long)x);
   }
 }
 
 // ------------------------------------------------------------------------
-// Plain FP64 walk: one thread per source, shells in order, exact stop rule.
-__device__ void walk_source_f64(const BatchBuffers &b, long long p, double *hd, int *hi, int S,
-                                LocalCounters &cnt) {
-  const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
-  const FrameDesc &fr = b.frames[f];
-  if (b.frame_flags[f] & kFrameNaN) {
-    push_replay(b, p);
-    ++cnt.replays;
-    return;
-  }
-  const int k = fr.k;
-  const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
-  const uint32_t lc = b.scell[p];
-  const int ix = int(lc % uint32_t(nx));
-  const int iy = int((lc / uint32_t(nx)) % uint32_t(ny));
-  const int iz = int(lc / (uint32_t(nx) * uint32_t(ny)));
-  const double px = b.sx[p], py = b.sy[p], pz = b.sz[p];
-  const long long cb = fr.cell_base;
-  const uint32_t *__restrict__ off = b.off;
-  int n = 0;
-  double rej = __longlong_as_double(0x7ff0000000000000ll);  // +inf
-  const int max_reach = fr.max_reach;
-  for (int R = 1; R <= max_reach; ++R) {
-    const bool dedupe = 2 * R + 1 > nx || 2 * R + 1 > ny || 2 * R + 1 > nz;
-    ++cnt.shells;
-    for_each_shell_offset(R, [&](int dx, int dy, int dz) {
-      int cx, cy, cz, wa, wb, wc;
-      wrap_axis(ix + dx, nx, cx, wa);
-      wrap_axis(iy + dy, ny, cy, wb);
-      wrap_axis(iz + dz, nz, cz, wc);
-      const long long c = cb + ((long long)cz * ny + cy) * (long long)nx + cx;
-      const uint32_t a0 = off[c], a1 = off[c + 1];
-      if (a0 == a1) return;
-      double shx, shy, shz;
-      lattice_shift(fr, wa, wb, wc, shx, shy, shz);
-      for (uint32_t t = a0; t < a1; ++t) {
-        if ((long long)t == p) continue;
-        const double d = dist2_shifted(px, py, pz, b.sx[t], b.sy[t], b.sz[t], shx, shy, shz);
-        ++cnt.pairs;
-        if (dedupe) {
-          const int j = b.sidx[t];
-          int s = 0;
-          for (; s < n; ++s)
-            if (hi[s * S] == j) break;
-          if (s < n) {
-            if (d < hd[s * S]) {
-              hd[s * S] = d;
-              if (n >= k) heap_sift_down(hd, hi, S, s, n);
-            }
-            continue;
-          }
-        }
-        if (n < k) {
-          hd[n * S] = d;
-          hi[n * S] = b.sidx[t];
-          ++n;
-          ++cnt.inserts;
-          if (n == k) heap_build(hd, hi, S, n);
-        } else if (d < hd[0]) {
-          rej = fmin(rej, hd[0]);
-          hd[0] = d;
-          hi[0] = b.sidx[t];
-          heap_sift_down(hd, hi, S, 0, n);
-          ++cnt.inserts;
-        } else {
-          rej = fmin(rej, d);
-        }
-      }
-    });
-    if (n >= k && hd[0] <= stop_bound(R, fr.cell_min)) break;
-  }
-  if (n >= k && !(rej > hd[0])) {
-    // a value equal to the k-th was left out: the kept subset of the tie
-    // depends on the reference push order
-    push_replay(b, p);
-    ++cnt.replays;
-    return;
-  }
-  if (n < k) heap_build(hd, hi, S, n);
-  heap_sort(hd, hi, S, n);
-  write_row(b, fr, b.sidx[p], hd, hi, S, n);
-}
-
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_walk_f64(BatchBuffers b) {
-  extern __shared__ double smem[];
-  double *hd = smem + threadIdx.x;
-  int *hi = reinterpret_cast<int *>(smem + (size_t)b.kmax * BLOCK) + threadIdx.x;
-  const long long total = b.off[b.ncells];
-  const int lane = threadIdx.x & 31;
-  LocalCounters cnt;
-  for (;;) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(b.work, 32u);
-    base = __shfl_sync(kFull, base, 0);
-    if ((long long)base >= total) break;
-    const long long p = (long long)base + lane;
-    if (p < total) walk_source_f64(b, p, hd, hi, BLOCK, cnt);
-    __syncwarp();
-  }
-  flush_counters(b, cnt);
-}
-
-// ------------------------------------------------------------------------
-// Exact replay of the reference push sequence for one source.
-__device__ void replay_source(const BatchBuffers &b, long long p, double *hd, int *hi) {
-  const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
-  const FrameDesc &fr = b.frames[f];
+// Literal replay of the reference walk for one source (KHeap::push,
+// src/knearest.rs:106-129, in the reference visit order). The pushes that
+// the reference turns into no-ops are skipped: a push of an index not in a
+// full heap with d >= the heap's first maximum, and the index scan outside
+// the wrapping regime, where no index is visited twice. Leaves the row
+// sorted by (total_cmp, index) in hd / hi (stride S) and returns its length.
+__device__ int replay_walk(const BatchBuffers &b, const FrameDesc &fr, long long p, double *hd,
+                           int *hi, int S) {
   const int k = fr.k;
   const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
   const uint32_t lc = b.scell[p];
@@ -273,7 +186,17 @@ __device__ void replay_source(const BatchBuffers &b, long long p, double *hd, in
   const double px = b.sx[p], py = b.sy[p], pz = b.sz[p];
   const long long cb = fr.cell_base;
   int n = 0;
+  int widx = 0;       // first slot holding the maximum (valid when n == k)
+  double wmax = 0.0;  // hd[widx]
+  auto rescan = [&]() {
+    int w = 0;
+    for (int u = 1; u < n; ++u)
+      if (hd[u * S] > hd[w * S]) w = u;
+    widx = w;
+    wmax = hd[w * S];
+  };
   for (int R = 1; R <= fr.max_reach; ++R) {
+    const bool dedupe = 2 * R + 1 > nx || 2 * R + 1 > ny || 2 * R + 1 > nz;
     for_each_shell_offset(R, [&](int dx, int dy, int dz) {
       int cx, cy, cz, wa, wb, wc;
       wrap_axis(ix + dx, nx, cx, wa);
@@ -289,58 +212,279 @@ __device__ void replay_source(const BatchBuffers &b, long long p, double *hd, in
         if ((long long)t == p) continue;
         const double d = dist2_shifted(px, py, pz, b.sx[t], b.sy[t], b.sz[t], shx, shy, shz);
         const int j = b.sidx[t];
-        // KHeap::push, src/knearest.rs:106-129
-        int s = 0;
-        for (; s < n; ++s)
-          if (hi[s] == j) break;
-        if (s < n) {
-          if (d < hd[s]) hd[s] = d;
-          continue;
+        if (dedupe) {
+          int s = 0;
+          for (; s < n; ++s)
+            if (hi[s * S] == j) break;
+          if (s < n) {
+            if (d < hd[s * S]) {
+              hd[s * S] = d;
+              if (n == k) rescan();
+            }
+            continue;
+          }
         }
         if (n < k) {
-          hd[n] = d;
-          hi[n] = j;
+          hd[n * S] = d;
+          hi[n * S] = j;
           ++n;
+          if (n == k) rescan();
           continue;
         }
-        int w = 0;
-        for (int u = 1; u < n; ++u)
-          if (hd[u] > hd[w]) w = u;
-        if (d < hd[w]) {
-          hd[w] = d;
-          hi[w] = j;
+        if (d < wmax) {
+          hd[widx * S] = d;
+          hi[widx * S] = j;
+          rescan();
         }
       }
     });
-    if (n >= k) {
-      double worst = hd[0];
-      for (int u = 1; u < n; ++u)
-        if (hd[u] > worst) worst = hd[u];
-      if (worst <= stop_bound(R, fr.cell_min)) break;
-    }
+    if (n >= k && wmax <= stop_bound(R, fr.cell_min)) break;
   }
   // KHeap::finish: sort by (total_cmp, idx), src/knearest.rs:146-158
   for (int a = 1; a < n; ++a) {
-    const double kd = hd[a];
-    const int ki = hi[a];
+    const double kd = hd[a * S];
+    const int ki = hi[a * S];
     const long long kk = total_key(kd);
     int q = a;
     while (q > 0) {
-      const long long pk = total_key(hd[q - 1]);
-      if (pk > kk || (pk == kk && hi[q - 1] > ki)) {
-        hd[q] = hd[q - 1];
-        hi[q] = hi[q - 1];
+      const long long pk = total_key(hd[(q - 1) * S]);
+      if (pk > kk || (pk == kk && hi[(q - 1) * S] > ki)) {
+        hd[q * S] = hd[(q - 1) * S];
+        hi[q * S] = hi[(q - 1) * S];
         --q;
       } else {
         break;
       }
     }
-    hd[q] = kd;
-    hi[q] = ki;
+    hd[q * S] = kd;
+    hi[q * S] = ki;
   }
-  write_row(b, fr, b.sidx[p], hd, hi, 1, n);
+  return n;
 }
 
+// FP32 filter threshold: a candidate with d32 > thr(theta) has exact
+// distance > theta. With e = per-component error bound of the FP32 offset
+// (rounding of the cell-local offsets, of the edge-vector sum and of the
+// two additions, plus the reference's own FP64 rounding eps64), the
+// distance error is at most 6u d + 3 e^2 (1/u + 1) (the cross terms
+// 2|D|e bounded by u D^2 + e^2 / u). alpha and beta carry margin.
+__device__ __forceinline__ float fp32_threshold(double theta, double beta) {
+  if (!(theta < pinf())) return __int_as_float(0x7f800000);
+  return __double2float_ru(theta * (1.0 + 8.0 * double(kU32)) + beta);
+}
+
+__device__ __forceinline__ double fp32_beta(const FrameDesc &fr, int R) {
+  const double e = double(kU32) * (6.0 * R + 8.0) * double(fr.ell) + fr.eps64 * (R + 2.0);
+  return 4.0 * e * e / double(kU32) + 4.0 * e * e;
+}
+
+// ------------------------------------------------------------------------
+// The walk of one source. MODE: kModePlainF64, kModeFastF32, kModeLearned.
+template <int MODE>
+__device__ void walk_source(const BatchBuffers &b, long long p, double *hd, int *hi, int S,
+                            LocalCounters &cnt) {
+  const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
+  const FrameDesc &fr = b.frames[f];
+  if (b.frame_flags[f] & kFrameNaN) {
+    push_replay(b, p);
+    ++cnt.v[kCntReplays];
+    return;
+  }
+  const int k = fr.k;
+  const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
+  const uint32_t lc = b.scell[p];
+  const int ix = int(lc % uint32_t(nx));
+  const int iy = int((lc / uint32_t(nx)) % uint32_t(ny));
+  const int iz = int(lc / (uint32_t(nx) * uint32_t(ny)));
+  const double px = b.sx[p], py = b.sy[p], pz = b.sz[p];
+  const long long cb = fr.cell_base;
+  const uint32_t *__restrict__ off = b.off;
+  const int max_reach = fr.max_reach;
+  const double cell_min = fr.cell_min;
+
+  // FP32 view: the source's offset from its cell corner and its position
+  // inside the cell in bin units (for the cell lower bound).
+  float plx = 0.f, ply = 0.f, plz = 0.f, fa = 0.f, fb = 0.f, fc = 0.f;
+  float ev[9];
+  float lam = 0.f;
+  if (MODE != kModePlainF64) {
+    const float4 r = b.rec[p];
+    plx = r.x;
+    ply = r.y;
+    plz = r.z;
+#pragma unroll
+    for (int t = 0; t < 9; ++t) ev[t] = fr.ev[t];
+    fa = fr.nhinv[0] * plx + fr.nhinv[1] * ply + fr.nhinv[2] * plz;
+    fb = fr.nhinv[3] * plx + fr.nhinv[4] * ply + fr.nhinv[5] * plz;
+    fc = fr.nhinv[6] * plx + fr.nhinv[7] * ply + fr.nhinv[8] * plz;
+    lam = float(fr.lam_min) * 0.99f;
+  }
+  int Rp = 0;
+  if (MODE == kModeLearned && b.proposal) {
+    Rp = b.proposal[p];
+    if (Rp > max_reach) Rp = max_reach;
+  }
+
+  int n = 0;
+  double rej = pinf();
+  int stopped = 0;
+  for (;;) {  // one pass, plus a restart when a learned proposal was short
+    n = 0;
+    rej = pinf();
+    stopped = 0;
+    const double filt = Rp > 0 ? stop_bound(Rp, cell_min) : pinf();
+    double theta = filt;  // everything above theta is certainly rejected
+    for (int R = 1; R <= max_reach; ++R) {
+      const bool dedupe = 2 * R + 1 > nx || 2 * R + 1 > ny || 2 * R + 1 > nz;
+      ++cnt.v[kCntShells];
+      const double beta = MODE != kModePlainF64 ? fp32_beta(fr, R) : 0.0;
+      float thr = MODE != kModePlainF64 ? fp32_threshold(theta, beta) : 0.f;
+      for_each_shell_offset(R, [&](int dx, int dy, int dz) {
+        int cx, cy, cz, wa, wb, wc;
+        wrap_axis(ix + dx, nx, cx, wa);
+        wrap_axis(iy + dy, ny, cy, wb);
+        wrap_axis(iz + dz, nz, cz, wc);
+        const long long c = cb + ((long long)cz * ny + cy) * (long long)nx + cx;
+        const uint32_t a0 = off[c], a1 = off[c + 1];
+        if (a0 == a1) return;
+        float Dx = 0.f, Dy = 0.f, Dz = 0.f;
+        if (MODE != kModePlainF64) {
+          // lower bound of the distance to any point of the cell
+          const float ga = dx > 0 ? dx - fa : (dx < 0 ? fa + float(-dx - 1) : 0.f);
+          const float gb = dy > 0 ? dy - fb : (dy < 0 ? fb + float(-dy - 1) : 0.f);
+          const float gc = dz > 0 ? dz - fc : (dz < 0 ? fc + float(-dz - 1) : 0.f);
+          const float ga0 = fmaxf(ga, 0.f), gb0 = fmaxf(gb, 0.f), gc0 = fmaxf(gc, 0.f);
+          const float lb = lam * (ga0 * ga0 + gb0 * gb0 + gc0 * gc0);
+          if (lb > thr) {
+            ++cnt.v[kCntPruned];
+            return;
+          }
+          const float fdx = float(dx), fdy = float(dy), fdz = float(dz);
+          Dx = fdx * ev[0] + fdy * ev[3] + fdz * ev[6];
+          Dy = fdx * ev[1] + fdy * ev[4] + fdz * ev[7];
+          Dz = fdx * ev[2] + fdy * ev[5] + fdz * ev[8];
+        }
+        bool have_shift = false;
+        double shx = 0.0, shy = 0.0, shz = 0.0;
+        for (uint32_t t = a0; t < a1; ++t) {
+          if ((long long)t == p) continue;
+          int j;
+          if (MODE != kModePlainF64) {
+            const float4 q = b.rec[t];
+            const float ex = (q.x - plx) + Dx;
+            const float ey = (q.y - ply) + Dy;
+            const float ez = (q.z - plz) + Dz;
+            const float d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+            ++cnt.v[kCntPairs];
+            if (d32 > thr) continue;  // exact distance > theta: rejected
+            ++cnt.v[kCntRerank];
+            j = __float_as_int(q.w);
+          } else {
+            ++cnt.v[kCntPairs];
+            j = -1;
+          }
+          if (!have_shift) {
+            lattice_shift(fr, wa, wb, wc, shx, shy, shz);
+            have_shift = true;
+          }
+          const double d = dist2_shifted(px, py, pz, b.sx[t], b.sy[t], b.sz[t], shx, shy, shz);
+          if (MODE == kModeLearned && d > filt) continue;  // beyond the proposed bound
+          if (j < 0) j = b.sidx[t];
+          if (dedupe) {
+            int s = 0;
+            for (; s < n; ++s)
+              if (hi[s * S] == j) break;
+            if (s < n) {
+              if (d < hd[s * S]) {
+                hd[s * S] = d;
+                if (n >= k) {
+                  heap_sift_down(hd, hi, S, s, n);
+                  theta = fmin(hd[0], filt);
+                  if (MODE != kModePlainF64) thr = fp32_threshold(theta, beta);
+                }
+              }
+              continue;
+            }
+          }
+          if (n < k) {
+            hd[n * S] = d;
+            hi[n * S] = j;
+            ++n;
+            ++cnt.v[kCntInserts];
+            if (n == k) {
+              heap_build(hd, hi, S, n);
+              theta = fmin(hd[0], filt);
+              if (MODE != kModePlainF64) thr = fp32_threshold(theta, beta);
+            }
+          } else if (d < hd[0]) {
+            rej = fmin(rej, hd[0]);
+            hd[0] = d;
+            hi[0] = j;
+            heap_sift_down(hd, hi, S, 0, n);
+            ++cnt.v[kCntInserts];
+            theta = fmin(hd[0], filt);
+            if (MODE != kModePlainF64) thr = fp32_threshold(theta, beta);
+          } else {
+            rej = fmin(rej, d);
+          }
+        }
+      });
+      if (n >= k && hd[0] <= stop_bound(R, cell_min)) {
+        stopped = R;
+        break;
+      }
+      if (MODE == kModeLearned && Rp > 0 && R == Rp) break;  // proposal too short
+    }
+    if (MODE == kModeLearned && Rp > 0) {
+      if (stopped == 0) {
+        ++cnt.v[kCntPropUnder];
+        cnt.v[kCntRevisit] += Rp;
+        Rp = 0;
+        continue;  // walk again without the filter
+      }
+      if (stopped < Rp)
+        ++cnt.v[kCntPropOver];
+      else
+        ++cnt.v[kCntPropExact];
+    }
+    break;
+  }
+  const int i = b.sidx[p];
+  if (n >= k && !(rej > hd[0])) {
+    // a value equal to the k-th was left out: which of the tied indices the
+    // reference keeps depends on its exact push order
+    ++cnt.v[kCntReplays];
+    const int m = replay_walk(b, fr, p, hd, hi, S);
+    write_row(b, fr, i, hd, hi, S, m);
+    return;
+  }
+  if (n < k) heap_build(hd, hi, S, n);
+  heap_sort(hd, hi, S, n);
+  write_row(b, fr, i, hd, hi, S, n);
+}
+
+// 128 registers per thread at every block size (the heap is in shared memory).
+template <int MODE, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 65536 / (128 * BLOCK)) k_walk(BatchBuffers b) {
+  extern __shared__ double smem[];
+  double *hd = smem + threadIdx.x;
+  int *hi = reinterpret_cast<int *>(smem + (size_t)b.kmax * BLOCK) + threadIdx.x;
+  const long long total = b.off[b.ncells];
+  const int lane = threadIdx.x & 31;
+  LocalCounters cnt;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(b.work, 32u);
+    base = __shfl_sync(kFull, base, 0);
+    if ((long long)base >= total) break;
+    const long long p = (long long)base + lane;
+    if (p < total) walk_source<MODE>(b, p, hd, hi, BLOCK, cnt);
+    __syncwarp();
+  }
+  flush_counters(b, cnt);
+}
+
+// Every queued source through the literal replay (NaN frames, very large k).
 __global__ void __launch_bounds__(128) k_replay(BatchBuffers b) {
   long long cnt = *b.replay_count;
   if (cnt > b.replay_cap) cnt = b.replay_cap;
@@ -348,10 +492,15 @@ __global__ void __launch_bounds__(128) k_replay(BatchBuffers b) {
   if (tid >= b.replay_threads) return;
   double *hd = b.replay_d + tid * b.kmax;
   int *hi = b.replay_i + tid * b.kmax;
-  for (long long q = tid; q < cnt; q += b.replay_threads) replay_source(b, b.replay_list[q], hd, hi);
+  for (long long q = tid; q < cnt; q += b.replay_threads) {
+    const long long p = b.replay_list[q];
+    const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
+    const FrameDesc &fr = b.frames[f];
+    const int m = replay_walk(b, fr, p, hd, hi, 1);
+    write_row(b, fr, b.sidx[p], hd, hi, 1, m);
+  }
 }
 
-// Every source of the batch through the exact replay (large k, or on request).
 __global__ void k_queue_all(BatchBuffers b) {
   const long long total = b.off[b.ncells];
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < total;
@@ -367,18 +516,29 @@ int sm_count() {
   return sms;
 }
 
-template <int BLOCK>
-cudaError_t launch_f64(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
-  const size_t sm = walk_smem_bytes(w.mode, BLOCK, b.kmax);
-  cudaError_t e = cudaFuncSetAttribute(k_walk_f64<BLOCK>,
+template <int MODE, int BLOCK>
+cudaError_t launch_mode(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
+  const size_t sm = walk_smem_bytes(MODE, BLOCK, b.kmax);
+  cudaError_t e = cudaFuncSetAttribute(k_walk<MODE, BLOCK>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
   if (e != cudaSuccess) return e;
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_f64<BLOCK>, BLOCK, sm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk<MODE, BLOCK>, BLOCK, sm);
   if (per_sm < 1) per_sm = 1;
   const int grid = w.grid > 0 ? w.grid : sm_count() * per_sm;
-  k_walk_f64<BLOCK><<<grid, BLOCK, sm, s>>>(b);
+  k_walk<MODE, BLOCK><<<grid, BLOCK, sm, s>>>(b);
   return cudaGetLastError();
+}
+
+template <int MODE>
+cudaError_t launch_block(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
+  switch (w.block) {
+    case 32: return launch_mode<MODE, 32>(b, w, s);
+    case 64: return launch_mode<MODE, 64>(b, w, s);
+    case 128: return launch_mode<MODE, 128>(b, w, s);
+    case 256: return launch_mode<MODE, 256>(b, w, s);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace
@@ -397,16 +557,13 @@ int walk_max_block(int mode, int kmax) {
 }
 
 cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
-  if (w.mode == kModeReplayAll) {
-    k_queue_all<<<sm_count() * 4, 256, 0, s>>>(b);
-    return cudaGetLastError();
-  }
-  switch (w.block) {
-    case 32: return launch_f64<32>(b, w, s);
-    case 64: return launch_f64<64>(b, w, s);
-    case 128: return launch_f64<128>(b, w, s);
-    case 256: return launch_f64<256>(b, w, s);
-    default: return cudaErrorInvalidValue;
+  switch (w.mode) {
+    case kModeReplayAll:
+      k_queue_all<<<sm_count() * 4, 256, 0, s>>>(b);
+      return cudaGetLastError();
+    case kModeFastF32: return launch_block<kModeFastF32>(b, w, s);
+    case kModeLearned: return launch_block<kModeLearned>(b, w, s);
+    default: return launch_block<kModePlainF64>(b, w, s);
   }
 }
 

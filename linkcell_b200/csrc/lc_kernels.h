@@ -46,6 +46,7 @@ struct BatchBuffers {
   int replay_threads = 0;
   int kmax = 0;
   long long *counters = nullptr; // walk statistics (see WalkCounters)
+  const int8_t *proposal = nullptr;  // learned walk: proposed shell per sorted source (0: none)
 };
 
 // Walk statistics accumulated on the device (counters[...]).

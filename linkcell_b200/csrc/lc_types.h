@@ -43,8 +43,10 @@ struct FrameDesc {
   double widths[3];  // perpendicular widths |det| / |b x c| ...
   double cell_min;   // min(w_a / n_a)
   double lam_min;    // smallest eigenvalue of the bin-unit metric (pruning)
+  double eps64;      // bound on the FP64 rounding of the reference distance terms
   float ev[9];       // FP32 cell edge vectors: ev[axis*3 + comp] = h[axis][comp] / n_axis
-  float corner_pad[3];
+  float nhinv[9];    // FP32 (H / n)^-1 rows: bin-unit coordinates of a Cartesian offset
+  float ell;         // max over components of sum over axes |ev[axis][comp]|
   int nx, ny, nz;
   int ortho;         // Cell::is_ortho (src/cell.rs:322-331)
   int max_reach;     // max(nx, ny, nz) / 2 + 1

@@ -153,7 +153,18 @@ Code plan_frame(const double *rows, const double *origin, double cell_hint, int 
   double g[3][3];
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) g[i][j] = ev[i][0] * ev[j][0] + ev[i][1] * ev[j][1] + ev[i][2] * ev[j][2];
-  fd.lam_min = std::max(0.0, min_eig_sym3(g));
+  fd.lam_min = std::max(0.0, min_eig_sym3(g)) * (1.0 - 1e-6);
+  // (H / n)^-1 = diag(n) Hinv: row a of Hinv times n_a
+  for (int ax = 0; ax < 3; ++ax)
+    for (int r = 0; r < 3; ++r) fd.nhinv[ax * 3 + r] = float(double(nb[ax]) * fd.hinv[r * 3 + ax]);
+  double ell = 0.0;
+  for (int r = 0; r < 3; ++r)
+    ell = std::max(ell, std::fabs(ev[0][r]) + std::fabs(ev[1][r]) + std::fabs(ev[2][r]));
+  fd.ell = float(ell * (1.0 + 1e-6));
+  double mag = std::fabs(origin[0]) + std::fabs(origin[1]) + std::fabs(origin[2]);
+  for (int t = 0; t < 9; ++t) mag += std::fabs(fd.h[t]);
+  // generous: 2^-36 of the largest coordinate / shift magnitude per unit wrap
+  fd.eps64 = std::ldexp(mag, -36);
   return Code::Ok;
 }
 
@@ -234,7 +245,7 @@ void WorkspaceImpl::release_all() {
   rel(work_); rel(replay_count_); rel(tile_state_); rel(status_); rel(frame_flags_);
   rel(sidx_); rel(replay_list_); rel(replay_i_); rel(scell_); rel(sx_); rel(sy_); rel(sz_);
   rel(replay_d_); rel(rec_); rel(frames_); rel(counters_); rel(h_xyz_); rel(h_d2_);
-  rel(h_mask_); rel(h_nn_); rel(active_);
+  rel(h_mask_); rel(h_nn_); rel(active_); rel(proposal_);
 }
 
 #define LC_TRY(expr)                        \
@@ -357,6 +368,16 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   LC_TRY(launch_fold_bin(b, s));
   LC_TRY(launch_scan(b, s));
   LC_TRY(launch_place(b, s));
+  if (wl.mode == kModeLearned) {
+    // shell proposals per sorted source
+    LC_TRY(grow(proposal_, P));
+    if (opts.fixed_proposal > 0) {
+      LC_TRY(cudaMemsetAsync(proposal_.p, std::min(opts.fixed_proposal, 127), P, s));
+    } else {
+      LC_TRY(cudaMemsetAsync(proposal_.p, 0, P, s));
+    }
+    b.proposal = proposal_.p;
+  }
   if (collect_stats) LC_TRY(cudaEventRecord(ev_[1], s));
   LC_TRY(launch_walk(b, wl, s));
   if (collect_stats) LC_TRY(cudaEventRecord(ev_[2], s));

@@ -46,6 +46,7 @@ struct WalkOptions {
   int mode = kModePlainF64;
   int block = 0;   // 0: autotune / default
   int prune = 1;
+  int fixed_proposal = 0;  // learned walk: > 0 proposes this shell for every source
 };
 
 struct Stats {
@@ -110,6 +111,7 @@ class WorkspaceImpl {
   Buf<float4> rec_;
   Buf<FrameDesc> frames_;
   Buf<long long> counters_;
+  Buf<int8_t> proposal_;
   // host-pointer staging
   Buf<double> h_xyz_, h_d2_;
   Buf<int> h_mask_, h_nn_;

@@ -58,6 +58,9 @@ class DeviceRunner:
     def set_mode(self, mode):
         assert self.L.lc_gpu_set_mode(self.ws, mode) == 0
 
+    def set_proposal(self, shell):
+        assert self.L.lc_gpu_set_proposal(self.ws, shell) == 0
+
     def run(self, xyz, cell, k, mask=None, hint=0.0, n_frames=1, wait=1):
         torch = self.torch
         x = torch.as_tensor(np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3),

@@ -193,3 +193,36 @@ def test_async_wait_and_reuse(runner, oracle_mod):
         xyz = rng.random((n, 3)) * 25.0
         want = _oracle(oracle_mod, xyz, [25.0, 25.0, 25.0], 8)
         assert_same(runner.run(xyz, [25.0, 25.0, 25.0], 8, wait=0), want, f"n={n}")
+
+
+@pytest.mark.parametrize("shell", [1, 2, 3, 6])
+def test_learned_walk_any_proposal_is_exact(runner, oracle_mod, shell):
+    """The learned walk opens the proposed shell with its stop bound as the
+    filter; short proposals restart, long ones over-visit; results never
+    change."""
+    from linkcell_b200 import workloads as W
+    w = W.bimodal_triclinic(n=80000, seed=31, k=32)
+    want = _oracle(oracle_mod, w["xyz"], w["cell"], 32, hint=3.0)
+    runner.set_mode(2)
+    runner.set_proposal(shell)
+    try:
+        assert_same(runner.run(w["xyz"], w["cell"], 32, hint=3.0), want, f"proposal {shell}")
+        cnt, _ = runner.stats()
+        under, over, exact = cnt[6], cnt[7], cnt[8]
+        assert under + over + exact > 0
+        if shell == 1:
+            assert under > 0
+    finally:
+        runner.set_proposal(0)
+        runner.set_mode(0)
+
+
+def test_fp32_counters_show_filtering(runner, oracle_mod):
+    from linkcell_b200 import workloads as W
+    w = W.bimodal_triclinic(n=100000, seed=41, k=16)
+    runner.set_mode(1)
+    runner.run(w["xyz"], w["cell"], 16, hint=3.0)
+    cnt, ms = runner.stats()
+    pairs, reranks, pruned = cnt[0], cnt[5], cnt[4]
+    assert reranks < pairs and pruned > 0 and ms > 0
+    runner.set_mode(0)
