@@ -92,6 +92,36 @@ int lc_gpu_get_mode(lc_gpu_workspace *ws);
  * proposal; only the work changes. */
 int lc_gpu_set_proposal(lc_gpu_workspace *ws, int shell);
 
+/* Learned walk: the shell-proposal network. params holds lc_gpu_mlp_params()
+ * host floats in the layout W1[64][126] b1[64] W2[64][64] b2[64] W3[8][64]
+ * b3[8] (inputs: log(1 + occupancy) of the 5x5x5 cells around the source's
+ * cell, then k / 64; outputs: logits of the settled shell 1..7 and "8 or
+ * more"). A cell's proposal is the smallest shell whose cumulative
+ * probability reaches tau. */
+int lc_gpu_set_model(lc_gpu_workspace *ws, const float *params, size_t n_params, float tau);
+
+/* Training data. With logging on, a search records the settled shell of
+ * every source; lc_gpu_training_rows then writes, for the sorted sources
+ * first, first + stride, ..., up to cap rows of 126 features into device
+ * X and the class (settled shell - 1, capped at 7) into device y. Returns
+ * the number of rows, or a negative value on error. */
+int lc_gpu_log_shells(lc_gpu_workspace *ws, int on);
+long long lc_gpu_training_rows(lc_gpu_workspace *ws, float *X, int *y, long long cap,
+                               long long stride, long long first);
+
+/* The network's kernels on device buffers, for training: forward
+ * (softmax probabilities, batch x 8), gradient of the mean cross-entropy
+ * (and the loss), and one Adam step (step counts from 1). scratch holds
+ * lc_gpu_mlp_scratch_floats(batch) floats. */
+int lc_gpu_mlp_params(void);
+size_t lc_gpu_mlp_scratch_floats(int batch);
+int lc_gpu_mlp_forward(const float *params, const float *X, int batch, float *probs,
+                       float *scratch, void *stream);
+int lc_gpu_mlp_grad(const float *params, const float *X, const int *y, int batch, float *grad,
+                    float *loss, float *scratch, void *stream);
+int lc_gpu_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr,
+                    void *stream);
+
 /* Enqueue on the caller's stream instead of the workspace's own one
  * (NULL restores the workspace stream). */
 int lc_gpu_set_stream(lc_gpu_workspace *ws, void *stream);

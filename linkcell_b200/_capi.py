@@ -34,7 +34,9 @@ EXPORTS = (
     "lc_gpu_knearest", "lc_gpu_knearest_many", "lc_gpu_knearest_many_dcell", "lc_gpu_queue",
     "lc_gpu_wait", "lc_gpu_alloc", "lc_gpu_free", "lc_gpu_fill_i32", "lc_gpu_memcpy",
     "lc_gpu_set_mode", "lc_gpu_get_mode", "lc_gpu_set_proposal", "lc_gpu_set_stream", "lc_gpu_stats",
-    "lc_gpu_phase_times",
+    "lc_gpu_phase_times", "lc_gpu_set_model", "lc_gpu_log_shells", "lc_gpu_training_rows",
+    "lc_gpu_mlp_params", "lc_gpu_mlp_scratch_floats", "lc_gpu_mlp_forward", "lc_gpu_mlp_grad",
+    "lc_gpu_mlp_adam",
     "lc_gpu_knearest_batch",
 )
 
@@ -85,6 +87,18 @@ def load():
     L.lc_gpu_set_stream.argtypes = [vp, vp]
     L.lc_gpu_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), i, dp]
     L.lc_gpu_phase_times.argtypes = [vp, dp, dp, dp]
+    fp = ctypes.POINTER(ctypes.c_float)
+    ll = ctypes.c_longlong
+    L.lc_gpu_set_model.argtypes = [vp, fp, sz, ctypes.c_float]
+    L.lc_gpu_log_shells.argtypes = [vp, i]
+    L.lc_gpu_training_rows.argtypes = [vp, vp, vp, ll, ll, ll]
+    L.lc_gpu_training_rows.restype = ll
+    L.lc_gpu_mlp_params.restype = i
+    L.lc_gpu_mlp_scratch_floats.argtypes = [i]
+    L.lc_gpu_mlp_scratch_floats.restype = sz
+    L.lc_gpu_mlp_forward.argtypes = [vp, vp, i, vp, vp, vp]
+    L.lc_gpu_mlp_grad.argtypes = [vp, vp, vp, i, vp, vp, vp, vp]
+    L.lc_gpu_mlp_adam.argtypes = [vp, vp, vp, vp, i, ctypes.c_float, vp]
     L.lc_gpu_knearest_batch.argtypes = [vp, vp, ctypes.POINTER(LcFrame), sz, vp, vp, vp, i]
     _lib = L
     return L

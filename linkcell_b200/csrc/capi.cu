@@ -18,6 +18,7 @@
 #include "../../include/linkcell.h"
 #include "../../include/linkcell_gpu.h"
 #include "../../include/linkcell_gpu.hpp"
+#include "lc_mlp.h"
 #include "workspace.h"
 
 namespace {
@@ -468,6 +469,65 @@ int lc_gpu_set_mode(lc_gpu_workspace *ws, int mode) {
 }
 
 int lc_gpu_get_mode(lc_gpu_workspace *ws) { return ws ? ws->ws.opts.mode : -1; }
+
+int lc_gpu_set_model(lc_gpu_workspace *ws, const float *params, size_t n_params, float tau) {
+  if (!ws || !params) return gpu_fail(Code::NullPointer);
+  if (!(tau > 0.f && tau <= 1.f)) return gpu_fail_msg("tau must lie in (0, 1]");
+  std::string detail;
+  const Code c = ws->ws.set_model(params, n_params, tau, detail);
+  if (c != Code::Ok) return gpu_fail_msg(detail.empty() ? lc::gpu_message(c) : detail);
+  return 0;
+}
+
+int lc_gpu_log_shells(lc_gpu_workspace *ws, int on) {
+  if (!ws) return gpu_fail(Code::NullPointer);
+  ws->ws.opts.log_shells = on ? 1 : 0;
+  return 0;
+}
+
+long long lc_gpu_training_rows(lc_gpu_workspace *ws, float *X, int *y, long long cap,
+                               long long stride, long long first) {
+  if (!ws || !X || !y) return -gpu_fail(Code::NullPointer);
+  long long rows = 0;
+  std::string detail;
+  const Code c = ws->ws.training_rows(X, y, cap, stride, first, rows, detail);
+  if (c != Code::Ok) return -gpu_fail_msg(detail.empty() ? lc::gpu_message(c) : detail);
+  return rows;
+}
+
+int lc_gpu_mlp_params(void) { return lc::kMlpParams; }
+
+size_t lc_gpu_mlp_scratch_floats(int batch) { return lc::MlpScratch::floats(batch); }
+
+int lc_gpu_mlp_forward(const float *params, const float *X, int batch, float *probs,
+                       float *scratch, void *stream) {
+  if (!params || !X || !probs || !scratch) return gpu_fail(Code::NullPointer);
+  lc::MlpScratch t = lc::MlpScratch::carve(scratch, batch);
+  const cudaError_t e =
+      lc::mlp_forward(params, X, batch, t, probs, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return gpu_fail(Code::Cuda, cudaGetErrorString(e));
+  return 0;
+}
+
+int lc_gpu_mlp_grad(const float *params, const float *X, const int *y, int batch, float *grad,
+                    float *loss, float *scratch, void *stream) {
+  if (!params || !X || !y || !grad || !scratch) return gpu_fail(Code::NullPointer);
+  lc::MlpScratch t = lc::MlpScratch::carve(scratch, batch);
+  const cudaError_t e =
+      lc::mlp_grad(params, X, y, batch, t, grad, loss, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return gpu_fail(Code::Cuda, cudaGetErrorString(e));
+  return 0;
+}
+
+int lc_gpu_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr,
+                    void *stream) {
+  if (!params || !grad || !m || !v) return gpu_fail(Code::NullPointer);
+  if (step < 1) return gpu_fail_msg("adam step starts at 1");
+  const cudaError_t e =
+      lc::mlp_adam(params, grad, m, v, step, lr, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return gpu_fail(Code::Cuda, cudaGetErrorString(e));
+  return 0;
+}
 
 int lc_gpu_set_proposal(lc_gpu_workspace *ws, int shell) {
   if (!ws) return gpu_fail(Code::NullPointer);

@@ -449,6 +449,7 @@ __device__ void walk_source(const BatchBuffers &b, long long p, double *hd, int 
     }
     break;
   }
+  if (b.stop_log) b.stop_log[p] = int8_t(stopped > 0 ? (stopped < 127 ? stopped : 127) : 0);
   const int i = b.sidx[p];
   if (n >= k && !(rej > hd[0])) {
     // a value equal to the k-th was left out: which of the tied indices the

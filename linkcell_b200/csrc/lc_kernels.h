@@ -47,6 +47,7 @@ struct BatchBuffers {
   int kmax = 0;
   long long *counters = nullptr; // walk statistics (see WalkCounters)
   const int8_t *proposal = nullptr;  // learned walk: proposed shell per sorted source (0: none)
+  int8_t *stop_log = nullptr;        // optional: settled shell per sorted source (training)
 };
 
 // Walk statistics accumulated on the device (counters[...]).

@@ -5,6 +5,8 @@
 // (src/cell.rs:97-124,322-388 and src/knearest.rs:42-48,377-397,430).
 #include "workspace.h"
 
+#include "lc_mlp.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -245,7 +247,8 @@ void WorkspaceImpl::release_all() {
   rel(work_); rel(replay_count_); rel(tile_state_); rel(status_); rel(frame_flags_);
   rel(sidx_); rel(replay_list_); rel(replay_i_); rel(scell_); rel(sx_); rel(sy_); rel(sz_);
   rel(replay_d_); rel(rec_); rel(frames_); rel(counters_); rel(h_xyz_); rel(h_d2_);
-  rel(h_mask_); rel(h_nn_); rel(active_); rel(proposal_);
+  rel(h_mask_); rel(h_nn_); rel(active_); rel(proposal_); rel(cell_prop_); rel(stop_log_);
+  rel(model_);
 }
 
 #define LC_TRY(expr)                        \
@@ -368,17 +371,24 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   LC_TRY(launch_fold_bin(b, s));
   LC_TRY(launch_scan(b, s));
   LC_TRY(launch_place(b, s));
+  if (opts.log_shells) {
+    LC_TRY(grow(stop_log_, P));
+    b.stop_log = stop_log_.p;
+  }
+  if (collect_stats) LC_TRY(cudaEventRecord(ev_[1], s));
   if (wl.mode == kModeLearned) {
-    // shell proposals per sorted source
+    // shell proposals per sorted source (part of the walk phase)
     LC_TRY(grow(proposal_, P));
     if (opts.fixed_proposal > 0) {
       LC_TRY(cudaMemsetAsync(proposal_.p, std::min(opts.fixed_proposal, 127), P, s));
+    } else if (has_model_) {
+      LC_TRY(grow(cell_prop_, C));
+      LC_TRY(mlp_propose(model_.p, b, cell_prop_.p, proposal_.p, tau_, s));
     } else {
       LC_TRY(cudaMemsetAsync(proposal_.p, 0, P, s));
     }
     b.proposal = proposal_.p;
   }
-  if (collect_stats) LC_TRY(cudaEventRecord(ev_[1], s));
   LC_TRY(launch_walk(b, wl, s));
   if (collect_stats) LC_TRY(cudaEventRecord(ev_[2], s));
   LC_TRY(launch_replay(b, s));
@@ -392,6 +402,38 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
     detail = "device status " + std::to_string(st);
     return Code::DeviceStatus;
   }
+  return Code::Ok;
+}
+
+Code WorkspaceImpl::set_model(const float *params, size_t n, float tau, std::string &detail) {
+  if (n != size_t(kMlpParams)) {
+    detail = "model must have " + std::to_string(kMlpParams) + " parameters";
+    return Code::DeviceStatus;
+  }
+  LC_TRY(grow(model_, n));
+  LC_TRY(cudaMemcpyAsync(model_.p, params, n * sizeof(float), cudaMemcpyHostToDevice, stream()));
+  LC_TRY(cudaStreamSynchronize(stream()));
+  has_model_ = true;
+  tau_ = tau;
+  return Code::Ok;
+}
+
+Code WorkspaceImpl::training_rows(float *X, int *y, long long cap, long long stride,
+                                  long long first, long long &rows, std::string &detail) {
+  rows = 0;
+  if (!bb_.stop_log || !bb_.off) {
+    detail = "no logged search";
+    return Code::DeviceStatus;
+  }
+  uint32_t total = 0;
+  LC_TRY(cudaStreamSynchronize(stream()));
+  LC_TRY(cudaMemcpy(&total, bb_.off + bb_.ncells, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (stride < 1) stride = 1;
+  if (first < 0 || first >= (long long)total) return Code::Ok;
+  const long long avail = ((long long)total - first + stride - 1) / stride;
+  rows = std::min(avail, cap);
+  LC_TRY(mlp_training_rows(bb_, bb_.stop_log, stride, first, X, y, rows, stream()));
+  LC_TRY(cudaStreamSynchronize(stream()));
   return Code::Ok;
 }
 

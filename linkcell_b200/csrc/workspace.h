@@ -47,6 +47,7 @@ struct WalkOptions {
   int block = 0;   // 0: autotune / default
   int prune = 1;
   int fixed_proposal = 0;  // learned walk: > 0 proposes this shell for every source
+  int log_shells = 0;      // record the settled shell of every source (training data)
 };
 
 struct Stats {
@@ -87,6 +88,13 @@ class WorkspaceImpl {
   // Device-side view of the last batch (diagnostics and tests).
   const BatchBuffers &buffers() const { return bb_; }
 
+  // Learned proposals: copy the MLP parameters (host floats) in.
+  Code set_model(const float *params, size_t n, float tau, std::string &detail);
+  bool has_model() const { return has_model_; }
+  // Training rows of the last logged search (device X / y buffers).
+  Code training_rows(float *X, int *y, long long cap, long long stride, long long first,
+                     long long &rows, std::string &detail);
+
  private:
   template <class T>
   struct Buf {
@@ -111,7 +119,10 @@ class WorkspaceImpl {
   Buf<float4> rec_;
   Buf<FrameDesc> frames_;
   Buf<long long> counters_;
-  Buf<int8_t> proposal_;
+  Buf<int8_t> proposal_, cell_prop_, stop_log_;
+  Buf<float> model_;
+  bool has_model_ = false;
+  float tau_ = 0.9f;
   // host-pointer staging
   Buf<double> h_xyz_, h_d2_;
   Buf<int> h_mask_, h_nn_;

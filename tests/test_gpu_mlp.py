@@ -1,0 +1,97 @@
+"""The shell-proposal network on the GPU: forward, gradient and Adam kernels
+against the CPU reference (oracle/mlp_ref.py); training lowers the loss; the
+learned walk with the shipped network stays exact and does less work than
+the walk without it."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _trainer(params, batch):
+    from linkcell_b200.learn import Trainer
+    return Trainer(params, batch=batch)
+
+
+def test_forward_and_gradient_match_cpu(gpu):
+    import torch
+    from linkcell_b200.learn import init_params
+    from oracle import mlp_ref as M
+    rng = np.random.default_rng(1)
+    p = init_params(5)
+    p[M.N_HID * M.N_IN:M.N_HID * M.N_IN + M.N_HID] = rng.normal(0, 0.1, M.N_HID)  # biases
+    for B in (1, 37, 300):
+        X = rng.random((B, M.N_IN)).astype(np.float32) * 2.0
+        y = rng.integers(0, M.N_OUT, B).astype(np.int32)
+        t = _trainer(p, B)
+        Xd, yd = torch.as_tensor(X, device="cuda"), torch.as_tensor(y, device="cuda")
+        probs = t.probs(Xd).cpu().numpy()
+        ref = M.forward(p, X)
+        assert np.max(np.abs(probs - ref["probs"])) < 2e-5
+        g, loss = t.grad(Xd, yd)
+        lref, gref = M.loss_and_grad(p, X, y)
+        g = g.cpu().numpy()
+        rel = np.linalg.norm(g - gref) / np.linalg.norm(gref)
+        assert rel < 1e-4, rel
+        assert abs(float(loss.item()) - lref) < 1e-4 * max(1.0, abs(lref))
+
+
+def test_adam_matches_cpu(gpu):
+    import torch
+    from linkcell_b200.learn import init_params
+    from oracle import mlp_ref as M
+    rng = np.random.default_rng(2)
+    p = init_params(7)
+    X = rng.random((64, M.N_IN)).astype(np.float32)
+    y = rng.integers(0, M.N_OUT, 64).astype(np.int32)
+    t = _trainer(p, 64)
+    Xd, yd = torch.as_tensor(X, device="cuda"), torch.as_tensor(y, device="cuda")
+    pc, m, v = p.astype(np.float64), np.zeros(p.size), np.zeros(p.size)
+    for step in range(1, 4):
+        g, _ = t.grad(Xd, yd)  # the Adam kernel is checked on the GPU's own gradient
+        pc, m, v = M.adam(pc, g.cpu().numpy().astype(np.float64), m, v, step, 1e-3)
+        t.adam_step(lr=1e-3)
+        assert np.max(np.abs(t.params() - pc)) < 1e-6
+
+
+def test_training_lowers_loss(gpu):
+    from linkcell_b200 import learn
+    X, y = learn.collect(runs=6, n=30000, rows_per_run=1500, log=lambda *a: None)
+    assert X.shape[0] > 5000 and int(y.min()) >= 0 and int(y.max()) <= 7
+    t0 = learn.Trainer(learn.init_params(0), batch=1024)
+    _, l0 = t0.grad(X[:1024].contiguous(), y[:1024].contiguous())
+    l0 = float(l0.item())
+    t, (Xv, yv) = learn.train(X, y, epochs=4, batch=1024, log=lambda *a: None)
+    _, l1 = t.grad(Xv[:1024].contiguous(), yv[:1024].contiguous())
+    assert float(l1.item()) < 0.7 * l0
+
+
+def test_learned_walk_with_network_is_exact_and_saves_work(gpu, oracle_mod):
+    """The shipped network's proposals keep every index exact and cut the
+    walk's work against the FP32 walk without proposals (same GPU, same
+    inputs): fewer candidate distances and FP64 reranks."""
+    import os
+    from gpu_helpers import DeviceRunner, assert_same
+    from linkcell_b200 import learn, workloads as W
+    if not os.path.exists(learn.MODEL_PATH):
+        pytest.skip("no trained network shipped")
+    w = W.bimodal_triclinic(n=150000, seed=77, k=32)
+    want = oracle_mod.knearest(w["xyz"], w["cell"], 32, cell_hint=3.0)
+    r = DeviceRunner()
+    try:
+        r.set_mode(1)
+        assert_same(r.run(w["xyz"], w["cell"], 32, hint=3.0), want, "fast")
+        fast, _ = r.stats()
+        learn.attach(r.ws)
+        r.set_mode(2)
+        assert_same(r.run(w["xyz"], w["cell"], 32, hint=3.0), want, "learned")
+        lrn, _ = r.stats()
+    finally:
+        r.close()
+    proposals = lrn[6] + lrn[7] + lrn[8]
+    assert proposals > 0.9 * 150000
+    assert lrn[6] < 0.05 * proposals  # short proposals (restarts) stay rare
+    assert lrn[5] < fast[5]  # fewer FP64 reranks
