@@ -225,6 +225,14 @@ def run_ours(args):
                                     nn.data_ptr(), d2.data_ptr(), 0)
         assert rc == 0, _capi.gpu_error()
 
+    model_info = None
+    if (args.mode if args.mode >= 0 else 2) == 2:
+        from linkcell_b200 import learn
+        if os.path.exists(learn.MODEL_PATH):
+            learn.attach(ws)
+            _, tau, meta = learn.load()
+            model_info = {"path": os.path.relpath(learn.MODEL_PATH, ROOT), "tau": tau, "trained": meta}
+
     def time_mode(mode, steps, warmup):
         assert L.lc_gpu_set_mode(ws, mode) == 0
         for _ in range(warmup):
@@ -342,7 +350,7 @@ def run_ours(args):
                           "walk_ms": statistics.mean(plain_walk)},
            "speedup_vs_plain": value / plain_value, "walk_ms": walk_avg_ms,
            "prep_ms": statistics.mean(prep_ms), "replay_ms": statistics.mean(replay_ms),
-           "walk_stats_last_step": walk_stats,
+           "walk_stats_last_step": walk_stats, "model": model_info,
            "plain_walk_stats_last_step": {nm: plain_cnt[i] for i, nm in enumerate(names)}}
     if rank == 0:
         print(json.dumps(out), flush=True)
