@@ -153,6 +153,24 @@ int lc_gpu_knearest_batch(lc_gpu_workspace *ws, const double *xyz, const lc_fram
                           size_t n_frames, const int *mask, int *out_nn, double *out_d2,
                           int wait);
 
+/* One search that allocates no device memory (no counterpart in the
+ * reference). For callers that cannot call cudaMalloc: hosts whose own pool
+ * allocator owns all device memory, real-time loops that must not allocate,
+ * plug-ins inside frameworks that own the allocator. Every scratch buffer
+ * lives in one fixed static device array (about 4.8 MB on each GPU that
+ * loads the library, held until exit); the caller passes device xyz, mask
+ * (n ints or NULL), out_nn and out_d2 (n * k each, out_d2 may be NULL) and
+ * a host lc_cell. Limits: n <= 65536 points, at most 65536 linked cells,
+ * k <= 64; larger searches fail with an error. Work is enqueued on stream
+ * (a cudaStream_t, NULL for the legacy default stream); wait != 0 also
+ * waits and checks the device status. The first call on a device looks up
+ * the array's device address. All calls share the array and leave their
+ * contents in it: calls that overlap on the GPU race and must not be
+ * issued. Results equal lc_gpu_knearest's. */
+int lc_gpu_knearest_noalloc(const double *xyz, size_t n, const struct lc_cell *simbox, size_t k,
+                            const int *mask, double cell_hint, int *out_nn, double *out_d2,
+                            void *stream, int wait);
+
 #ifdef __cplusplus
 }
 #endif

@@ -147,6 +147,16 @@ int host_search(const double *xyz, size_t n, size_t n_frames, const lc_cell *sim
 
 }  // namespace
 
+namespace lc {
+// Sets (or, with nullptr, clears) this thread's lc_gpu_last_error slot.
+void set_gpu_error_message(const char *msg) {
+  if (msg)
+    t_gpu_err = msg;
+  else
+    t_gpu_err.clear();
+}
+}  // namespace lc
+
 // ======================================================================
 // C++ class (include/linkcell_gpu.hpp)
 namespace linkcell {
