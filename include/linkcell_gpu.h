@@ -122,6 +122,11 @@ int lc_gpu_mlp_grad(const float *params, const float *X, const int *y, int batch
 int lc_gpu_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr,
                     void *stream);
 
+/* Threads per source of the walk: 32 (a warp per source, the default) or 1
+ * (a thread per source, its heap in shared memory). The environment
+ * variable LINKCELL_TPP sets the default of new workspaces. */
+int lc_gpu_set_tpp(lc_gpu_workspace *ws, int tpp);
+
 /* Enqueue on the caller's stream instead of the workspace's own one
  * (NULL restores the workspace stream). */
 int lc_gpu_set_stream(lc_gpu_workspace *ws, void *stream);

@@ -480,6 +480,13 @@ int lc_gpu_set_mode(lc_gpu_workspace *ws, int mode) {
 
 int lc_gpu_get_mode(lc_gpu_workspace *ws) { return ws ? ws->ws.opts.mode : -1; }
 
+int lc_gpu_set_tpp(lc_gpu_workspace *ws, int tpp) {
+  if (!ws) return gpu_fail(Code::NullPointer);
+  if (tpp != 1 && tpp != 32) return gpu_fail_msg("threads per source must be 1 or 32");
+  ws->ws.opts.tpp = tpp;
+  return 0;
+}
+
 int lc_gpu_set_model(lc_gpu_workspace *ws, const float *params, size_t n_params, float tau) {
   if (!ws || !params) return gpu_fail(Code::NullPointer);
   if (!(tau > 0.f && tau <= 1.f)) return gpu_fail_msg("tau must lie in (0, 1]");

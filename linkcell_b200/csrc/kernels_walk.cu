@@ -35,6 +35,10 @@
 //    passes R_p without stopping restarts without it.
 #include <cuda/atomic>
 
+#include <algorithm>
+#include <cstdlib>
+#include <vector>
+
 #include "lc_kernels.h"
 
 namespace lc {
@@ -510,11 +514,472 @@ __global__ void k_queue_all(BatchBuffers b) {
   if (blockIdx.x == 0 && threadIdx.x == 0) *b.replay_count = uint32_t(total);
 }
 
+// ------------------------------------------------------------------------
+// Team walk: one warp per source.
+//
+// Lanes take the offsets of a shell (32 at a time, near-first order), load
+// their cells' occupant ranges, and a warp scan lays the candidates out so
+// that every lane evaluates one candidate per round. The k best (d2, index)
+// pairs live in a warp-distributed list sorted ascending: position
+// lane * KPL + s. Control flow is uniform across the warp; only the FP32
+// test, the exact recompute and the insertions are predicated.
+
+// Offset e of shell R: the near-first table for R <= rmax (entries of shell
+// R at [(2R-1)^3, (2R+1)^3)), else decoded from the index.
+__device__ __forceinline__ void shell_offset(const BatchBuffers &b, int R, int e, int &dx, int &dy,
+                                             int &dz) {
+  if (R <= b.shell_rmax) {
+    const int base = (2 * R - 1) * (2 * R - 1) * (2 * R - 1);
+    const uint32_t w = b.shell_table[base + e];
+    dx = int(w & 1023u) - 512;
+    dy = int((w >> 10) & 1023u) - 512;
+    dz = int((w >> 20) & 1023u) - 512;
+    return;
+  }
+  const int w = 2 * R + 1, v = 2 * R - 1;
+  const int f1 = 2 * w * w, f2 = 2 * v * w;
+  if (e < f1) {
+    const int side = e / (w * w), r = e - side * w * w;
+    dx = side ? R : -R;
+    dy = r / w - R;
+    dz = r % w - R;
+  } else if (e < f1 + f2) {
+    const int e2 = e - f1, side = e2 / (v * w), r = e2 - side * v * w;
+    dy = side ? R : -R;
+    dx = r / w - (R - 1);
+    dz = r % w - R;
+  } else {
+    const int e3 = e - f1 - f2, side = e3 / (v * v), r = e3 - side * v * v;
+    dz = side ? R : -R;
+    dx = r / v - (R - 1);
+    dy = r % v - (R - 1);
+  }
+}
+
+__device__ __forceinline__ double shfl_d(double v, int src) {
+  return __shfl_sync(kFull, v, src);
+}
+
+__device__ __forceinline__ bool lex_less(double d1, int i1, double d2, int i2) {
+  return d1 < d2 || (d1 == d2 && i1 < i2);
+}
+
+// The warp's sorted k-list.
+template <int KPL>
+struct TeamList {
+  double d[KPL];
+  int j[KPL];
+};
+
+// Inserts (x, jx) (same on every lane) into the sorted list; returns the
+// value pushed to position k (the evicted k-th entry) or +inf.
+template <int KPL>
+__device__ __forceinline__ double team_insert(TeamList<KPL> &L, int lane, int k, double x, int jx) {
+  int c = 0;
+#pragma unroll
+  for (int s = 0; s < KPL; ++s) c += lex_less(L.d[s], L.j[s], x, jx) ? 1 : 0;
+  int P;
+  if (KPL == 1) {
+    P = __popc(__ballot_sync(kFull, c != 0));
+  } else {
+    P = c;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) P += __shfl_xor_sync(kFull, P, o);
+  }
+  // value at position k-1 before the shift: evicted when P < k
+  const double at_km1 = shfl_d(L.d[(k - 1) % KPL], (k - 1) / KPL);
+  const double up_d = shfl_d(L.d[KPL - 1], (lane + 31) & 31);
+  const int up_j = __shfl_sync(kFull, L.j[KPL - 1], (lane + 31) & 31);
+#pragma unroll
+  for (int s = KPL - 1; s >= 0; --s) {
+    const int pos = lane * KPL + s;
+    const double bd = s == 0 ? up_d : L.d[s - 1];
+    const int bj = s == 0 ? up_j : L.j[s - 1];
+    if (pos > P) {
+      L.d[s] = bd;
+      L.j[s] = bj;
+    } else if (pos == P) {
+      L.d[s] = x;
+      L.j[s] = jx;
+    }
+  }
+  return P < k ? at_km1 : x;
+}
+
+// Removes position q from the sorted list (entries above move down; the
+// last slot becomes +inf).
+template <int KPL>
+__device__ __forceinline__ void team_remove(TeamList<KPL> &L, int lane, int q) {
+  const double dn_d = shfl_d(L.d[0], (lane + 1) & 31);
+  const int dn_j = __shfl_sync(kFull, L.j[0], (lane + 1) & 31);
+#pragma unroll
+  for (int s = 0; s < KPL; ++s) {
+    const int pos = lane * KPL + s;
+    if (pos >= q) {
+      if (s + 1 < KPL) {
+        L.d[s] = L.d[s + 1];
+        L.j[s] = L.j[s + 1];
+      } else if (lane < 31) {
+        L.d[s] = dn_d;
+        L.j[s] = dn_j;
+      } else {
+        L.d[s] = pinf();
+        L.j[s] = 0x7fffffff;
+      }
+    }
+  }
+}
+
+// Bitonic sort of one (d, j) pair per lane, ascending by (d, j).
+__device__ __forceinline__ void warp_sort_pairs(double &d, int &j, int lane) {
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const double od = __shfl_xor_sync(kFull, d, stride);
+      const int oj = __shfl_xor_sync(kFull, j, stride);
+      const bool up = ((lane & size) == 0);
+      const bool lower = (lane & stride) == 0;
+      const bool other_less = lex_less(od, oj, d, j);
+      const bool take = (lower == up) ? other_less : !other_less && !(od == d && oj == j);
+      if (take) {
+        d = od;
+        j = oj;
+      }
+    }
+  }
+}
+
+// Merges the (already filtered) candidates of a round, one per lane
+// (+inf where none), into a KPL == 1 list. Returns, per lane, the smallest
+// value that left the first k positions (or +inf).
+__device__ __forceinline__ double team_merge32(TeamList<1> &L, int lane, int k, double cd, int cj) {
+  warp_sort_pairs(cd, cj, lane);
+  // reversed candidates against the ascending list: the lane-wise minima
+  // are the 32 smallest of the union, as a bitonic sequence
+  const double rd = __shfl_sync(kFull, cd, 31 - lane);
+  const int rj = __shfl_sync(kFull, cj, 31 - lane);
+  double out_d;
+  if (lex_less(rd, rj, L.d[0], L.j[0])) {
+    out_d = L.d[0];
+    L.d[0] = rd;
+    L.j[0] = rj;
+  } else {
+    out_d = rd;
+  }
+  // bitonic merge (ascending)
+#pragma unroll
+  for (int stride = 16; stride > 0; stride >>= 1) {
+    const double od = __shfl_xor_sync(kFull, L.d[0], stride);
+    const int oj = __shfl_xor_sync(kFull, L.j[0], stride);
+    const bool lower = (lane & stride) == 0;
+    const bool other_less = lex_less(od, oj, L.d[0], L.j[0]);
+    if (lower ? other_less : (!other_less && !(od == L.d[0] && oj == L.j[0]))) {
+      L.d[0] = od;
+      L.j[0] = oj;
+    }
+  }
+  // the lane-wise maxima left the list; so did positions >= k
+  double gone = out_d;
+  if (lane >= k) gone = fmin(gone, L.d[0]);
+  return gone;
+}
+
+template <int MODE, int KPL>
+__device__ void team_source(const BatchBuffers &b, long long p, int lane, LocalCounters &cnt) {
+  const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
+  const FrameDesc &fr = b.frames[f];
+  if (b.frame_flags[f] & kFrameNaN) {
+    if (lane == 0) {
+      push_replay(b, p);
+      ++cnt.v[kCntReplays];
+    }
+    return;
+  }
+  const int k = fr.k;
+  const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
+  const uint32_t lc = b.scell[p];
+  const int ix = int(lc % uint32_t(nx));
+  const int iy = int((lc / uint32_t(nx)) % uint32_t(ny));
+  const int iz = int(lc / (uint32_t(nx) * uint32_t(ny)));
+  const double px = b.sx[p], py = b.sy[p], pz = b.sz[p];
+  const long long cb = fr.cell_base;
+  const int max_reach = fr.max_reach;
+  const double cell_min = fr.cell_min;
+
+  float plx = 0.f, ply = 0.f, plz = 0.f, fa = 0.f, fb = 0.f, fc = 0.f, lam = 0.f;
+  if (MODE != kModePlainF64) {
+    const float4 r = b.rec[p];
+    plx = r.x;
+    ply = r.y;
+    plz = r.z;
+    fa = fr.nhinv[0] * plx + fr.nhinv[1] * ply + fr.nhinv[2] * plz;
+    fb = fr.nhinv[3] * plx + fr.nhinv[4] * ply + fr.nhinv[5] * plz;
+    fc = fr.nhinv[6] * plx + fr.nhinv[7] * ply + fr.nhinv[8] * plz;
+    lam = float(fr.lam_min) * 0.99f;
+  }
+  int Rp = 0;
+  if (MODE == kModeLearned && b.proposal) {
+    Rp = b.proposal[p];
+    if (Rp > max_reach) Rp = max_reach;
+  }
+
+  TeamList<KPL> L;
+  int filled = 0;
+  double rej = pinf();
+  int stopped = 0;
+  for (;;) {  // one pass, plus a restart when a learned proposal was short
+#pragma unroll
+    for (int s = 0; s < KPL; ++s) {
+      L.d[s] = pinf();
+      L.j[s] = 0x7fffffff;
+    }
+    filled = 0;
+    rej = pinf();
+    stopped = 0;
+    const double filt = Rp > 0 ? stop_bound(Rp, cell_min) : pinf();
+    double theta = filt;
+    for (int R = 1; R <= max_reach; ++R) {
+      const bool dedupe = 2 * R + 1 > nx || 2 * R + 1 > ny || 2 * R + 1 > nz;
+      if (lane == 0) ++cnt.v[kCntShells];
+      const double beta = MODE != kModePlainF64 ? fp32_beta(fr, R) : 0.0;
+      float thr = MODE != kModePlainF64 ? fp32_threshold(theta, beta) : 0.f;
+      const int E = R == 1 ? 27 : 24 * R * R + 2;
+      for (int e0 = 0; e0 < E; e0 += 32) {
+        const int e = e0 + lane;
+        int a0 = 0, nc = 0, wa = 0, wb = 0, wc = 0;
+        float Dx = 0.f, Dy = 0.f, Dz = 0.f;
+        if (e < E) {
+          int dx, dy, dz;
+          shell_offset(b, R, e, dx, dy, dz);
+          int cx, cy, cz;
+          wrap_axis(ix + dx, nx, cx, wa);
+          wrap_axis(iy + dy, ny, cy, wb);
+          wrap_axis(iz + dz, nz, cz, wc);
+          const long long c = cb + ((long long)cz * ny + cy) * (long long)nx + cx;
+          a0 = int(b.off[c]);
+          nc = int(b.off[c + 1]) - a0;
+          if (MODE != kModePlainF64 && nc > 0) {
+            const float ga = dx > 0 ? dx - fa : (dx < 0 ? fa + float(-dx - 1) : 0.f);
+            const float gb = dy > 0 ? dy - fb : (dy < 0 ? fb + float(-dy - 1) : 0.f);
+            const float gc = dz > 0 ? dz - fc : (dz < 0 ? fc + float(-dz - 1) : 0.f);
+            const float ga0 = fmaxf(ga, 0.f), gb0 = fmaxf(gb, 0.f), gc0 = fmaxf(gc, 0.f);
+            if (lam * (ga0 * ga0 + gb0 * gb0 + gc0 * gc0) > thr) {
+              ++cnt.v[kCntPruned];
+              nc = 0;
+            } else {
+              const float fdx = float(dx), fdy = float(dy), fdz = float(dz);
+              Dx = fdx * fr.ev[0] + fdy * fr.ev[3] + fdz * fr.ev[6];
+              Dy = fdx * fr.ev[1] + fdy * fr.ev[4] + fdz * fr.ev[7];
+              Dz = fdx * fr.ev[2] + fdy * fr.ev[5] + fdz * fr.ev[8];
+            }
+          }
+        }
+        // candidates of this chunk: inclusive scan of the cell counts
+        int incl = nc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(kFull, incl, o);
+          if (lane >= o) incl += y;
+        }
+        const int tot = __shfl_sync(kFull, incl, 31);
+        const int excl = incl - nc;
+        for (int g0 = 0; g0 < tot; g0 += 32) {
+          const int g = g0 + lane;
+          // owner lane: number of lanes whose inclusive count is <= g
+          int owner = 0;
+#pragma unroll
+          for (int step = 16; step > 0; step >>= 1) {
+            const int v = __shfl_sync(kFull, incl, owner + step - 1);
+            if (v <= g) owner += step;
+          }
+          owner &= 31;
+          const int oa0 = __shfl_sync(kFull, a0, owner);
+          const int oex = __shfl_sync(kFull, excl, owner);
+          const int owa = __shfl_sync(kFull, wa, owner);
+          const int owb = __shfl_sync(kFull, wb, owner);
+          const int owc = __shfl_sync(kFull, wc, owner);
+          const float oDx = __shfl_sync(kFull, Dx, owner);
+          const float oDy = __shfl_sync(kFull, Dy, owner);
+          const float oDz = __shfl_sync(kFull, Dz, owner);
+          const long long t = (long long)oa0 + (g - oex);
+          bool pass = g < tot && t != p;
+          int j = 0;
+          if (pass) {
+            ++cnt.v[kCntPairs];
+            if (MODE != kModePlainF64) {
+              const float4 q = b.rec[t];
+              const float ex = (q.x - plx) + oDx;
+              const float ey = (q.y - ply) + oDy;
+              const float ez = (q.z - plz) + oDz;
+              const float d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+              pass = !(d32 > thr);
+              j = __float_as_int(q.w);
+            } else {
+              j = b.sidx[t];
+            }
+          }
+          const unsigned pm = __ballot_sync(kFull, pass);
+          if (pm == 0) continue;
+          double d = pinf();
+          if (pass) {
+            if (MODE != kModePlainF64) ++cnt.v[kCntRerank];
+            double shx, shy, shz;
+            lattice_shift(fr, owa, owb, owc, shx, shy, shz);
+            d = dist2_shifted(px, py, pz, b.sx[t], b.sy[t], b.sz[t], shx, shy, shz);
+            if (MODE == kModeLearned && d > filt) pass = false;  // beyond the proposed bound
+          }
+          // insertion candidates: below theta, or anything while the list fills
+          bool ins = pass && (filled < k || d < theta);
+          if (pass && !ins) rej = fmin(rej, d);
+          unsigned im = __ballot_sync(kFull, ins);
+          if (im == 0) continue;
+          if (KPL == 1 && !dedupe && __popc(im) >= 6) {
+            const int added = __popc(im);
+            const double gone = team_merge32(reinterpret_cast<TeamList<1> &>(L), lane, k,
+                                             ins ? d : pinf(), ins ? j : 0x7fffffff);
+            if (filled + added > k) rej = fmin(rej, gone);
+            filled = min(filled + added, k);
+            cnt.v[kCntInserts] += lane == 0 ? added : 0;
+          } else {
+            while (im) {
+              const int src = __ffs(im) - 1;
+              im &= im - 1;
+              const double x = shfl_d(d, src);
+              const int jx = __shfl_sync(kFull, j, src);
+              if (filled >= k && !(x < theta)) {  // theta fell below it in this round
+                rej = fmin(rej, x);
+                continue;
+              }
+              if (dedupe) {
+                // an index already listed keeps its smaller distance
+                bool has = false;
+                int qpos = 0;
+#pragma unroll
+                for (int s = 0; s < KPL; ++s) {
+                  const int pos = lane * KPL + s;
+                  const bool hit = pos < filled && L.j[s] == jx;
+                  const unsigned hm = __ballot_sync(kFull, hit);
+                  if (hm) {
+                    has = true;
+                    qpos = (__ffs(hm) - 1) * KPL + s;
+                  }
+                }
+                if (has) {
+                  const double old = shfl_d(L.d[qpos % KPL], qpos / KPL);
+                  if (!(x < old)) continue;
+                  team_remove(L, lane, qpos);
+                  --filled;
+                }
+              }
+              const double gone = team_insert(L, lane, k, x, jx);
+              if (filled >= k) rej = fmin(rej, gone);
+              filled = min(filled + 1, k);
+              if (lane == 0) ++cnt.v[kCntInserts];
+              if (filled >= k) {
+                theta = fmin(shfl_d(L.d[(k - 1) % KPL], (k - 1) / KPL), filt);
+                if (MODE != kModePlainF64) thr = fp32_threshold(theta, beta);
+              }
+            }
+            continue;
+          }
+          if (filled >= k) {
+            theta = fmin(shfl_d(L.d[(k - 1) % KPL], (k - 1) / KPL), filt);
+            if (MODE != kModePlainF64) thr = fp32_threshold(theta, beta);
+          }
+        }
+      }
+      if (filled >= k && shfl_d(L.d[(k - 1) % KPL], (k - 1) / KPL) <= stop_bound(R, cell_min)) {
+        stopped = R;
+        break;
+      }
+      if (MODE == kModeLearned && Rp > 0 && R == Rp) break;  // proposal too short
+    }
+    if (MODE == kModeLearned && Rp > 0) {
+      if (stopped == 0) {
+        if (lane == 0) {
+          ++cnt.v[kCntPropUnder];
+          cnt.v[kCntRevisit] += Rp;
+        }
+        Rp = 0;
+        continue;
+      }
+      if (lane == 0) ++cnt.v[stopped < Rp ? kCntPropOver : kCntPropExact];
+    }
+    break;
+  }
+  if (b.stop_log && lane == 0)
+    b.stop_log[p] = int8_t(stopped > 0 ? (stopped < 127 ? stopped : 127) : 0);
+  // tie across the k-th slot: the reference's push order decides
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) rej = fmin(rej, __shfl_xor_sync(kFull, rej, o));
+  if (filled >= k) {
+    const double vk = shfl_d(L.d[(k - 1) % KPL], (k - 1) / KPL);
+    if (!(rej > vk)) {
+      if (lane == 0) {
+        push_replay(b, p);
+        ++cnt.v[kCntReplays];
+      }
+      return;
+    }
+  }
+  const int i = b.sidx[p];
+  int *row = b.out_nn + fr.out_base + (long long)i * k;
+  double *drow = b.out_d2 ? b.out_d2 + fr.out_base + (long long)i * k : nullptr;
+#pragma unroll
+  for (int s = 0; s < KPL; ++s) {
+    const int pos = lane * KPL + s;
+    if (pos < k) {
+      const bool ok = pos < filled;
+      row[pos] = ok ? L.j[s] : -1;
+      if (drow) drow[pos] = ok ? L.d[s] : qnan();
+    }
+  }
+}
+
+template <int MODE, int KPL>
+__global__ void __launch_bounds__(256, 2) k_team_walk(BatchBuffers b) {
+  const long long total = b.off[b.ncells];
+  const int lane = threadIdx.x & 31;
+  LocalCounters cnt;
+  constexpr int kGrab = 4;  // sources per work-queue grab (consecutive, share candidates)
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(b.work, uint32_t(kGrab));
+    base = __shfl_sync(kFull, base, 0);
+    if ((long long)base >= total) break;
+    for (int q = 0; q < kGrab; ++q) {
+      const long long p = (long long)base + q;
+      if (p >= total) break;
+      team_source<MODE, KPL>(b, p, lane, cnt);
+    }
+  }
+  flush_counters(b, cnt);
+}
+
 int sm_count() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   return sms;
+}
+
+template <int MODE, int KPL>
+cudaError_t launch_team(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_team_walk<MODE, KPL>, 256, 0);
+  if (per_sm < 1) per_sm = 1;
+  const int grid = w.grid > 0 ? w.grid : sm_count() * per_sm;
+  k_team_walk<MODE, KPL><<<grid, 256, 0, s>>>(b);
+  return cudaGetLastError();
+}
+
+template <int MODE>
+cudaError_t launch_team_k(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
+  if (b.kmax <= 32) return launch_team<MODE, 1>(b, w, s);
+  if (b.kmax <= 64) return launch_team<MODE, 2>(b, w, s);
+  if (b.kmax <= 128) return launch_team<MODE, 4>(b, w, s);
+  return launch_team<MODE, 8>(b, w, s);
 }
 
 template <int MODE, int BLOCK>
@@ -558,10 +1023,18 @@ int walk_max_block(int mode, int kmax) {
 }
 
 cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
+  if (w.mode == kModeReplayAll) {
+    k_queue_all<<<sm_count() * 4, 256, 0, s>>>(b);
+    return cudaGetLastError();
+  }
+  if (w.tpp == 32 && b.kmax <= 256) {
+    switch (w.mode) {
+      case kModeFastF32: return launch_team_k<kModeFastF32>(b, w, s);
+      case kModeLearned: return launch_team_k<kModeLearned>(b, w, s);
+      default: return launch_team_k<kModePlainF64>(b, w, s);
+    }
+  }
   switch (w.mode) {
-    case kModeReplayAll:
-      k_queue_all<<<sm_count() * 4, 256, 0, s>>>(b);
-      return cudaGetLastError();
     case kModeFastF32: return launch_block<kModeFastF32>(b, w, s);
     case kModeLearned: return launch_block<kModeLearned>(b, w, s);
     default: return launch_block<kModePlainF64>(b, w, s);
@@ -574,6 +1047,33 @@ cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s) {
   const int grid = (b.replay_threads + block - 1) / block;
   k_replay<<<grid, block, 0, s>>>(b);
   return cudaGetLastError();
+}
+
+}  // namespace lc
+
+namespace lc {
+
+// Offsets of shells 1..rmax, each shell sorted near-first by |d|^2 in bin
+// units (ties by lexicographic order). Shell R occupies entries
+// [(2R-1)^3, (2R+1)^3); the walk's result does not depend on this order.
+void build_shell_table(int rmax, uint32_t *out) {
+  size_t o = 0;
+  for (int R = 1; R <= rmax; ++R) {
+    struct Off {
+      int d2, dx, dy, dz;
+    };
+    std::vector<Off> v;
+    for (int dx = -R; dx <= R; ++dx)
+      for (int dy = -R; dy <= R; ++dy)
+        for (int dz = -R; dz <= R; ++dz) {
+          const int m = std::max(std::abs(dx), std::max(std::abs(dy), std::abs(dz)));
+          if (m != R && !(R == 1 && m == 0)) continue;
+          v.push_back({dx * dx + dy * dy + dz * dz, dx, dy, dz});
+        }
+    std::stable_sort(v.begin(), v.end(), [](const Off &a, const Off &b) { return a.d2 < b.d2; });
+    for (const Off &x : v)
+      out[o++] = uint32_t(x.dx + 512) | (uint32_t(x.dy + 512) << 10) | (uint32_t(x.dz + 512) << 20);
+  }
 }
 
 }  // namespace lc

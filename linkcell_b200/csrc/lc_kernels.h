@@ -48,6 +48,8 @@ struct BatchBuffers {
   long long *counters = nullptr; // walk statistics (see WalkCounters)
   const int8_t *proposal = nullptr;  // learned walk: proposed shell per sorted source (0: none)
   int8_t *stop_log = nullptr;        // optional: settled shell per sorted source (training)
+  const uint32_t *shell_table = nullptr;  // near-first shell offsets, shells 1..shell_rmax
+  int shell_rmax = 0;
 };
 
 // Walk statistics accumulated on the device (counters[...]).
@@ -64,6 +66,8 @@ enum WalkCounters : int {
   kCntRevisit = 9,    // shells walked again after a short proposal
   kNumCounters = 16
 };
+
+constexpr int kShellTableRmax = 16;
 
 constexpr int kScanBlock = 256;
 constexpr int kScanItems = 8;
@@ -88,6 +92,7 @@ enum WalkMode : int {
 
 struct WalkLaunch {
   int mode = kModePlainF64;
+  int tpp = 1;      // threads per source: 1 (heap in shared memory) or 32 (warp team)
   int block = 128;
   int grid = 0;
   int kmax = 32;
@@ -98,6 +103,8 @@ struct WalkLaunch {
 cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s);
 cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s);
 size_t walk_smem_bytes(int mode, int block, int kmax);
+// Near-first shell-offset table for shells 1..rmax ((2 rmax + 1)^3 entries).
+void build_shell_table(int rmax, uint32_t *out);
 int walk_max_block(int mode, int kmax);
 cudaError_t walk_prepare(int mode, int kmax, int block);  // sets the dynamic smem attribute
 

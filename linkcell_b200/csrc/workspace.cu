@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <vector>
 
 namespace lc {
 
@@ -179,6 +180,10 @@ WorkspaceImpl::WorkspaceImpl() {
     const int v = std::atoi(m);
     if (v >= 0 && v <= 3) opts.mode = v;
   }
+  if (const char *t = std::getenv("LINKCELL_TPP")) {
+    const int v = std::atoi(t);
+    if (v == 1 || v == 32) opts.tpp = v;
+  }
   if (const char *b = std::getenv("LINKCELL_BLOCK")) {
     const int v = std::atoi(b);
     if (v == 32 || v == 64 || v == 128 || v == 256) opts.block = v;
@@ -248,7 +253,8 @@ void WorkspaceImpl::release_all() {
   rel(sidx_); rel(replay_list_); rel(replay_i_); rel(scell_); rel(sx_); rel(sy_); rel(sz_);
   rel(replay_d_); rel(rec_); rel(frames_); rel(counters_); rel(h_xyz_); rel(h_d2_);
   rel(h_mask_); rel(h_nn_); rel(active_); rel(proposal_); rel(cell_prop_); rel(stop_log_);
-  rel(model_);
+  rel(model_); rel(shell_table_);
+  shell_table_ready_ = false;
 }
 
 #define LC_TRY(expr)                        \
@@ -302,8 +308,21 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   LC_TRY(grow(frames_, size_t(nf)));
   LC_TRY(grow(counters_, size_t(kNumCounters)));
 
+  if (!shell_table_ready_) {
+    const int rmax = kShellTableRmax;
+    const size_t entries = size_t(2 * rmax + 1) * (2 * rmax + 1) * (2 * rmax + 1);
+    std::vector<uint32_t> h(entries);
+    build_shell_table(rmax, h.data());
+    LC_TRY(grow(shell_table_, entries));
+    LC_TRY(cudaMemcpyAsync(shell_table_.p, h.data(), entries * sizeof(uint32_t),
+                           cudaMemcpyHostToDevice, s));
+    LC_TRY(cudaStreamSynchronize(s));
+    shell_table_ready_ = true;
+  }
+
   WalkLaunch wl;
   wl.mode = opts.mode;
+  wl.tpp = opts.tpp;
   wl.prune = opts.prune;
   wl.kmax = kmax;
   // The shared-memory heap walk covers k <= 256; larger k runs the exact
@@ -366,6 +385,8 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   b.replay_threads = replay_threads;
   b.kmax = kmax;
   b.counters = counters_.p;
+  b.shell_table = shell_table_.p;
+  b.shell_rmax = kShellTableRmax;
 
   if (collect_stats) LC_TRY(cudaEventRecord(ev_[0], s));
   LC_TRY(launch_fold_bin(b, s));

@@ -44,6 +44,7 @@ Code plan_frame(const double *rows, const double *origin, double cell_hint, int 
 // Options that pick the walk.
 struct WalkOptions {
   int mode = kModePlainF64;
+  int tpp = 32;    // threads per source: 32 (warp team) or 1 (one thread, heap in shared memory)
   int block = 0;   // 0: autotune / default
   int prune = 1;
   int fixed_proposal = 0;  // learned walk: > 0 proposes this shell for every source
@@ -121,6 +122,8 @@ class WorkspaceImpl {
   Buf<long long> counters_;
   Buf<int8_t> proposal_, cell_prop_, stop_log_;
   Buf<float> model_;
+  Buf<uint32_t> shell_table_;
+  bool shell_table_ready_ = false;
   bool has_model_ = false;
   float tau_ = 0.9f;
   // host-pointer staging

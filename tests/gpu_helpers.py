@@ -58,6 +58,9 @@ class DeviceRunner:
     def set_mode(self, mode):
         assert self.L.lc_gpu_set_mode(self.ws, mode) == 0
 
+    def set_tpp(self, tpp):
+        assert self.L.lc_gpu_set_tpp(self.ws, tpp) == 0
+
     def set_proposal(self, shell):
         assert self.L.lc_gpu_set_proposal(self.ws, shell) == 0
 

@@ -17,9 +17,11 @@ HEX = [[10.0, 0.0, 0.0], [5.0, 8.660254037844386, 0.0], [0.0, 0.0, 10.0]]
 TRI = [[10.0, 0.0, 0.0], [3.0, 9.0, 0.0], [1.0, 2.0, 8.0]]
 
 
-@pytest.fixture(scope="module")
-def runner(gpu):
+@pytest.fixture(scope="module", params=[32, 1], ids=["team", "thread"])
+def runner(gpu, request):
+    """Both walk designs: a warp per source and a thread per source."""
     r = DeviceRunner()
+    r.set_tpp(request.param)
     yield r
     r.close()
 
