@@ -524,12 +524,13 @@ __global__ void k_queue_all(BatchBuffers b) {
 // lane * KPL + s. Control flow is uniform across the warp; only the FP32
 // test, the exact recompute and the insertions are predicated.
 
-// Offset e of shell R: the near-first table for R <= rmax (entries of shell
-// R at [(2R-1)^3, (2R+1)^3)), else decoded from the index.
+// Offset e of shell R: the near-first table for R <= rmax (shell 1, the
+// whole 3x3x3 cube, at [0, 27); shell R > 1 at [(2R-1)^3, (2R+1)^3)), else
+// decoded from the index.
 __device__ __forceinline__ void shell_offset(const BatchBuffers &b, int R, int e, int &dx, int &dy,
                                              int &dz) {
   if (R <= b.shell_rmax) {
-    const int base = (2 * R - 1) * (2 * R - 1) * (2 * R - 1);
+    const int base = R == 1 ? 0 : (2 * R - 1) * (2 * R - 1) * (2 * R - 1);
     const uint32_t w = b.shell_table[base + e];
     dx = int(w & 1023u) - 512;
     dy = int((w >> 10) & 1023u) - 512;
@@ -1054,8 +1055,9 @@ cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s) {
 namespace lc {
 
 // Offsets of shells 1..rmax, each shell sorted near-first by |d|^2 in bin
-// units (ties by lexicographic order). Shell R occupies entries
-// [(2R-1)^3, (2R+1)^3); the walk's result does not depend on this order.
+// units (ties by lexicographic order). Shell 1 (the whole 3x3x3 cube)
+// occupies [0, 27), shell R > 1 [(2R-1)^3, (2R+1)^3); the walk's result
+// does not depend on this order.
 void build_shell_table(int rmax, uint32_t *out) {
   size_t o = 0;
   for (int R = 1; R <= rmax; ++R) {
