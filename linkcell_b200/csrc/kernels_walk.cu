@@ -958,6 +958,395 @@ __global__ void __launch_bounds__(256, 2) k_team_walk(BatchBuffers b) {
   flush_counters(b, cnt);
 }
 
+// ------------------------------------------------------------------------
+// Cube walk of the learned mode: one warp per source opens the proposed
+// cube (shells 1..R_p) in a single pass and selects instead of inserting.
+//
+//  1. Gather: every candidate of the cube whose cell is not pruned and whose
+//     FP32 distance passes the filter at B(R_p) = (R_p cell_min)^2 goes to a
+//     per-warp shared-memory buffer (FP32 distance, sorted position, shell,
+//     wrap counts).
+//  2. Stop reach: the reference stops at the first R with at least k
+//     candidates of shells <= R within B(R). Each candidate counts from
+//     reach max(shell, b(d)), b(d) = the first R with d <= B(R); b is exact
+//     (an FP64 recompute decides whenever d32 lies within the error band of
+//     a bound). No R <= R_p qualifies: the proposal was short, the source
+//     takes the incremental walk instead.
+//  3. Select: a 32-bucket histogram (equal volume in d^1.5) over the
+//     candidates of shells <= R* locates the k-th FP32 value; S = every such
+//     candidate with d32 <= T + 2 band(T), T = the largest d32 of the
+//     buckets up to the k-th, holds the k smallest exact distances and every
+//     value tied with the k-th, and nothing else can tie (with the FP32
+//     error band(x) = 8u x + beta, any candidate above T + 3 band(T) has an
+//     exact distance above T + band(T), which bounds the k-th value).
+//  4. S is recomputed in exact FP64, bitonic-sorted by (d2, index), and its
+//     first k are the row; a tie across the k-th slot goes to the literal
+//     replay.
+// Any proposal gives the reference result; a cube that overflows the
+// buffer, a short proposal, a cube that wraps the box, or an S larger than
+// the sort also fall back to the incremental walk.
+constexpr int kSelectCap = 256;     // candidates per warp buffer (KPL == 1)
+constexpr int kSelectWarps = 8;     // warps per block
+
+template <int KPL>
+struct SelectShared {
+  float d[kSelectWarps][kSelectCap * KPL];
+  int t[kSelectWarps][kSelectCap * KPL];
+  uint32_t meta[kSelectWarps][kSelectCap * KPL];
+  int bucket[kSelectWarps][32];
+};
+
+__device__ __forceinline__ float band32(double theta, double beta) {
+  return __double2float_ru(theta * 8.0 * double(kU32) + beta);
+}
+
+// Bitonic sort of 2 * 32 (d, j) pairs held two per lane: element e = s * 32 + lane.
+__device__ __forceinline__ void warp_sort64(double (&d)[2], int (&j)[2], int lane) {
+#pragma unroll
+  for (int size = 2; size <= 64; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride == 32) {
+        // both partners in this lane: element lane (s = 0) and lane + 32 (s = 1)
+        const bool up = true;  // size == 64: one ascending block
+        const bool swap = up ? lex_less(d[1], j[1], d[0], j[0]) : lex_less(d[0], j[0], d[1], j[1]);
+        if (swap) {
+          const double td = d[0];
+          const int tj = j[0];
+          d[0] = d[1];
+          j[0] = j[1];
+          d[1] = td;
+          j[1] = tj;
+        }
+        continue;
+      }
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const int e = s * 32 + lane;
+        const double od = __shfl_xor_sync(kFull, d[s], stride);
+        const int oj = __shfl_xor_sync(kFull, j[s], stride);
+        const bool up = ((e & size) == 0);
+        const bool lower = (e & stride) == 0;
+        const bool other_less = lex_less(od, oj, d[s], j[s]);
+        const bool take = (lower == up) ? other_less : !other_less && !(od == d[s] && oj == j[s]);
+        if (take) {
+          d[s] = od;
+          j[s] = oj;
+        }
+      }
+    }
+  }
+}
+
+template <int KPL>
+__device__ bool select_source(const BatchBuffers &b, long long p, int lane, int warp,
+                              LocalCounters &cnt, SelectShared<KPL> &sh) {
+  const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
+  const FrameDesc &fr = b.frames[f];
+  if (b.frame_flags[f] & kFrameNaN) return false;
+  int Rp = b.proposal ? b.proposal[p] : 0;
+  const int k = fr.k;
+  const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
+  if (Rp <= 0 || Rp > 8 || Rp > b.shell_rmax || Rp > fr.max_reach || k > 32) return false;
+  if (2 * Rp + 1 > nx || 2 * Rp + 1 > ny || 2 * Rp + 1 > nz) return false;  // cube wraps the box
+  constexpr int CAP = kSelectCap * KPL;
+  float *bd = sh.d[warp];
+  int *bt = sh.t[warp];
+  uint32_t *bm = sh.meta[warp];
+  int *bk = sh.bucket[warp];
+
+  const uint32_t lc = b.scell[p];
+  const int ix = int(lc % uint32_t(nx));
+  const int iy = int((lc / uint32_t(nx)) % uint32_t(ny));
+  const int iz = int(lc / (uint32_t(nx) * uint32_t(ny)));
+  const long long cb = fr.cell_base;
+  const double cell_min = fr.cell_min;
+  const float4 r = b.rec[p];
+  const float plx = r.x, ply = r.y, plz = r.z;
+  const float fa = fr.nhinv[0] * plx + fr.nhinv[1] * ply + fr.nhinv[2] * plz;
+  const float fb = fr.nhinv[3] * plx + fr.nhinv[4] * ply + fr.nhinv[5] * plz;
+  const float fc = fr.nhinv[6] * plx + fr.nhinv[7] * ply + fr.nhinv[8] * plz;
+  const float lam = float(fr.lam_min) * 0.99f;
+  const double beta = fp32_beta(fr, Rp);
+  const double Bp = stop_bound(Rp, cell_min);
+  const float thr = fp32_threshold(Bp, beta);
+
+  // 1. gather
+  const int E = (2 * Rp + 1) * (2 * Rp + 1) * (2 * Rp + 1);
+  int total = 0;
+  for (int e0 = 0; e0 < E; e0 += 32) {
+    const int e = e0 + lane;
+    int a0 = 0, nc = 0;
+    uint32_t meta = 0;
+    float Dx = 0.f, Dy = 0.f, Dz = 0.f;
+    if (e < E) {
+      const uint32_t w = b.shell_table[e];
+      const int dx = int(w & 1023u) - 512, dy = int((w >> 10) & 1023u) - 512,
+                dz = int((w >> 20) & 1023u) - 512;
+      int cx, cy, cz, wa, wb, wc;
+      wrap_axis(ix + dx, nx, cx, wa);
+      wrap_axis(iy + dy, ny, cy, wb);
+      wrap_axis(iz + dz, nz, cz, wc);
+      const long long c = cb + ((long long)cz * ny + cy) * (long long)nx + cx;
+      a0 = int(b.off[c]);
+      nc = int(b.off[c + 1]) - a0;
+      if (nc > 0) {
+        const float ga = dx > 0 ? dx - fa : (dx < 0 ? fa + float(-dx - 1) : 0.f);
+        const float gb = dy > 0 ? dy - fb : (dy < 0 ? fb + float(-dy - 1) : 0.f);
+        const float gc = dz > 0 ? dz - fc : (dz < 0 ? fc + float(-dz - 1) : 0.f);
+        const float ga0 = fmaxf(ga, 0.f), gb0 = fmaxf(gb, 0.f), gc0 = fmaxf(gc, 0.f);
+        if (lam * (ga0 * ga0 + gb0 * gb0 + gc0 * gc0) > thr) {
+          ++cnt.v[kCntPruned];
+          nc = 0;
+        } else {
+          const float fdx = float(dx), fdy = float(dy), fdz = float(dz);
+          Dx = fdx * fr.ev[0] + fdy * fr.ev[3] + fdz * fr.ev[6];
+          Dy = fdx * fr.ev[1] + fdy * fr.ev[4] + fdz * fr.ev[7];
+          Dz = fdx * fr.ev[2] + fdy * fr.ev[5] + fdz * fr.ev[8];
+          const int s = max(1, max(abs(dx), max(abs(dy), abs(dz))));
+          meta = uint32_t(s) | (uint32_t(wa + 1) << 8) | (uint32_t(wb + 1) << 10) |
+                 (uint32_t(wc + 1) << 12);
+        }
+      }
+    }
+    int incl = nc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int tot = __shfl_sync(kFull, incl, 31);
+    if (total + tot > CAP) return false;  // cube too full for the buffer
+    const int excl = incl - nc;
+    for (int g0 = 0; g0 < tot; g0 += 32) {
+      const int g = g0 + lane;
+      int owner = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int v = __shfl_sync(kFull, incl, owner + step - 1);
+        if (v <= g) owner += step;
+      }
+      owner &= 31;
+      const int oa0 = __shfl_sync(kFull, a0, owner);
+      const int oex = __shfl_sync(kFull, excl, owner);
+      const uint32_t om = __shfl_sync(kFull, meta, owner);
+      const float oDx = __shfl_sync(kFull, Dx, owner);
+      const float oDy = __shfl_sync(kFull, Dy, owner);
+      const float oDz = __shfl_sync(kFull, Dz, owner);
+      if (g < tot) {
+        const int t = oa0 + (g - oex);
+        float d32 = __int_as_float(0x7f800000);
+        if ((long long)t != p) {
+          ++cnt.v[kCntPairs];
+          const float4 q = b.rec[t];
+          const float ex = (q.x - plx) + oDx;
+          const float ey = (q.y - ply) + oDy;
+          const float ez = (q.z - plz) + oDz;
+          d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+          if (d32 > thr) d32 = __int_as_float(0x7f800000);  // beyond the proposed bound
+        }
+        bd[total + g] = d32;
+        bt[total + g] = t;
+        bm[total + g] = om;
+      }
+    }
+    total += tot;
+  }
+  __syncwarp();
+
+  const double px = b.sx[p], py = b.sy[p], pz = b.sz[p];
+  auto exact = [&](int i) -> double {
+    const int t = bt[i];
+    const uint32_t m = bm[i];
+    double shx, shy, shz;
+    lattice_shift(fr, int((m >> 8) & 3u) - 1, int((m >> 10) & 3u) - 1, int((m >> 12) & 3u) - 1, shx,
+                  shy, shz);
+    return dist2_shifted(px, py, pz, b.sx[t], b.sy[t], b.sz[t], shx, shy, shz);
+  };
+
+  // 2. stop reach: count[R] = #{key <= R}, key = max(shell, b(d))
+  int key_cnt[9];
+#pragma unroll
+  for (int R = 0; R < 9; ++R) key_cnt[R] = 0;
+  for (int i = lane; i < total; i += 32) {
+    const float d32 = bd[i];
+    if (!(d32 < __int_as_float(0x7f800000))) continue;
+    const int s = int(bm[i] & 255u);
+    int bR = Rp + 1;
+    double dex = -1.0;
+    for (int R = 1; R <= Rp; ++R) {
+      const double BR = stop_bound(R, cell_min);
+      const float band = band32(BR, beta);
+      const float hi = __double2float_ru(BR) + 2.f * band;
+      const float lo = __double2float_rd(BR) - band;
+      bool within;
+      if (d32 <= lo) {
+        within = true;
+      } else if (d32 > hi) {
+        within = false;
+      } else {
+        if (dex < 0.0) {
+          dex = exact(i);
+          ++cnt.v[kCntRerank];
+        }
+        within = dex <= BR;
+      }
+      if (within) {
+        bR = R;
+        break;
+      }
+    }
+    const int key = max(s, bR);
+#pragma unroll
+    for (int R = 1; R <= 8; ++R) key_cnt[R] += (key <= R) ? 1 : 0;
+  }
+  int Rs = 0;
+  for (int R = 1; R <= Rp; ++R) {
+    int c = key_cnt[R];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+    if (c >= k) {
+      Rs = R;
+      break;
+    }
+  }
+  if (Rs == 0) {  // proposal too short: the incremental walk takes over
+    if (lane == 0) {
+      ++cnt.v[kCntPropUnder];
+      cnt.v[kCntRevisit] += Rp;
+    }
+    return false;
+  }
+  if (lane == 0) ++cnt.v[Rs < Rp ? kCntPropOver : kCntPropExact];
+  if (lane == 0) cnt.v[kCntShells] += Rs;
+
+  // 3. select: histogram of shells <= R* over [0, B(R*)]
+  const double Bs = stop_bound(Rs, cell_min);
+  const float Bs32 = float(Bs);
+  const float Bs_hi = __double2float_ru(Bs) + 2.f * band32(Bs, beta);
+  bk[lane] = 0;
+  __syncwarp();
+  for (int i = lane; i < total; i += 32) {
+    const float d32 = bd[i];
+    if (int(bm[i] & 255u) > Rs || !(d32 <= Bs_hi)) continue;
+    const float x = fminf(d32 / Bs32, 1.f);
+    const int bucket = min(31, int(32.f * x * sqrtf(x)));
+    atomicAdd(&bk[bucket], 1);
+  }
+  __syncwarp();
+  int c = bk[lane];
+  int incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const unsigned reach = __ballot_sync(kFull, incl >= k);
+  if (!reach) return false;  // cannot happen: R* guarantees k candidates within B(R*)
+  const int bstar = __ffs(reach) - 1;
+  // T = the largest d32 in buckets <= bstar
+  float T = 0.f;
+  for (int i = lane; i < total; i += 32) {
+    const float d32 = bd[i];
+    if (int(bm[i] & 255u) > Rs || !(d32 <= Bs_hi)) continue;
+    const float x = fminf(d32 / Bs32, 1.f);
+    const int bucket = min(31, int(32.f * x * sqrtf(x)));
+    if (bucket <= bstar) T = fmaxf(T, d32);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) T = fmaxf(T, __shfl_xor_sync(kFull, T, o));
+  const float TS = T + 3.f * band32(double(T), beta);
+
+  // S = shells <= R*, d32 <= TS, compacted into two slots per lane
+  // (position q: lane q % 32, slot q / 32)
+  double sd[2] = {pinf(), pinf()};
+  int sj[2] = {0x7fffffff, 0x7fffffff};
+  int nS = 0;
+  for (int i0 = 0; i0 < total; i0 += 32) {
+    const int i = i0 + lane;
+    bool in = false;
+    if (i < total) in = int(bm[i] & 255u) <= Rs && bd[i] <= TS;
+    const unsigned m = __ballot_sync(kFull, in);
+    const int cntm = __popc(m);
+    if (cntm == 0) continue;
+    if (nS + cntm > 64) return false;  // S larger than the sort
+    double dd = 0.0;
+    int jj = 0;
+    if (in) {
+      dd = exact(i);
+      jj = b.sidx[bt[i]];
+    }
+    // this round fills positions nS .. nS + cntm - 1; lane L takes position
+    // nS + ((L - nS) & 31) from the source lane holding the r-th set bit
+    const int r = (lane - nS) & 31;
+    const int src = r < cntm ? int(__fns(m, 0, r + 1)) : lane;
+    const double vd = shfl_d(dd, src);
+    const int vj = __shfl_sync(kFull, jj, src);
+    if (r < cntm) {
+      const int q = nS + r;
+      if (q < 32) {
+        sd[0] = vd;
+        sj[0] = vj;
+      } else {
+        sd[1] = vd;
+        sj[1] = vj;
+      }
+    }
+    nS += cntm;
+  }
+  if (lane == 0) cnt.v[kCntRerank] += nS;
+  warp_sort64(sd, sj, lane);
+
+  // 4. tie across the k-th slot: (k-1)-th and k-th sorted values
+  const double vk = __shfl_sync(kFull, sd[(k - 1) >> 5], (k - 1) & 31);
+  const double vn = k < 64 ? __shfl_sync(kFull, sd[k >> 5], k & 31) : pinf();
+  if (nS > k && vn == vk) {
+    if (lane == 0) {
+      push_replay(b, p);
+      ++cnt.v[kCntReplays];
+    }
+    return true;
+  }
+  if (b.stop_log && lane == 0) b.stop_log[p] = int8_t(Rs);
+  const int i = b.sidx[p];
+  int *row = b.out_nn + fr.out_base + (long long)i * k;
+  double *drow = b.out_d2 ? b.out_d2 + fr.out_base + (long long)i * k : nullptr;
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const int pos = s * 32 + lane;
+    if (pos < k) {
+      row[pos] = sj[s];
+      if (drow) drow[pos] = sd[s];
+    }
+  }
+  if (lane == 0) cnt.v[kCntInserts] += k;
+  return true;
+}
+
+template <int KPL>
+__global__ void __launch_bounds__(kSelectWarps * 32, 2) k_select_walk(BatchBuffers b) {
+  __shared__ SelectShared<KPL> sh;
+  const long long total = b.off[b.ncells];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  LocalCounters cnt;
+  constexpr int kGrab = 4;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(b.work, uint32_t(kGrab));
+    base = __shfl_sync(kFull, base, 0);
+    if ((long long)base >= total) break;
+    for (int q = 0; q < kGrab; ++q) {
+      const long long p = (long long)base + q;
+      if (p >= total) break;
+      if (!select_source<KPL>(b, p, lane, warp, cnt, sh))
+        team_source<kModeFastF32, KPL>(b, p, lane, cnt);
+      __syncwarp();
+    }
+  }
+  flush_counters(b, cnt);
+}
+
 int sm_count() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -1026,6 +1415,14 @@ int walk_max_block(int mode, int kmax) {
 cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
   if (w.mode == kModeReplayAll) {
     k_queue_all<<<sm_count() * 4, 256, 0, s>>>(b);
+    return cudaGetLastError();
+  }
+  if (w.tpp == 32 && w.mode == kModeLearned && b.kmax <= 32 && b.proposal && b.shell_table) {
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk<1>, kSelectWarps * 32, 0);
+    if (per_sm < 1) per_sm = 1;
+    const int grid = w.grid > 0 ? w.grid : sm_count() * per_sm;
+    k_select_walk<1><<<grid, kSelectWarps * 32, 0, s>>>(b);
     return cudaGetLastError();
   }
   if (w.tpp == 32 && b.kmax <= 256) {
