@@ -106,6 +106,12 @@ int lc_gpu_set_model(lc_gpu_workspace *ws, const float *params, size_t n_params,
  * X and the class (settled shell - 1, capped at 7) into device y. Returns
  * the number of rows, or a negative value on error. */
 int lc_gpu_log_shells(lc_gpu_workspace *ws, int on);
+/* Proposed shells (0: none) the last learned search used for the sorted
+ * sources first, first + stride, ..., into host out (up to cap); returns
+ * the count, or a negative value on error. Rows line up with
+ * lc_gpu_training_rows of the same search. */
+long long lc_gpu_proposals(lc_gpu_workspace *ws, signed char *out, long long cap, long long stride,
+                           long long first);
 long long lc_gpu_training_rows(lc_gpu_workspace *ws, float *X, int *y, long long cap,
                                long long stride, long long first);
 

@@ -35,6 +35,7 @@ EXPORTS = (
     "lc_gpu_wait", "lc_gpu_alloc", "lc_gpu_free", "lc_gpu_fill_i32", "lc_gpu_memcpy",
     "lc_gpu_set_mode", "lc_gpu_get_mode", "lc_gpu_set_proposal", "lc_gpu_set_tpp", "lc_gpu_set_stream", "lc_gpu_stats",
     "lc_gpu_phase_times", "lc_gpu_set_model", "lc_gpu_log_shells", "lc_gpu_training_rows",
+    "lc_gpu_proposals",
     "lc_gpu_mlp_params", "lc_gpu_mlp_scratch_floats", "lc_gpu_mlp_forward", "lc_gpu_mlp_grad",
     "lc_gpu_mlp_adam",
     "lc_gpu_knearest_batch", "lc_gpu_knearest_noalloc",
@@ -94,6 +95,8 @@ def load():
     L.lc_gpu_log_shells.argtypes = [vp, i]
     L.lc_gpu_training_rows.argtypes = [vp, vp, vp, ll, ll, ll]
     L.lc_gpu_training_rows.restype = ll
+    L.lc_gpu_proposals.argtypes = [vp, vp, ll, ll, ll]
+    L.lc_gpu_proposals.restype = ll
     L.lc_gpu_mlp_params.restype = i
     L.lc_gpu_mlp_scratch_floats.argtypes = [i]
     L.lc_gpu_mlp_scratch_floats.restype = sz

@@ -512,6 +512,17 @@ long long lc_gpu_training_rows(lc_gpu_workspace *ws, float *X, int *y, long long
   return rows;
 }
 
+long long lc_gpu_proposals(lc_gpu_workspace *ws, signed char *out, long long cap, long long stride,
+                           long long first) {
+  if (!ws || !out) return -gpu_fail(Code::NullPointer);
+  long long rows = 0;
+  std::string detail;
+  const Code c =
+      ws->ws.proposals(reinterpret_cast<int8_t *>(out), cap, stride, first, rows, detail);
+  if (c != Code::Ok) return -gpu_fail_msg(detail.empty() ? lc::gpu_message(c) : detail);
+  return rows;
+}
+
 int lc_gpu_mlp_params(void) { return lc::kMlpParams; }
 
 size_t lc_gpu_mlp_scratch_floats(int batch) { return lc::MlpScratch::floats(batch); }

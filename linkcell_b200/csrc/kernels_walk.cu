@@ -1116,7 +1116,6 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, int 
       if (lane >= o) incl += y;
     }
     const int tot = __shfl_sync(kFull, incl, 31);
-    if (total + tot > CAP) return false;  // cube too full for the buffer
     const int excl = incl - nc;
     for (int g0 = 0; g0 < tot; g0 += 32) {
       const int g = g0 + lane;
@@ -1133,24 +1132,28 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, int 
       const float oDx = __shfl_sync(kFull, Dx, owner);
       const float oDy = __shfl_sync(kFull, Dy, owner);
       const float oDz = __shfl_sync(kFull, Dz, owner);
-      if (g < tot) {
-        const int t = oa0 + (g - oex);
-        float d32 = __int_as_float(0x7f800000);
-        if ((long long)t != p) {
-          ++cnt.v[kCntPairs];
-          const float4 q = b.rec[t];
-          const float ex = (q.x - plx) + oDx;
-          const float ey = (q.y - ply) + oDy;
-          const float ez = (q.z - plz) + oDz;
-          d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-          if (d32 > thr) d32 = __int_as_float(0x7f800000);  // beyond the proposed bound
-        }
-        bd[total + g] = d32;
-        bt[total + g] = t;
-        bm[total + g] = om;
+      const int t = oa0 + (g - oex);
+      bool keep = false;
+      float d32 = 0.f;
+      if (g < tot && (long long)t != p) {
+        ++cnt.v[kCntPairs];
+        const float4 q = b.rec[t];
+        const float ex = (q.x - plx) + oDx;
+        const float ey = (q.y - ply) + oDy;
+        const float ez = (q.z - plz) + oDz;
+        d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+        keep = !(d32 > thr);  // beyond the proposed bound: never in the row
       }
+      const unsigned km = __ballot_sync(kFull, keep);
+      if (total + __popc(km) > CAP) return false;  // too many candidates for the buffer
+      if (keep) {
+        const int pos = total + __popc(km & ((1u << lane) - 1u));
+        bd[pos] = d32;
+        bt[pos] = t;
+        bm[pos] = om;
+      }
+      total += __popc(km);
     }
-    total += tot;
   }
   __syncwarp();
 

@@ -8,9 +8,10 @@
 //   - forward (k_dense: tiled FP32 GEMM with bias and optional SiLU),
 //     softmax cross-entropy, backward (GEMMs for input and weight
 //     gradients, SiLU derivative), and Adam;
-//   - k_cell_proposal: inference per non-empty cell with the weights in
-//     shared memory, writing the proposed shell of every cell; the walk
-//     reads it for each source.
+//   - k_cell_proposal_tc: inference per non-empty cell on the tensor cores
+//     (mma.sync TF32, FP32 accumulation), writing the proposed shell of
+//     every cell (the smallest R with P(settled shell <= R) >= tau); the
+//     walk reads it for each source.
 //
 // Parameter layout (floats): W1[64][126] b1[64] W2[64][64] b2[64]
 // W3[8][64] b3[8].
@@ -190,92 +191,6 @@ __global__ void k_adam(float *__restrict__ p, const float *__restrict__ g, float
   p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
-// Inference per cell: the proposed shell is the smallest R with
-// P(settled shell <= R) >= tau. Weights live in shared memory.
-__global__ void __launch_bounds__(128) k_cell_proposal(const float *__restrict__ params,
-                                                       const FrameDesc *__restrict__ frames,
-                                                       int nframes, const uint32_t *__restrict__ off,
-                                                       long long ncells, float tau,
-                                                       int8_t *__restrict__ cell_prop) {
-  extern __shared__ float w[];
-  for (int t = threadIdx.x; t < kMlpParams; t += blockDim.x) w[t] = params[t];
-  __syncthreads();
-  const float *W1 = w, *b1 = W1 + kMlpHidden * kMlpIn;
-  const float *W2 = b1 + kMlpHidden, *b2 = W2 + kMlpHidden * kMlpHidden;
-  const float *W3 = b2 + kMlpHidden, *b3 = W3 + kMlpOut * kMlpHidden;
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncells;
-       c += (long long)gridDim.x * blockDim.x) {
-    if (off[c + 1] == off[c]) continue;  // no source here
-    int f = 0;
-    if (nframes > 1) {
-      int lo = 0, hi = nframes - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (frames[mid].cell_base <= c)
-          lo = mid;
-        else
-          hi = mid - 1;
-      }
-      f = lo;
-    }
-    const FrameDesc &fr = frames[f];
-    const uint32_t lc = uint32_t(c - fr.cell_base);
-    const int cx = int(lc % uint32_t(fr.nx));
-    const int cy = int((lc / uint32_t(fr.nx)) % uint32_t(fr.ny));
-    const int cz = int(lc / (uint32_t(fr.nx) * uint32_t(fr.ny)));
-    float h1[kMlpHidden];
-#pragma unroll
-    for (int u = 0; u < kMlpHidden; ++u) h1[u] = b1[u];
-    int t = 0;
-    for (int dx = -2; dx <= 2; ++dx) {
-      const int jx = rem_euclid(cx + dx, fr.nx);
-      for (int dy = -2; dy <= 2; ++dy) {
-        const int jy = rem_euclid(cy + dy, fr.ny);
-        for (int dz = -2; dz <= 2; ++dz, ++t) {
-          const int jz = rem_euclid(cz + dz, fr.nz);
-          const long long q = fr.cell_base + ((long long)jz * fr.ny + jy) * (long long)fr.nx + jx;
-          const float xv = log1pf(float(off[q + 1] - off[q]));
-          if (xv == 0.f) continue;
-#pragma unroll
-          for (int u = 0; u < kMlpHidden; ++u) h1[u] = fmaf(W1[u * kMlpIn + t], xv, h1[u]);
-        }
-      }
-    }
-    const float kf = float(fr.k) / 64.0f;
-#pragma unroll
-    for (int u = 0; u < kMlpHidden; ++u) h1[u] = silu(fmaf(W1[u * kMlpIn + 125], kf, h1[u]));
-    float z3[kMlpOut];
-#pragma unroll
-    for (int o = 0; o < kMlpOut; ++o) z3[o] = b3[o];
-    for (int u = 0; u < kMlpHidden; ++u) {
-      float z = b2[u];
-#pragma unroll
-      for (int v = 0; v < kMlpHidden; ++v) z = fmaf(W2[u * kMlpHidden + v], h1[v], z);
-      const float h2 = silu(z);
-#pragma unroll
-      for (int o = 0; o < kMlpOut; ++o) z3[o] = fmaf(W3[o * kMlpHidden + u], h2, z3[o]);
-    }
-    float m = z3[0];
-#pragma unroll
-    for (int o = 1; o < kMlpOut; ++o) m = fmaxf(m, z3[o]);
-    float s = 0.f;
-#pragma unroll
-    for (int o = 0; o < kMlpOut; ++o) {
-      z3[o] = __expf(z3[o] - m);
-      s += z3[o];
-    }
-    int prop = kMlpOut;
-    float cum = 0.f;
-#pragma unroll
-    for (int o = 0; o < kMlpOut; ++o) {
-      cum += z3[o] / s;
-      if (cum >= tau && prop == kMlpOut) prop = o + 1;
-    }
-    // the top class is "8 or more": propose nothing there
-    cell_prop[c] = int8_t(prop >= kMlpOut ? 0 : prop);
-  }
-}
-
 // proposal per sorted source = proposal of its cell
 __global__ void k_source_proposal(const FrameDesc *__restrict__ frames, int nframes,
                                   const uint32_t *__restrict__ off, long long ncells,
@@ -331,6 +246,245 @@ __global__ void k_training_rows(BatchBuffers b, const int8_t *__restrict__ stop_
     int R = stop_log[p];
     if (R <= 0 || R > kMlpOut) R = kMlpOut;
     y[r] = R - 1;
+  }
+}
+
+// ---------------------------------------------------------------------
+// Tensor-core inference: mma.sync m16n8k8 TF32 (FP32 accumulate). One warp
+// evaluates 16 cells at a time: layer 1 is [16 x 128] x [128 x 64] (126
+// features padded with zeros), layer 2 [16 x 64] x [64 x 64], layer 3
+// [16 x 64] x [64 x 8]. Features are gathered straight into the A
+// fragments; the hidden layer goes through shared memory to change from
+// the accumulator layout to the A-operand layout.
+constexpr int kW1Stride = 132;  // padded rows: conflict-free B-fragment loads
+constexpr int kW2Stride = 68;
+constexpr int kTcWarps = 4;
+
+struct TcShared {
+  float w1[kMlpHidden * kW1Stride];
+  float w2[kMlpHidden * kW2Stride];
+  float w3[kMlpOut * kW2Stride];
+  float b1[kMlpHidden], b2[kMlpHidden], b3[kMlpOut];
+  float h[kTcWarps][16 * kW2Stride];
+};
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Non-empty cells into a list (order does not matter).
+__global__ void k_list_cells(const uint32_t *__restrict__ off, long long ncells,
+                             uint32_t *__restrict__ list, uint32_t *__restrict__ count) {
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncells;
+       c += (long long)gridDim.x * blockDim.x) {
+    const bool has = off[c + 1] > off[c];
+    const unsigned m = __ballot_sync(0xffffffffu, has);
+    if (m == 0) continue;
+    const int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd(count, uint32_t(__popc(m)));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+    if (has) list[base + __popc(m & ((1u << lane) - 1u))] = uint32_t(c);
+  }
+}
+
+__global__ void __launch_bounds__(kTcWarps * 32) k_cell_proposal_tc(
+    const float *__restrict__ params, const FrameDesc *__restrict__ frames, int nframes,
+    const uint32_t *__restrict__ off, const uint32_t *__restrict__ list,
+    const uint32_t *__restrict__ list_count, float tau, int8_t *__restrict__ cell_prop) {
+  extern __shared__ float smem_raw[];
+  TcShared &sh = *reinterpret_cast<TcShared *>(smem_raw);
+  const float *W1 = params, *B1 = W1 + kMlpHidden * kMlpIn;
+  const float *W2 = B1 + kMlpHidden, *B2 = W2 + kMlpHidden * kMlpHidden;
+  const float *W3 = B2 + kMlpHidden, *B3 = W3 + kMlpOut * kMlpHidden;
+  for (int t = threadIdx.x; t < kMlpHidden * kW1Stride; t += blockDim.x) {
+    const int n = t / kW1Stride, kk = t % kW1Stride;
+    sh.w1[t] = kk < kMlpIn ? __uint_as_float(to_tf32(W1[n * kMlpIn + kk])) : 0.f;
+  }
+  for (int t = threadIdx.x; t < kMlpHidden * kW2Stride; t += blockDim.x) {
+    const int n = t / kW2Stride, kk = t % kW2Stride;
+    sh.w2[t] = kk < kMlpHidden ? __uint_as_float(to_tf32(W2[n * kMlpHidden + kk])) : 0.f;
+  }
+  for (int t = threadIdx.x; t < kMlpOut * kW2Stride; t += blockDim.x) {
+    const int n = t / kW2Stride, kk = t % kW2Stride;
+    sh.w3[t] = kk < kMlpHidden ? __uint_as_float(to_tf32(W3[n * kMlpHidden + kk])) : 0.f;
+  }
+  for (int t = threadIdx.x; t < kMlpHidden; t += blockDim.x) {
+    sh.b1[t] = B1[t];
+    sh.b2[t] = B2[t];
+  }
+  if (threadIdx.x < kMlpOut) sh.b3[threadIdx.x] = B3[threadIdx.x];
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, tig = lane & 3;
+  const uint32_t ncl = *list_count;
+  float *hbuf = sh.h[warp];
+  const long long tiles = (ncl + 15) / 16;
+  for (long long tile = (long long)blockIdx.x * kTcWarps + warp; tile < tiles;
+       tile += (long long)gridDim.x * kTcWarps) {
+    // the two cells (rows g and g + 8) whose features this lane gathers
+    int cxs[2], cys[2], czs[2];
+    const FrameDesc *frs[2];
+    bool valid[2];
+    long long cellid[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const long long row = tile * 16 + g + 8 * h;
+      valid[h] = row < ncl;
+      const long long c = valid[h] ? (long long)list[row] : 0;
+      cellid[h] = c;
+      int f = 0;
+      if (nframes > 1) {
+        int lo = 0, hi = nframes - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (frames[mid].cell_base <= c)
+            lo = mid;
+          else
+            hi = mid - 1;
+        }
+        f = lo;
+      }
+      frs[h] = &frames[f];
+      const uint32_t lc = uint32_t(c - frs[h]->cell_base);
+      cxs[h] = int(lc % uint32_t(frs[h]->nx));
+      cys[h] = int((lc / uint32_t(frs[h]->nx)) % uint32_t(frs[h]->ny));
+      czs[h] = int(lc / (uint32_t(frs[h]->nx) * uint32_t(frs[h]->ny)));
+    }
+    auto feature = [&](int h, int fi) -> float {
+      if (!valid[h]) return 0.f;
+      const FrameDesc &fr = *frs[h];
+      if (fi < 125) {
+        const int dx = fi / 25 - 2, dy = (fi / 5) % 5 - 2, dz = fi % 5 - 2;
+        const int jx = rem_euclid(cxs[h] + dx, fr.nx);
+        const int jy = rem_euclid(cys[h] + dy, fr.ny);
+        const int jz = rem_euclid(czs[h] + dz, fr.nz);
+        const long long q = fr.cell_base + ((long long)jz * fr.ny + jy) * (long long)fr.nx + jx;
+        return log1pf(float(off[q + 1] - off[q]));
+      }
+      return fi == 125 ? float(fr.k) / 64.0f : 0.f;
+    };
+    // layer 1
+    float acc[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      const float b0 = sh.b1[nt * 8 + 2 * tig], b1v = sh.b1[nt * 8 + 2 * tig + 1];
+      acc[nt][0] = b0;
+      acc[nt][1] = b1v;
+      acc[nt][2] = b0;
+      acc[nt][3] = b1v;
+    }
+    for (int k0 = 0; k0 < 128; k0 += 8) {
+      const uint32_t a0 = to_tf32(feature(0, k0 + tig));
+      const uint32_t a1 = to_tf32(feature(1, k0 + tig));
+      const uint32_t a2 = to_tf32(feature(0, k0 + tig + 4));
+      const uint32_t a3 = to_tf32(feature(1, k0 + tig + 4));
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        const int n = nt * 8 + g;
+        const uint32_t b0 = __float_as_uint(sh.w1[n * kW1Stride + k0 + tig]);
+        const uint32_t b1 = __float_as_uint(sh.w1[n * kW1Stride + k0 + tig + 4]);
+        mma_tf32(acc[nt], a0, a1, a2, a3, b0, b1);
+      }
+    }
+    // SiLU, then to shared memory (row-major 16 x 64)
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      const int col = nt * 8 + 2 * tig;
+      hbuf[g * kW2Stride + col] = silu(acc[nt][0]);
+      hbuf[g * kW2Stride + col + 1] = silu(acc[nt][1]);
+      hbuf[(g + 8) * kW2Stride + col] = silu(acc[nt][2]);
+      hbuf[(g + 8) * kW2Stride + col + 1] = silu(acc[nt][3]);
+    }
+    __syncwarp();
+    // layer 2
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      const float b0 = sh.b2[nt * 8 + 2 * tig], b1v = sh.b2[nt * 8 + 2 * tig + 1];
+      acc[nt][0] = b0;
+      acc[nt][1] = b1v;
+      acc[nt][2] = b0;
+      acc[nt][3] = b1v;
+    }
+#pragma unroll
+    for (int k0 = 0; k0 < 64; k0 += 8) {
+      const uint32_t a0 = to_tf32(hbuf[g * kW2Stride + k0 + tig]);
+      const uint32_t a1 = to_tf32(hbuf[(g + 8) * kW2Stride + k0 + tig]);
+      const uint32_t a2 = to_tf32(hbuf[g * kW2Stride + k0 + tig + 4]);
+      const uint32_t a3 = to_tf32(hbuf[(g + 8) * kW2Stride + k0 + tig + 4]);
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        const int n = nt * 8 + g;
+        const uint32_t b0 = __float_as_uint(sh.w2[n * kW2Stride + k0 + tig]);
+        const uint32_t b1 = __float_as_uint(sh.w2[n * kW2Stride + k0 + tig + 4]);
+        mma_tf32(acc[nt], a0, a1, a2, a3, b0, b1);
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      const int col = nt * 8 + 2 * tig;
+      hbuf[g * kW2Stride + col] = silu(acc[nt][0]);
+      hbuf[g * kW2Stride + col + 1] = silu(acc[nt][1]);
+      hbuf[(g + 8) * kW2Stride + col] = silu(acc[nt][2]);
+      hbuf[(g + 8) * kW2Stride + col + 1] = silu(acc[nt][3]);
+    }
+    __syncwarp();
+    // layer 3: 8 logits per cell
+    float z[4] = {sh.b3[2 * tig], sh.b3[2 * tig + 1], sh.b3[2 * tig], sh.b3[2 * tig + 1]};
+#pragma unroll
+    for (int k0 = 0; k0 < 64; k0 += 8) {
+      const uint32_t a0 = to_tf32(hbuf[g * kW2Stride + k0 + tig]);
+      const uint32_t a1 = to_tf32(hbuf[(g + 8) * kW2Stride + k0 + tig]);
+      const uint32_t a2 = to_tf32(hbuf[g * kW2Stride + k0 + tig + 4]);
+      const uint32_t a3 = to_tf32(hbuf[(g + 8) * kW2Stride + k0 + tig + 4]);
+      const uint32_t b0 = __float_as_uint(sh.w3[g * kW2Stride + k0 + tig]);
+      const uint32_t b1 = __float_as_uint(sh.w3[g * kW2Stride + k0 + tig + 4]);
+      mma_tf32(z, a0, a1, a2, a3, b0, b1);
+    }
+    __syncwarp();
+    // each quad holds the 8 logits of rows g (z[0], z[1]) and g + 8 (z[2], z[3])
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float lg[8];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        lg[2 * q] = __shfl_sync(0xffffffffu, z[2 * h], (lane & ~3) | q);
+        lg[2 * q + 1] = __shfl_sync(0xffffffffu, z[2 * h + 1], (lane & ~3) | q);
+      }
+      if (tig == 0 && valid[h]) {
+        float m = lg[0];
+#pragma unroll
+        for (int o = 1; o < 8; ++o) m = fmaxf(m, lg[o]);
+        float e[8], sum = 0.f;
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+          e[o] = __expf(lg[o] - m);
+          sum += e[o];
+        }
+        int prop = kMlpOut;
+        float cum = 0.f;
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+          cum += e[o] / sum;
+          if (cum >= tau && prop == kMlpOut) prop = o + 1;
+        }
+        cell_prop[cellid[h]] = int8_t(prop >= kMlpOut ? 0 : prop);
+      }
+    }
+    __syncwarp();
   }
 }
 
@@ -419,15 +573,21 @@ cudaError_t mlp_training_rows(const BatchBuffers &b, const int8_t *stop_log, lon
 }
 
 cudaError_t mlp_propose(const float *params, const BatchBuffers &b, int8_t *cell_prop,
-                        int8_t *source_prop, float tau, cudaStream_t s) {
-  const size_t sm = size_t(kMlpParams) * sizeof(float);
-  cudaError_t e = cudaFuncSetAttribute(k_cell_proposal, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(sm));
+                        int8_t *source_prop, float tau, uint32_t *cell_list, uint32_t *list_count,
+                        cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(list_count, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
-  k_cell_proposal<<<grid_of(b.ncells, 128, 4), 128, sm, s>>>(params, b.frames, b.nframes, b.off,
-                                                             b.ncells, tau, cell_prop);
-  e = cudaGetLastError();
+  k_list_cells<<<grid_of(b.ncells, 256), 256, 0, s>>>(b.off, b.ncells, cell_list, list_count);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const size_t sm = sizeof(TcShared);
+  e = cudaFuncSetAttribute(k_cell_proposal_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
   if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  k_cell_proposal_tc<<<sms * 3, kTcWarps * 32, sm, s>>>(params, b.frames, b.nframes, b.off,
+                                                         cell_list, list_count, tau, cell_prop);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_source_proposal<<<grid_of(b.npts, 256), 256, 0, s>>>(b.frames, b.nframes, b.off, b.ncells,
                                                          b.scell, cell_prop, source_prop);
   return cudaGetLastError();

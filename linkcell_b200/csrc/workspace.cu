@@ -253,7 +253,7 @@ void WorkspaceImpl::release_all() {
   rel(sidx_); rel(replay_list_); rel(replay_i_); rel(scell_); rel(sx_); rel(sy_); rel(sz_);
   rel(replay_d_); rel(rec_); rel(frames_); rel(counters_); rel(h_xyz_); rel(h_d2_);
   rel(h_mask_); rel(h_nn_); rel(active_); rel(proposal_); rel(cell_prop_); rel(stop_log_);
-  rel(model_); rel(shell_table_);
+  rel(model_); rel(shell_table_); rel(cell_list_); rel(list_count_);
   shell_table_ready_ = false;
 }
 
@@ -404,7 +404,10 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
       LC_TRY(cudaMemsetAsync(proposal_.p, std::min(opts.fixed_proposal, 127), P, s));
     } else if (has_model_) {
       LC_TRY(grow(cell_prop_, C));
-      LC_TRY(mlp_propose(model_.p, b, cell_prop_.p, proposal_.p, tau_, s));
+      LC_TRY(grow(cell_list_, C));
+      LC_TRY(grow(list_count_, 1));
+      LC_TRY(mlp_propose(model_.p, b, cell_prop_.p, proposal_.p, tau_, cell_list_.p, list_count_.p,
+                         s));
     } else {
       LC_TRY(cudaMemsetAsync(proposal_.p, 0, P, s));
     }
@@ -455,6 +458,25 @@ Code WorkspaceImpl::training_rows(float *X, int *y, long long cap, long long str
   rows = std::min(avail, cap);
   LC_TRY(mlp_training_rows(bb_, bb_.stop_log, stride, first, X, y, rows, stream()));
   LC_TRY(cudaStreamSynchronize(stream()));
+  return Code::Ok;
+}
+
+Code WorkspaceImpl::proposals(int8_t *out, long long cap, long long stride, long long first,
+                              long long &rows, std::string &detail) {
+  rows = 0;
+  if (!bb_.proposal || !bb_.off) {
+    detail = "no learned search";
+    return Code::DeviceStatus;
+  }
+  uint32_t total = 0;
+  LC_TRY(cudaStreamSynchronize(stream()));
+  LC_TRY(cudaMemcpy(&total, bb_.off + bb_.ncells, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (stride < 1) stride = 1;
+  if (first < 0 || first >= (long long)total) return Code::Ok;
+  const long long avail = ((long long)total - first + stride - 1) / stride;
+  rows = std::min(avail, cap);
+  LC_TRY(cudaMemcpy2D(out, 1, bb_.proposal + first, size_t(stride), 1, size_t(rows),
+                      cudaMemcpyDeviceToHost));
   return Code::Ok;
 }
 

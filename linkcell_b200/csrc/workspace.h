@@ -92,6 +92,10 @@ class WorkspaceImpl {
   // Learned proposals: copy the MLP parameters (host floats) in.
   Code set_model(const float *params, size_t n, float tau, std::string &detail);
   bool has_model() const { return has_model_; }
+  // Proposed shells of the last learned search for the sorted sources
+  // first, first + stride, ... (host buffer).
+  Code proposals(int8_t *out, long long cap, long long stride, long long first, long long &rows,
+                 std::string &detail);
   // Training rows of the last logged search (device X / y buffers).
   Code training_rows(float *X, int *y, long long cap, long long stride, long long first,
                      long long &rows, std::string &detail);
@@ -122,7 +126,7 @@ class WorkspaceImpl {
   Buf<long long> counters_;
   Buf<int8_t> proposal_, cell_prop_, stop_log_;
   Buf<float> model_;
-  Buf<uint32_t> shell_table_;
+  Buf<uint32_t> shell_table_, cell_list_, list_count_;
   bool shell_table_ready_ = false;
   bool has_model_ = false;
   float tau_ = 0.9f;

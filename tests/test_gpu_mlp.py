@@ -95,3 +95,46 @@ def test_learned_walk_with_network_is_exact_and_saves_work(gpu, oracle_mod):
     assert proposals > 0.9 * 150000
     assert lrn[6] < 0.05 * proposals  # short proposals (restarts) stay rare
     assert lrn[5] < fast[5]  # fewer FP64 reranks
+
+
+def test_tensor_core_proposals_match_cpu_network(gpu):
+    """The walk's proposals (tensor-core inference, TF32) agree with the CPU
+    reference network on the same features for nearly every source; a
+    disagreement only moves work, never the result."""
+    import ctypes
+    import os
+    import torch
+    from linkcell_b200 import _capi, _cell_struct, learn, workloads as W
+    from oracle import mlp_ref as M
+    if not os.path.exists(learn.MODEL_PATH):
+        pytest.skip("no trained network shipped")
+    params, tau, _ = learn.load()
+    L = _capi.load()
+    w = W.bimodal_triclinic(n=60000, seed=5, k=32)
+    ws = L.lc_gpu_workspace_new()
+    try:
+        learn.attach(ws)
+        assert L.lc_gpu_set_mode(ws, 2) == 0 and L.lc_gpu_log_shells(ws, 1) == 0
+        x = torch.as_tensor(w["xyz"], device="cuda")
+        nn = torch.empty((60000, 32), dtype=torch.int32, device="cuda")
+        cell = _cell_struct(np.asarray(w["cell"]))
+        torch.cuda.synchronize()
+        assert L.lc_gpu_knearest_many(ws, x.data_ptr(), 60000, 1, ctypes.byref(cell), 32, None, 3.0,
+                                      nn.data_ptr(), None, 1) == 0, _capi.gpu_error()
+        rows = 3000
+        X = torch.empty((rows, 126), dtype=torch.float32, device="cuda")
+        y = torch.empty((rows,), dtype=torch.int32, device="cuda")
+        got = L.lc_gpu_training_rows(ws, ctypes.c_void_p(X.data_ptr()), ctypes.c_void_p(y.data_ptr()),
+                                     rows, 20, 0)
+        prop = np.empty(rows, dtype=np.int8)
+        got2 = L.lc_gpu_proposals(ws, prop.ctypes.data_as(ctypes.c_void_p), rows, 20, 0)
+    finally:
+        L.lc_gpu_workspace_free(ws)
+    assert got == got2 > 1000
+    probs = M.forward(params.astype(np.float64), X[:got].cpu().numpy())["probs"]
+    cum = np.cumsum(probs, axis=1)
+    want = np.argmax(cum >= tau, axis=1) + 1
+    want[want >= 8] = 0
+    want[~(cum >= tau).any(axis=1)] = 0
+    agree = np.mean(want == prop[:got])
+    assert agree > 0.99, agree
