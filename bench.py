@@ -48,7 +48,8 @@ def parse():
     p.add_argument("--mode", type=int, default=-1, help="walk mode; -1 = best available")
     p.add_argument("--n", type=int, default=4_000_000)
     p.add_argument("--k", type=int, default=32)
-    p.add_argument("--tpp", type=int, default=32, help="threads per source of the walk (32 or 1)")
+    p.add_argument("--tpp", type=int, default=0,
+                   help="threads per source of the walk: 32 or 1; 0 lets the autotuner pick")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -218,7 +219,8 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     ws = L.lc_gpu_workspace_new()
     assert ws, _capi.gpu_error()
-    assert L.lc_gpu_set_tpp(ws, args.tpp) == 0
+    if args.tpp:
+        assert L.lc_gpu_set_tpp(ws, args.tpp) == 0
     stream = ctypes.c_void_p(L.lc_gpu_queue(ws))
     tstream = torch.cuda.ExternalStream(stream.value)
 
@@ -264,6 +266,7 @@ def run_ours(args):
         buf = (ctypes.c_longlong * 16)()
         L.lc_gpu_stats(ws, buf, 16, None)
         counters = list(buf)
+        counters.append(int(L.lc_gpu_get_tpp(ws)))  # walk design used (autotuned unless forced)
         total = sum(a.elapsed_time(b) for a, b in ev)
         if world > 1:
             t = torch.tensor([total], dtype=torch.float64, device="cuda")
@@ -308,7 +311,8 @@ def run_ours(args):
         ip = ctypes.POINTER(ctypes.c_int)
         # the host ABI walks with the library's default mode; select the headline mode
         os.environ["LINKCELL_MODE"] = str(best_mode)
-        os.environ["LINKCELL_TPP"] = str(args.tpp)
+        if args.tpp:
+            os.environ["LINKCELL_TPP"] = str(args.tpp)
 
         def host_step():
             rc = L.lc_knearest_d2(ctypes.cast(hx.data_ptr(), dp), n, ctypes.byref(cell), k, None, 3.0,
@@ -345,13 +349,14 @@ def run_ours(args):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic",
            "config": {"workload": "bimodal_triclinic_4M_k32", "n": n, "k": k, "cell_hint": 3.0,
-                      "mode": MODE_NAMES[best_mode], "tpp": args.tpp,
+                      "mode": MODE_NAMES[best_mode], "tpp": cnt[-1],
+                      "tpp_source": "forced" if args.tpp else "autotuned",
                       "parallelism": f"replicas x{world}",
                       "l2": "flushed between timed steps (256 MB write)"},
            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
            "gpu_launches": launches_per_step * args.steps, "clocks": sampler.summary(),
            "plain_fp64": {"value": plain_value, "unit": "sources/s",
-                          "walk_ms": statistics.mean(plain_walk)},
+                          "walk_ms": statistics.mean(plain_walk), "tpp": plain_cnt[-1]},
            "speedup_vs_plain": value / plain_value, "walk_ms": walk_avg_ms,
            "prep_ms": statistics.mean(prep_ms), "replay_ms": statistics.mean(replay_ms),
            "walk_stats_last_step": walk_stats, "model": model_info,

@@ -128,10 +128,22 @@ int lc_gpu_mlp_grad(const float *params, const float *X, const int *y, int batch
 int lc_gpu_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr,
                     void *stream);
 
-/* Threads per source of the walk: 32 (a warp per source, the default) or 1
- * (a thread per source, its heap in shared memory). The environment
- * variable LINKCELL_TPP sets the default of new workspaces. */
+/* Threads per source of the walk: 32 (a warp per source) or 1 (a thread
+ * per source, its heap in shared memory); 0 restores the autotuner, which
+ * times both designs on the first batch of each kind (walk mode, k class,
+ * single or many frames) and keeps the faster. The environment variables
+ * LINKCELL_TPP and LINKCELL_BLOCK override the autotuner for new
+ * workspaces. lc_gpu_get_tpp reports the design of the last batch. */
 int lc_gpu_set_tpp(lc_gpu_workspace *ws, int tpp);
+int lc_gpu_get_tpp(lc_gpu_workspace *ws);
+
+/* CUDA graphs: with on != 0 a search captures its whole launch sequence
+ * (frame-table copy, memsets, kernels) in a CUDA graph and replays it while
+ * the batch keeps its sizes, pointers and configuration; the frame table
+ * (cells may change) is re-read from pinned memory at every replay.
+ * lc_gpu_graph_captures counts the captures. */
+int lc_gpu_set_graph(lc_gpu_workspace *ws, int on);
+int lc_gpu_graph_captures(lc_gpu_workspace *ws);
 
 /* Enqueue on the caller's stream instead of the workspace's own one
  * (NULL restores the workspace stream). */

@@ -482,10 +482,26 @@ int lc_gpu_get_mode(lc_gpu_workspace *ws) { return ws ? ws->ws.opts.mode : -1; }
 
 int lc_gpu_set_tpp(lc_gpu_workspace *ws, int tpp) {
   if (!ws) return gpu_fail(Code::NullPointer);
-  if (tpp != 1 && tpp != 32) return gpu_fail_msg("threads per source must be 1 or 32");
-  ws->ws.opts.tpp = tpp;
+  if (tpp != 0 && tpp != 1 && tpp != 32)
+    return gpu_fail_msg("threads per source must be 1 or 32 (0: autotune)");
+  if (tpp == 0) {
+    ws->ws.opts.tpp_forced = false;
+  } else {
+    ws->ws.opts.tpp = tpp;
+    ws->ws.opts.tpp_forced = true;
+  }
   return 0;
 }
+
+int lc_gpu_get_tpp(lc_gpu_workspace *ws) { return ws ? ws->ws.last_tpp : -1; }
+
+int lc_gpu_set_graph(lc_gpu_workspace *ws, int on) {
+  if (!ws) return gpu_fail(Code::NullPointer);
+  ws->ws.opts.graph = on != 0;
+  return 0;
+}
+
+int lc_gpu_graph_captures(lc_gpu_workspace *ws) { return ws ? ws->ws.graph_captures : -1; }
 
 int lc_gpu_set_model(lc_gpu_workspace *ws, const float *params, size_t n_params, float tau) {
   if (!ws || !params) return gpu_fail(Code::NullPointer);

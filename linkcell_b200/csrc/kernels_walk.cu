@@ -1350,6 +1350,327 @@ __global__ void __launch_bounds__(kSelectWarps * 32, 2) k_select_walk(BatchBuffe
   flush_counters(b, cnt);
 }
 
+// ------------------------------------------------------------------------
+// Warp-parallel literal replay of the reference heap for one source (finite
+// coordinates). The warp evaluates the reference visit sequence 32
+// candidates at a time -- shells ascending, offsets in lexicographic order
+// (src/knearest.rs:436-445), occupants in descending point index -- and
+// applies KHeap::push in that order: the first k candidates fill slots 0..k-1;
+// afterwards a candidate replaces the first slot holding the maximum only
+// when it is strictly smaller, which is a no-op otherwise. Slots are
+// distributed: slot s lives in lane s % 32, register s / 32. With finite
+// values "first slot with the maximum" is the parallel argmax (largest
+// value, then smallest slot), so the result is the reference's exactly.
+
+// Offset e of shell R in the reference's lexicographic order.
+__device__ __forceinline__ void lex_offset(int R, int e, int &dx, int &dy, int &dz) {
+  if (R == 1) {
+    dx = e / 9 - 1;
+    dy = (e / 3) % 3 - 1;
+    dz = e % 3 - 1;
+    return;
+  }
+  const int w = 2 * R + 1;
+  const int full = w * w, part = 8 * R;
+  if (e < full) {
+    dx = -R;
+    dy = e / w - R;
+    dz = e % w - R;
+    return;
+  }
+  e -= full;
+  if (e < (2 * R - 1) * part) {
+    const int slab = e / part;
+    int r = e - slab * part;
+    dx = -R + 1 + slab;
+    if (r < w) {
+      dy = -R;
+      dz = r - R;
+      return;
+    }
+    r -= w;
+    if (r < 2 * (2 * R - 1)) {
+      dy = -R + 1 + r / 2;
+      dz = (r & 1) ? R : -R;
+      return;
+    }
+    r -= 2 * (2 * R - 1);
+    dy = R;
+    dz = r - R;
+    return;
+  }
+  e -= (2 * R - 1) * part;
+  dx = R;
+  dy = e / w - R;
+  dz = e % w - R;
+}
+
+template <int KPL>
+struct ReplayHeap {
+  double d[KPL];
+  int j[KPL];
+};
+
+// First slot holding the maximum value among the n filled slots.
+template <int KPL>
+__device__ __forceinline__ void heap_argmax(const ReplayHeap<KPL> &H, int lane, int n, double &wmax,
+                                            int &widx) {
+  double bd = -pinf();
+  int bs = 0x7fffffff;
+#pragma unroll
+  for (int r = 0; r < KPL; ++r) {
+    const int slot = r * 32 + lane;
+    if (slot < n && (H.d[r] > bd || (H.d[r] == bd && slot < bs))) {
+      bd = H.d[r];
+      bs = slot;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double od = __shfl_xor_sync(kFull, bd, o);
+    const int os = __shfl_xor_sync(kFull, bs, o);
+    if (od > bd || (od == bd && os < bs)) {
+      bd = od;
+      bs = os;
+    }
+  }
+  wmax = bd;
+  widx = bs;
+}
+
+template <int KPL>
+__device__ void warp_replay(const BatchBuffers &b, const FrameDesc &fr, long long p, int lane) {
+  const int k = fr.k;
+  const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
+  const uint32_t lc = b.scell[p];
+  const int ix = int(lc % uint32_t(nx));
+  const int iy = int((lc / uint32_t(nx)) % uint32_t(ny));
+  const int iz = int(lc / (uint32_t(nx) * uint32_t(ny)));
+  const double px = b.sx[p], py = b.sy[p], pz = b.sz[p];
+  const long long cb = fr.cell_base;
+  ReplayHeap<KPL> H;
+#pragma unroll
+  for (int r = 0; r < KPL; ++r) {
+    H.d[r] = pinf();
+    H.j[r] = 0x7fffffff;
+  }
+  int n = 0, widx = 0;
+  double wmax = pinf();
+  for (int R = 1; R <= fr.max_reach; ++R) {
+    const bool dedupe = 2 * R + 1 > nx || 2 * R + 1 > ny || 2 * R + 1 > nz;
+    const int E = R == 1 ? 27 : 24 * R * R + 2;
+    for (int e0 = 0; e0 < E; e0 += 32) {
+      const int e = e0 + lane;
+      int a1 = 0, nc = 0, wa = 0, wb = 0, wc = 0;
+      if (e < E) {
+        int dx, dy, dz, cx, cy, cz;
+        lex_offset(R, e, dx, dy, dz);
+        wrap_axis(ix + dx, nx, cx, wa);
+        wrap_axis(iy + dy, ny, cy, wb);
+        wrap_axis(iz + dz, nz, cz, wc);
+        const long long c = cb + ((long long)cz * ny + cy) * (long long)nx + cx;
+        const int a0 = int(b.off[c]);
+        a1 = int(b.off[c + 1]);
+        nc = a1 - a0;
+      }
+      int incl = nc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int tot = __shfl_sync(kFull, incl, 31);
+      const int excl = incl - nc;
+      for (int g0 = 0; g0 < tot; g0 += 32) {
+        const int g = g0 + lane;
+        int owner = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int v = __shfl_sync(kFull, incl, owner + step - 1);
+          if (v <= g) owner += step;
+        }
+        owner &= 31;
+        const int oa1 = __shfl_sync(kFull, a1, owner);
+        const int oex = __shfl_sync(kFull, excl, owner);
+        const int owa = __shfl_sync(kFull, wa, owner);
+        const int owb = __shfl_sync(kFull, wb, owner);
+        const int owc = __shfl_sync(kFull, wc, owner);
+        const long long t = (long long)oa1 - 1 - (g - oex);  // descending point index
+        bool valid = g < tot && t != p;
+        double d = 0.0;
+        int j = 0;
+        if (valid) {
+          double shx, shy, shz;
+          lattice_shift(fr, owa, owb, owc, shx, shy, shz);
+          d = dist2_shifted(px, py, pz, b.sx[t], b.sy[t], b.sz[t], shx, shy, shz);
+          j = b.sidx[t];
+        }
+        unsigned vm = __ballot_sync(kFull, valid);
+        if (dedupe) {
+          // index repeats possible: push one candidate at a time
+          while (vm) {
+            const int src = __ffs(vm) - 1;
+            vm &= vm - 1;
+            const double x = shfl_d(d, src);
+            const int jx = __shfl_sync(kFull, j, src);
+            int hit = -1;
+#pragma unroll
+            for (int r = 0; r < KPL; ++r) {
+              const int slot = r * 32 + lane;
+              const unsigned hm = __ballot_sync(kFull, slot < n && H.j[r] == jx);
+              if (hm) hit = r * 32 + __ffs(hm) - 1;
+            }
+            if (hit >= 0) {
+              const double old = shfl_d(H.d[hit >> 5], hit & 31);
+              if (x < old) {
+                if ((hit & 31) == lane) H.d[hit >> 5] = x;
+                if (n >= k) heap_argmax(H, lane, n, wmax, widx);
+              }
+              continue;
+            }
+            if (n < k) {
+              if ((n & 31) == lane) {
+                H.d[n >> 5] = x;
+                H.j[n >> 5] = jx;
+              }
+              ++n;
+              if (n == k) heap_argmax(H, lane, n, wmax, widx);
+              continue;
+            }
+            if (x < wmax) {
+              if ((widx & 31) == lane) {
+                H.d[widx >> 5] = x;
+                H.j[widx >> 5] = jx;
+              }
+              heap_argmax(H, lane, n, wmax, widx);
+            }
+          }
+          continue;
+        }
+        // fill: the first k - n valid candidates append in order
+        if (n < k) {
+          const int cntv = __popc(vm);
+          const int take = min(cntv, k - n);
+#pragma unroll
+          for (int r = 0; r < KPL; ++r) {
+            const int slot = r * 32 + lane;
+            const int rank = slot - n;
+            const bool mine = rank >= 0 && rank < take;
+            const int src = mine ? int(__fns(vm, 0, rank + 1)) : lane;
+            const double vd = shfl_d(d, src);
+            const int vj = __shfl_sync(kFull, j, src);
+            if (mine) {
+              H.d[r] = vd;
+              H.j[r] = vj;
+            }
+          }
+          n += take;
+          // drop the appended lanes: the first `take` set bits of vm
+          for (int q = 0; q < take; ++q) vm &= vm - 1;
+          if (n == k) heap_argmax(H, lane, n, wmax, widx);
+        }
+        // replacements in lane order
+        while (vm) {
+          const unsigned cm = __ballot_sync(kFull, ((vm >> lane) & 1u) && d < wmax);
+          if (!cm) break;
+          const int src = __ffs(cm) - 1;
+          vm &= (src == 31) ? 0u : ~((2u << src) - 1u);  // lanes up to src are done
+          const double x = shfl_d(d, src);
+          const int jx = __shfl_sync(kFull, j, src);
+          if ((widx & 31) == lane) {
+            H.d[widx >> 5] = x;
+            H.j[widx >> 5] = jx;
+          }
+          heap_argmax(H, lane, n, wmax, widx);
+        }
+      }
+    }
+    if (n >= k && wmax <= stop_bound(R, fr.cell_min)) break;
+  }
+  // KHeap::finish: ascending (total_cmp, index)
+  if (KPL == 1) {
+    double sdv = lane < n ? H.d[0] : pinf();
+    int sjv = lane < n ? H.j[0] : 0x7fffffff;
+    warp_sort_pairs(sdv, sjv, lane);
+    H.d[0] = sdv;
+    H.j[0] = sjv;
+  } else {
+    // small k-lists beyond 32: gather to lane 0 order through insertion by rank
+    double rd[KPL];
+    int rj[KPL];
+#pragma unroll
+    for (int r = 0; r < KPL; ++r) {
+      const int slot = r * 32 + lane;
+      rd[r] = slot < n ? H.d[r] : pinf();
+      rj[r] = slot < n ? H.j[r] : 0x7fffffff;
+    }
+    // rank of every slot = number of slots ordered before it
+    int rank[KPL];
+#pragma unroll
+    for (int r = 0; r < KPL; ++r) rank[r] = 0;
+    for (int src = 0; src < 32; ++src) {
+#pragma unroll
+      for (int r2 = 0; r2 < KPL; ++r2) {
+        const double od = shfl_d(rd[r2], src);
+        const int oj = __shfl_sync(kFull, rj[r2], src);
+#pragma unroll
+        for (int r = 0; r < KPL; ++r) rank[r] += lex_less(od, oj, rd[r], rj[r]) ? 1 : 0;
+      }
+    }
+    const int i = b.sidx[p];
+    int *row = b.out_nn + fr.out_base + (long long)i * k;
+    double *drow = b.out_d2 ? b.out_d2 + fr.out_base + (long long)i * k : nullptr;
+#pragma unroll
+    for (int r = 0; r < KPL; ++r) {
+      const int slot = r * 32 + lane;
+      if (slot < n) {
+        row[rank[r]] = rj[r];
+        if (drow) drow[rank[r]] = rd[r];
+      }
+    }
+    for (int pos = n + lane; pos < k; pos += 32) {
+      row[pos] = -1;
+      if (drow) drow[pos] = qnan();
+    }
+    return;
+  }
+  const int i = b.sidx[p];
+  int *row = b.out_nn + fr.out_base + (long long)i * k;
+  double *drow = b.out_d2 ? b.out_d2 + fr.out_base + (long long)i * k : nullptr;
+  if (lane < k) {
+    const bool ok = lane < n;
+    row[lane] = ok ? H.j[0] : -1;
+    if (drow) drow[lane] = ok ? H.d[0] : qnan();
+  }
+}
+
+template <int KPL>
+__global__ void __launch_bounds__(256, 2) k_replay_warp(BatchBuffers b) {
+  long long cnt = *b.replay_count;
+  if (cnt > b.replay_cap) cnt = b.replay_cap;
+  const int lane = threadIdx.x & 31;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long q = warp; q < cnt; q += nwarps) {
+    const long long p = b.replay_list[q];
+    const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
+    const FrameDesc &fr = b.frames[f];
+    if ((b.frame_flags[f] & kFrameNaN) || fr.k > 32 * KPL) {
+      // NaN comparisons follow the reference's sequential scans: one thread
+      if (lane == 0 && warp < b.replay_threads) {
+        double *hd = b.replay_d + warp * b.kmax;
+        int *hi = b.replay_i + warp * b.kmax;
+        const int m = replay_walk(b, fr, p, hd, hi, 1);
+        write_row(b, fr, b.sidx[p], hd, hi, 1, m);
+      }
+      __syncwarp();
+      continue;
+    }
+    warp_replay<KPL>(b, fr, p, lane);
+    __syncwarp();
+  }
+}
+
 int sm_count() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -1444,6 +1765,20 @@ cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t
 
 cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s) {
   if (b.replay_threads <= 0) return cudaSuccess;
+  if (b.kmax <= 256) {
+    // one warp per queued source; NaN frames take one thread of the warp
+    const int warps = std::max(1, std::min(b.replay_threads, sm_count() * 16));
+    const int grid = (warps + 7) / 8;
+    if (b.kmax <= 32)
+      k_replay_warp<1><<<grid, 256, 0, s>>>(b);
+    else if (b.kmax <= 64)
+      k_replay_warp<2><<<grid, 256, 0, s>>>(b);
+    else if (b.kmax <= 128)
+      k_replay_warp<4><<<grid, 256, 0, s>>>(b);
+    else
+      k_replay_warp<8><<<grid, 256, 0, s>>>(b);
+    return cudaGetLastError();
+  }
   const int block = 128;
   const int grid = (b.replay_threads + block - 1) / block;
   k_replay<<<grid, block, 0, s>>>(b);

@@ -182,7 +182,10 @@ WorkspaceImpl::WorkspaceImpl() {
   }
   if (const char *t = std::getenv("LINKCELL_TPP")) {
     const int v = std::atoi(t);
-    if (v == 1 || v == 32) opts.tpp = v;
+    if (v == 1 || v == 32) {
+      opts.tpp = v;
+      opts.tpp_forced = true;
+    }
   }
   if (const char *b = std::getenv("LINKCELL_BLOCK")) {
     const int v = std::atoi(b);
@@ -191,12 +194,16 @@ WorkspaceImpl::WorkspaceImpl() {
   cudaGetDevice(&device_);
   cudaStreamCreateWithFlags(&own_, cudaStreamNonBlocking);
   for (auto &e : ev_) cudaEventCreate(&e);
+  cudaEventCreateWithFlags(&ev_done_, cudaEventDisableTiming);
 }
 
 WorkspaceImpl::~WorkspaceImpl() {
   if (own_) cudaStreamSynchronize(own_);
   if (user_set_ && user_) cudaStreamSynchronize(user_);
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
   release_all();
+  if (h_frames_) cudaFreeHost(h_frames_);
+  if (ev_done_) cudaEventDestroy(ev_done_);
   for (auto &e : ev_)
     if (e) cudaEventDestroy(e);
   if (own_) cudaStreamDestroy(own_);
@@ -287,6 +294,8 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
     ~LastStream() { slot = s; }
   } last_guard{last_stream_, s};
   const long long tiles = scan_tiles(ncells);
+
+  // ---- 1. buffers (grow-only; nothing is allocated once they fit)
   LC_TRY(grow(cell_of_, P));
   LC_TRY(grow(arank_, P));
   LC_TRY(grow(tmp_, P));
@@ -307,7 +316,16 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   LC_TRY(grow(replay_list_, P));
   LC_TRY(grow(frames_, size_t(nf)));
   LC_TRY(grow(counters_, size_t(kNumCounters)));
-
+  if (opts.log_shells) LC_TRY(grow(stop_log_, P));
+  const bool learned = opts.mode == kModeLearned && kmax <= 256;
+  if (learned) {
+    LC_TRY(grow(proposal_, P));
+    if (opts.fixed_proposal <= 0 && has_model_) {
+      LC_TRY(grow(cell_prop_, C));
+      LC_TRY(grow(cell_list_, C));
+      LC_TRY(grow(list_count_, 1));
+    }
+  }
   if (!shell_table_ready_) {
     const int rmax = kShellTableRmax;
     const size_t entries = size_t(2 * rmax + 1) * (2 * rmax + 1) * (2 * rmax + 1);
@@ -319,18 +337,6 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
     LC_TRY(cudaStreamSynchronize(s));
     shell_table_ready_ = true;
   }
-
-  WalkLaunch wl;
-  wl.mode = opts.mode;
-  wl.tpp = opts.tpp;
-  wl.prune = opts.prune;
-  wl.kmax = kmax;
-  // The shared-memory heap walk covers k <= 256; larger k runs the exact
-  // sequential replay for every source.
-  if (kmax > 256) wl.mode = kModeReplayAll;
-  wl.block = opts.block > 0 ? std::min(opts.block, walk_max_block(wl.mode, kmax))
-                            : walk_max_block(wl.mode, kmax);
-
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_);
   const int replay_threads = int(std::min<long long>(
@@ -339,18 +345,23 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
                                                                      (256LL << 20) / (kmax * 12)))));
   LC_TRY(grow(replay_d_, size_t(replay_threads) * kmax));
   LC_TRY(grow(replay_i_, size_t(replay_threads) * kmax));
+  // pinned staging of the frame table (the previous batch may still read it)
+  if (done_pending_) {
+    LC_TRY(cudaEventSynchronize(ev_done_));
+    done_pending_ = false;
+  }
+  if (size_t(nf) > h_frames_cap_) {
+    if (h_frames_) cudaFreeHost(h_frames_);
+    h_frames_ = nullptr;
+    h_frames_cap_ = 0;
+    void *hp = nullptr;
+    LC_TRY(cudaMallocHost(&hp, sizeof(FrameDesc) * size_t(nf) * 2));
+    h_frames_ = static_cast<FrameDesc *>(hp);
+    h_frames_cap_ = size_t(nf) * 2;
+  }
+  std::memcpy(h_frames_, frames.data(), sizeof(FrameDesc) * size_t(nf));
 
-  LC_TRY(cudaMemcpyAsync(frames_.p, frames.data(), sizeof(FrameDesc) * nf, cudaMemcpyHostToDevice,
-                         s));
-  LC_TRY(cudaMemsetAsync(count_.p, 0, C * sizeof(uint32_t), s));
-  LC_TRY(cudaMemsetAsync(tile_state_.p, 0, size_t(tiles) * sizeof(unsigned long long), s));
-  LC_TRY(cudaMemsetAsync(tile_counter_.p, 0, sizeof(uint32_t), s));
-  LC_TRY(cudaMemsetAsync(work_.p, 0, sizeof(uint32_t), s));
-  LC_TRY(cudaMemsetAsync(replay_count_.p, 0, sizeof(uint32_t), s));
-  LC_TRY(cudaMemsetAsync(status_.p, 0, sizeof(int), s));
-  LC_TRY(cudaMemsetAsync(frame_flags_.p, 0, sizeof(int) * nf, s));
-  LC_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(long long) * kNumCounters, s));
-
+  // ---- 2. device view of the batch
   BatchBuffers &b = bb_;
   b = BatchBuffers();
   b.xyz = xyz;
@@ -387,45 +398,135 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   b.counters = counters_.p;
   b.shell_table = shell_table_.p;
   b.shell_rmax = kShellTableRmax;
+  b.stop_log = opts.log_shells ? stop_log_.p : nullptr;
+  b.proposal = learned ? proposal_.p : nullptr;
 
-  if (collect_stats) LC_TRY(cudaEventRecord(ev_[0], s));
-  LC_TRY(launch_fold_bin(b, s));
-  LC_TRY(launch_scan(b, s));
-  LC_TRY(launch_place(b, s));
-  if (opts.log_shells) {
-    LC_TRY(grow(stop_log_, P));
-    b.stop_log = stop_log_.p;
-  }
-  if (collect_stats) LC_TRY(cudaEventRecord(ev_[1], s));
-  if (wl.mode == kModeLearned) {
-    // shell proposals per sorted source (part of the walk phase)
-    LC_TRY(grow(proposal_, P));
-    if (opts.fixed_proposal > 0) {
-      LC_TRY(cudaMemsetAsync(proposal_.p, std::min(opts.fixed_proposal, 127), P, s));
-    } else if (has_model_) {
-      LC_TRY(grow(cell_prop_, C));
-      LC_TRY(grow(cell_list_, C));
-      LC_TRY(grow(list_count_, 1));
-      LC_TRY(mlp_propose(model_.p, b, cell_prop_.p, proposal_.p, tau_, cell_list_.p, list_count_.p,
-                         s));
-    } else {
-      LC_TRY(cudaMemsetAsync(proposal_.p, 0, P, s));
+  // ---- 3. walk configuration: overrides, else the autotuned choice
+  WalkLaunch wl;
+  wl.mode = kmax > 256 ? int(kModeReplayAll) : opts.mode;
+  wl.kmax = kmax;
+  wl.prune = opts.prune;
+  const int kclass = kmax <= 32 ? 0 : (kmax <= 64 ? 1 : (kmax <= 128 ? 2 : 3));
+  const int tkey = (wl.mode * 4 + kclass) * 2 + (nf > 1 ? 1 : 0);
+  auto set_tpp = [&](int tpp) {
+    wl.tpp = tpp;
+    const int maxblk = walk_max_block(wl.mode, kmax);
+    wl.block = opts.block > 0 ? std::min(opts.block, maxblk) : maxblk;
+  };
+  bool done = false;  // the batch's results are already in place
+  if (opts.tpp_forced || !opts.autotune || wl.mode == kModeReplayAll) {
+    set_tpp(opts.tpp);
+  } else if (tuned_.count(tkey)) {
+    set_tpp(tuned_[tkey]);
+  } else {
+    // time both walk designs once on this batch (their results are
+    // identical) and keep the faster one for every later batch of this kind
+    const int cand[2] = {32, 1};
+    float ms[2] = {0.f, 0.f};
+    for (int c = 0; c < 2; ++c) {
+      set_tpp(cand[c]);
+      const Code rc = enqueue(b, wl, nf, C, tiles, s, true, detail);
+      if (rc != Code::Ok) return rc;
+      LC_TRY(cudaEventSynchronize(ev_[3]));
+      LC_TRY(cudaEventElapsedTime(&ms[c], ev_[1], ev_[2]));
     }
-    b.proposal = proposal_.p;
+    const int best = ms[1] < ms[0] ? 1 : 0;
+    tuned_[tkey] = cand[best];
+    set_tpp(cand[best]);
+    done = best == 1 && !opts.graph;  // the last run used the winner
+    if (!done && !opts.graph) {
+      const Code rc = enqueue(b, wl, nf, C, tiles, s, collect_stats, detail);
+      if (rc != Code::Ok) return rc;
+      done = true;
+    }
+    timed_ = true;
+    graph_total_ = false;
   }
-  LC_TRY(launch_walk(b, wl, s));
-  if (collect_stats) LC_TRY(cudaEventRecord(ev_[2], s));
-  LC_TRY(launch_replay(b, s));
-  if (collect_stats) LC_TRY(cudaEventRecord(ev_[3], s));
-  timed_ = collect_stats;
+  last_tpp = wl.tpp;
+
+  // ---- 4. enqueue: direct launches, or a CUDA graph replayed while the
+  // batch signature (sizes, pointers, configuration) stays the same
+  if (done) {
+    // autotuning left this batch's results and stats in place
+  } else if (opts.graph) {
+    const GraphKey key{npts, ncells, nf, kmax, xyz, mask, out_nn, out_d2, wl.mode, wl.tpp,
+                       wl.block, has_model_ ? 1 : 0, opts.fixed_proposal, opts.log_shells};
+    if (!graph_exec_ || !(key == graph_key_)) {
+      if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+      graph_exec_ = nullptr;
+      cudaGraph_t g = nullptr;
+      LC_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      const Code c = enqueue(b, wl, nf, C, tiles, s, false, detail);
+      const cudaError_t ce = cudaStreamEndCapture(s, &g);
+      if (c != Code::Ok) {
+        if (g) cudaGraphDestroy(g);
+        return c;
+      }
+      LC_TRY(ce);
+      const cudaError_t ie = cudaGraphInstantiate(&graph_exec_, g, 0);
+      cudaGraphDestroy(g);
+      LC_TRY(ie);
+      graph_key_ = key;
+      ++graph_captures;
+    }
+    LC_TRY(cudaEventRecord(ev_[0], s));
+    LC_TRY(cudaGraphLaunch(graph_exec_, s));
+    LC_TRY(cudaEventRecord(ev_[3], s));
+    timed_ = false;
+    graph_total_ = true;
+  } else {
+    const Code c = enqueue(b, wl, nf, C, tiles, s, collect_stats, detail);
+    if (c != Code::Ok) return c;
+    timed_ = collect_stats;
+    graph_total_ = false;
+  }
+  LC_TRY(cudaEventRecord(ev_done_, s));
+  done_pending_ = true;
   if (!wait) return Code::Ok;
   LC_TRY(cudaStreamSynchronize(s));
+  done_pending_ = false;
   int st = 0;
   LC_TRY(cudaMemcpy(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost));
   if (st != 0) {
     detail = "device status " + std::to_string(st);
     return Code::DeviceStatus;
   }
+  return Code::Ok;
+}
+
+Code WorkspaceImpl::enqueue(BatchBuffers &b, const WalkLaunch &wl, int nf, size_t C,
+                            long long tiles, cudaStream_t s, bool timed, std::string &detail) {
+  LC_TRY(cudaMemcpyAsync(frames_.p, h_frames_, sizeof(FrameDesc) * size_t(nf),
+                         cudaMemcpyHostToDevice, s));
+  LC_TRY(cudaMemsetAsync(count_.p, 0, C * sizeof(uint32_t), s));
+  LC_TRY(cudaMemsetAsync(tile_state_.p, 0, size_t(tiles) * sizeof(unsigned long long), s));
+  LC_TRY(cudaMemsetAsync(tile_counter_.p, 0, sizeof(uint32_t), s));
+  LC_TRY(cudaMemsetAsync(work_.p, 0, sizeof(uint32_t), s));
+  LC_TRY(cudaMemsetAsync(replay_count_.p, 0, sizeof(uint32_t), s));
+  LC_TRY(cudaMemsetAsync(status_.p, 0, sizeof(int), s));
+  LC_TRY(cudaMemsetAsync(frame_flags_.p, 0, sizeof(int) * size_t(nf), s));
+  LC_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(long long) * kNumCounters, s));
+  if (timed) LC_TRY(cudaEventRecord(ev_[0], s));
+  LC_TRY(launch_fold_bin(b, s));
+  LC_TRY(launch_scan(b, s));
+  LC_TRY(launch_place(b, s));
+  if (timed) LC_TRY(cudaEventRecord(ev_[1], s));
+  if (b.proposal) {
+    // shell proposals per sorted source (part of the walk phase)
+    const size_t P = size_t(b.npts);
+    if (opts.fixed_proposal > 0) {
+      LC_TRY(cudaMemsetAsync(proposal_.p, std::min(opts.fixed_proposal, 127), P, s));
+    } else if (has_model_) {
+      LC_TRY(mlp_propose(model_.p, b, cell_prop_.p, proposal_.p, tau_, cell_list_.p,
+                         list_count_.p, s));
+    } else {
+      LC_TRY(cudaMemsetAsync(proposal_.p, 0, P, s));
+    }
+  }
+  LC_TRY(launch_walk(b, wl, s));
+  if (timed) LC_TRY(cudaEventRecord(ev_[2], s));
+  LC_TRY(launch_replay(b, s));
+  if (timed) LC_TRY(cudaEventRecord(ev_[3], s));
   return Code::Ok;
 }
 
@@ -483,7 +584,12 @@ Code WorkspaceImpl::proposals(int8_t *out, long long cap, long long stride, long
 Code WorkspaceImpl::fetch_stats(Stats &out, std::string &detail) {
   out = Stats();
   if (!counters_.p) return Code::Ok;
-  if (timed_) {
+  if (graph_total_) {
+    LC_TRY(cudaEventSynchronize(ev_[3]));
+    float t = 0.f;
+    LC_TRY(cudaEventElapsedTime(&t, ev_[0], ev_[3]));
+    out.ms_total = t;
+  } else if (timed_) {
     LC_TRY(cudaEventSynchronize(ev_[3]));
     float a = 0.f, b = 0.f, c = 0.f, t = 0.f;
     LC_TRY(cudaEventElapsedTime(&a, ev_[0], ev_[1]));

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -49,6 +50,9 @@ struct WalkOptions {
   int prune = 1;
   int fixed_proposal = 0;  // learned walk: > 0 proposes this shell for every source
   int log_shells = 0;      // record the settled shell of every source (training data)
+  bool tpp_forced = false; // tpp set explicitly (API or LINKCELL_TPP): no autotuning
+  bool autotune = true;    // time the walk designs on the first batch of each kind
+  bool graph = false;      // capture the launch sequence in a CUDA graph and replay it
 };
 
 struct Stats {
@@ -78,6 +82,8 @@ class WorkspaceImpl {
 
   WalkOptions opts;
   bool collect_stats = true;
+  int last_tpp = 0;          // walk design of the last batch
+  int graph_captures = 0;    // CUDA graphs captured so far
   // Counters and phase times of the last run (waits for it to finish).
   Code fetch_stats(Stats &out, std::string &detail);
 
@@ -108,6 +114,28 @@ class WorkspaceImpl {
   };
   template <class T>
   cudaError_t grow(Buf<T> &b, size_t n);
+  Code enqueue(BatchBuffers &b, const WalkLaunch &wl, int nf, size_t C, long long tiles,
+               cudaStream_t s, bool timed, std::string &detail);
+
+  struct GraphKey {
+    long long npts = -1, ncells = -1;
+    int nf = 0, kmax = 0;
+    const void *xyz = nullptr, *mask = nullptr, *nn = nullptr, *d2 = nullptr;
+    int mode = 0, tpp = 0, block = 0, model = 0, fixed = 0, log = 0;
+    bool operator==(const GraphKey &o) const {
+      return npts == o.npts && ncells == o.ncells && nf == o.nf && kmax == o.kmax && xyz == o.xyz &&
+             mask == o.mask && nn == o.nn && d2 == o.d2 && mode == o.mode && tpp == o.tpp &&
+             block == o.block && model == o.model && fixed == o.fixed && log == o.log;
+    }
+  };
+  GraphKey graph_key_;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  bool graph_total_ = false;
+  std::map<int, int> tuned_;
+  FrameDesc *h_frames_ = nullptr;
+  size_t h_frames_cap_ = 0;
+  cudaEvent_t ev_done_ = nullptr;
+  bool done_pending_ = false;
   void release_all();
 
   int device_ = -1;
