@@ -341,7 +341,7 @@ def run_ours(args):
         cpu = cpu_baseline(w, args.cpu_seconds)
 
     names = ["pairs", "inserts", "replays", "shells", "pruned", "reranks", "prop_under",
-             "prop_over", "prop_exact", "revisited"]
+             "prop_over", "prop_exact", "revisited", "fallback"]
     walk_stats = {nm: cnt[i] for i, nm in enumerate(names)}  # counters of the last step
     launches_per_step = 6
     out = {"metric": METRIC, "value": value, "unit": "sources/s", "n_gpus": world,

@@ -165,7 +165,7 @@ class Workspace:
         ms = ctypes.c_double()
         self._L.lc_gpu_stats(self._ws, buf, 16, ctypes.byref(ms))
         names = ["pairs", "inserts", "replays", "shells", "pruned", "reranks", "prop_under",
-                 "prop_over", "prop_exact", "revisited"]
+                 "prop_over", "prop_exact", "revisited", "fallback"]
         out = {name: int(buf[i]) for i, name in enumerate(names)}
         out["device_ms"] = ms.value
         return out

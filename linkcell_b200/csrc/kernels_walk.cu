@@ -959,45 +959,94 @@ __global__ void __launch_bounds__(256, 2) k_team_walk(BatchBuffers b) {
 }
 
 // ------------------------------------------------------------------------
-// Cube walk of the learned mode: one warp per source opens the proposed
-// cube (shells 1..R_p) in a single pass and selects instead of inserting.
+// Cube select walk of the learned mode: one warp per source opens the
+// proposed cube (shells 1..R_p) in one pass and selects instead of inserting.
 //
-//  1. Gather: every candidate of the cube whose cell is not pruned and whose
-//     FP32 distance passes the filter at B(R_p) = (R_p cell_min)^2 goes to a
-//     per-warp shared-memory buffer (FP32 distance, sorted position, shell,
-//     wrap counts).
-//  2. Stop reach: the reference stops at the first R with at least k
+//  1. Gather. The cube is (2 R_p + 1)^2 rows of cells along x; cells sort by
+//     (z, y, x), so the cells of a row that survive the distance bound form
+//     at most two contiguous ranges of the sorted points (two when the row
+//     wraps the box in x). Each lane trims one row to the x range whose FP32
+//     lower bound lam |gap|^2 can pass the filter at B(R_p) = (R_p cell_min)^2,
+//     the warp walks the concatenated ranges 32 candidates at a time (the
+//     row of candidate g is found from one OR-reduction of row starts), and
+//     candidates with d32 <= thr(B(R_p)) go to a per-warp buffer (FP32
+//     distance, sorted position, shell, wrap counts).
+//  2. Stop reach. The reference stops at the first R with at least k
 //     candidates of shells <= R within B(R). Each candidate counts from
-//     reach max(shell, b(d)), b(d) = the first R with d <= B(R); b is exact
-//     (an FP64 recompute decides whenever d32 lies within the error band of
-//     a bound). No R <= R_p qualifies: the proposal was short, the source
-//     takes the incremental walk instead.
-//  3. Select: a 32-bucket histogram (equal volume in d^1.5) over the
-//     candidates of shells <= R* locates the k-th FP32 value; S = every such
-//     candidate with d32 <= T + 2 band(T), T = the largest d32 of the
-//     buckets up to the k-th, holds the k smallest exact distances and every
-//     value tied with the k-th, and nothing else can tie (with the FP32
-//     error band(x) = 8u x + beta, any candidate above T + 3 band(T) has an
-//     exact distance above T + band(T), which bounds the k-th value).
+//     reach max(shell, b(d)), b(d) = the first R >= 1 with d <= B(R), read
+//     from sqrt(d32) / cell_min and decided in exact FP64 whenever that value
+//     lies within its error band of an integer. No R <= R_p qualifies: the
+//     proposal was short and the source goes to the literal replay.
+//  3. Select. Two 32-bucket histograms (linear in d32 over [0, B(R*)], then
+//     within the bucket holding the k-th value) give T = the largest d32 of
+//     the buckets up to the k-th; S = the candidates of shells <= R* with
+//     d32 <= T + 3 band(T) holds the k smallest exact distances and every
+//     value tied with the k-th, and nothing else can tie (with the FP32 error
+//     band(x) = 8u x + beta, any candidate above T + 3 band(T) has an exact
+//     distance above T + band(T), which bounds the k-th value).
 //  4. S is recomputed in exact FP64, bitonic-sorted by (d2, index), and its
 //     first k are the row; a tie across the k-th slot goes to the literal
 //     replay.
-// Any proposal gives the reference result; a cube that overflows the
-// buffer, a short proposal, a cube that wraps the box, or an S larger than
-// the sort also fall back to the incremental walk.
-constexpr int kSelectCap = 256;     // candidates per warp buffer (KPL == 1)
-constexpr int kSelectWarps = 8;     // warps per block
+// Any proposal gives the reference result: a short proposal, a buffer
+// overflow, a cube that wraps the box, k > 32 or an S larger than 64 sends
+// the source to the literal replay.
+constexpr int kSelCap = 512;   // FP32-filtered candidates per warp
+constexpr int kSelWarps = 8;   // warps per block
 
-template <int KPL>
-struct SelectShared {
-  float d[kSelectWarps][kSelectCap * KPL];
-  int t[kSelectWarps][kSelectCap * KPL];
-  uint32_t meta[kSelectWarps][kSelectCap * KPL];
-  int bucket[kSelectWarps][32];
+struct __align__(16) SelRow {  // one non-empty row of the cube
+  int excl;                    // first candidate position of the row
+  int startA, lenA;            // sorted range of the cells inside the box
+  int startB;                  // sorted range of the cells wrapped in x
+  int rowbase;                 // local cell id of (0, cy, cz)
+  int meta;                    // dy + 16 | dz + 16 << 5 | wb + 1 << 10 | wc + 1 << 12 | wrapB + 1 << 14
+  float Dx, Dy, Dz;            // dy e_b + dz e_c (FP32)
+  int pad[3];
+};
+
+struct SelShared {
+  float d[kSelCap];
+  int t[kSelCap];
+  uint32_t m[kSelCap];  // shell | wa + 1 << 8 | wb + 1 << 10 | wc + 1 << 12
+  SelRow rows[32];
+  double sd[64];
+  int sj[64];
+  int hist[32];
+  unsigned hmax[32];
 };
 
 __device__ __forceinline__ float band32(double theta, double beta) {
   return __double2float_ru(theta * 8.0 * double(kU32) + beta);
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Gap (cell units) between a source at fraction f of its cell and the cell
+// at offset d along one axis.
+__device__ __forceinline__ float axis_gap(int d, float f) {
+  return d > 0 ? float(d) - f : (d < 0 ? f + float(-d - 1) : 0.f);
+}
+
+// Bitonic sort of 32 (d, j) pairs, one per lane, ascending by (d2, index).
+__device__ __forceinline__ void warp_sort32(double &d, int &j, int lane) {
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const double od = __shfl_xor_sync(kFull, d, stride);
+      const int oj = __shfl_xor_sync(kFull, j, stride);
+      const bool up = (lane & size) == 0 || size == 32;
+      const bool lower = (lane & stride) == 0;
+      const bool take = (lower == up) ? lex_less(od, oj, d, j) : lex_less(d, j, od, oj);
+      if (take) {
+        d = od;
+        j = oj;
+      }
+    }
+  }
 }
 
 // Bitonic sort of 2 * 32 (d, j) pairs held two per lane: element e = s * 32 + lane.
@@ -1007,10 +1056,8 @@ __device__ __forceinline__ void warp_sort64(double (&d)[2], int (&j)[2], int lan
 #pragma unroll
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
       if (stride == 32) {
-        // both partners in this lane: element lane (s = 0) and lane + 32 (s = 1)
-        const bool up = true;  // size == 64: one ascending block
-        const bool swap = up ? lex_less(d[1], j[1], d[0], j[0]) : lex_less(d[0], j[0], d[1], j[1]);
-        if (swap) {
+        // both partners in this lane (size == 64: one ascending block)
+        if (lex_less(d[1], j[1], d[0], j[0])) {
           const double td = d[0];
           const int tj = j[0];
           d[0] = d[1];
@@ -1027,8 +1074,8 @@ __device__ __forceinline__ void warp_sort64(double (&d)[2], int (&j)[2], int lan
         const int oj = __shfl_xor_sync(kFull, j[s], stride);
         const bool up = ((e & size) == 0);
         const bool lower = (e & stride) == 0;
-        const bool other_less = lex_less(od, oj, d[s], j[s]);
-        const bool take = (lower == up) ? other_less : !other_less && !(od == d[s] && oj == j[s]);
+        const bool take =
+            (lower == up) ? lex_less(od, oj, d[s], j[s]) : lex_less(d[s], j[s], od, oj);
         if (take) {
           d[s] = od;
           j[s] = oj;
@@ -1038,23 +1085,23 @@ __device__ __forceinline__ void warp_sort64(double (&d)[2], int (&j)[2], int lan
   }
 }
 
-template <int KPL>
-__device__ bool select_source(const BatchBuffers &b, long long p, int lane, int warp,
-                              LocalCounters &cnt, SelectShared<KPL> &sh) {
+struct SelCounters {
+  unsigned pairs = 0, pruned = 0, rerank = 0;          // per lane
+  unsigned inserts = 0, shells = 0, replays = 0;       // warp-uniform
+  unsigned under = 0, over = 0, exact = 0, fallback = 0;
+};
+
+// One source; false: the source must go to the literal replay.
+__device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelShared &sh,
+                              SelCounters &cnt) {
   const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
   const FrameDesc &fr = b.frames[f];
-  if (b.frame_flags[f] & kFrameNaN) return false;
-  int Rp = b.proposal ? b.proposal[p] : 0;
+  const int Rp = b.proposal[p];
   const int k = fr.k;
   const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
-  if (Rp <= 0 || Rp > 8 || Rp > b.shell_rmax || Rp > fr.max_reach || k > 32) return false;
-  if (2 * Rp + 1 > nx || 2 * Rp + 1 > ny || 2 * Rp + 1 > nz) return false;  // cube wraps the box
-  constexpr int CAP = kSelectCap * KPL;
-  float *bd = sh.d[warp];
-  int *bt = sh.t[warp];
-  uint32_t *bm = sh.meta[warp];
-  int *bk = sh.bucket[warp];
-
+  if ((b.frame_flags[f] & kFrameNaN) || Rp <= 0 || Rp > 8 || Rp > fr.max_reach || k > 32 ||
+      2 * Rp + 1 > nx || 2 * Rp + 1 > ny || 2 * Rp + 1 > nz)
+    return false;
   const uint32_t lc = b.scell[p];
   const int ix = int(lc % uint32_t(nx));
   const int iy = int((lc / uint32_t(nx)) % uint32_t(ny));
@@ -1066,91 +1113,123 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, int 
   const float fa = fr.nhinv[0] * plx + fr.nhinv[1] * ply + fr.nhinv[2] * plz;
   const float fb = fr.nhinv[3] * plx + fr.nhinv[4] * ply + fr.nhinv[5] * plz;
   const float fc = fr.nhinv[6] * plx + fr.nhinv[7] * ply + fr.nhinv[8] * plz;
-  const float lam = float(fr.lam_min) * 0.99f;
+  const float ev0 = fr.ev[0], ev1 = fr.ev[1], ev2 = fr.ev[2];
   const double beta = fp32_beta(fr, Rp);
   const double Bp = stop_bound(Rp, cell_min);
   const float thr = fp32_threshold(Bp, beta);
+  const float qlim = thr / (float(fr.lam_min) * 0.99f) * 1.0001f;
 
   // 1. gather
-  const int E = (2 * Rp + 1) * (2 * Rp + 1) * (2 * Rp + 1);
+  const int W = 2 * Rp + 1;
+  const int nrow = W * W;
   int total = 0;
-  for (int e0 = 0; e0 < E; e0 += 32) {
-    const int e = e0 + lane;
-    int a0 = 0, nc = 0;
-    uint32_t meta = 0;
+  for (int r0 = 0; r0 < nrow; r0 += 32) {
+    const int row = r0 + lane;
+    int lenA = 0, lenB = 0, startA = 0, startB = 0, rowbase = 0, meta = 0;
     float Dx = 0.f, Dy = 0.f, Dz = 0.f;
-    if (e < E) {
-      const uint32_t w = b.shell_table[e];
-      const int dx = int(w & 1023u) - 512, dy = int((w >> 10) & 1023u) - 512,
-                dz = int((w >> 20) & 1023u) - 512;
-      int cx, cy, cz, wa, wb, wc;
-      wrap_axis(ix + dx, nx, cx, wa);
-      wrap_axis(iy + dy, ny, cy, wb);
-      wrap_axis(iz + dz, nz, cz, wc);
-      const long long c = cb + ((long long)cz * ny + cy) * (long long)nx + cx;
-      a0 = int(b.off[c]);
-      nc = int(b.off[c + 1]) - a0;
-      if (nc > 0) {
-        const float ga = dx > 0 ? dx - fa : (dx < 0 ? fa + float(-dx - 1) : 0.f);
-        const float gb = dy > 0 ? dy - fb : (dy < 0 ? fb + float(-dy - 1) : 0.f);
-        const float gc = dz > 0 ? dz - fc : (dz < 0 ? fc + float(-dz - 1) : 0.f);
-        const float ga0 = fmaxf(ga, 0.f), gb0 = fmaxf(gb, 0.f), gc0 = fmaxf(gc, 0.f);
-        if (lam * (ga0 * ga0 + gb0 * gb0 + gc0 * gc0) > thr) {
-          ++cnt.v[kCntPruned];
-          nc = 0;
-        } else {
-          const float fdx = float(dx), fdy = float(dy), fdz = float(dz);
-          Dx = fdx * fr.ev[0] + fdy * fr.ev[3] + fdz * fr.ev[6];
-          Dy = fdx * fr.ev[1] + fdy * fr.ev[4] + fdz * fr.ev[7];
-          Dz = fdx * fr.ev[2] + fdy * fr.ev[5] + fdz * fr.ev[8];
-          const int s = max(1, max(abs(dx), max(abs(dy), abs(dz))));
-          meta = uint32_t(s) | (uint32_t(wa + 1) << 8) | (uint32_t(wb + 1) << 10) |
-                 (uint32_t(wc + 1) << 12);
+    if (row < nrow) {
+      const int dy = row % W - Rp, dz = row / W - Rp;
+      const float gb = fmaxf(axis_gap(dy, fb), 0.f), gc = fmaxf(axis_gap(dz, fc), 0.f);
+      const float Q = qlim - (gb * gb + gc * gc);
+      if (Q >= 0.f) {
+        const float gm = sqrtf(Q) * 1.0001f + 1e-4f;
+        const int dxh = int(floorf(fminf(fa + gm, float(Rp))));
+        const int dxl = -int(floorf(fminf(gm + 1.f - fa, float(Rp))));
+        cnt.pruned += unsigned(W - (dxh - dxl + 1));
+        int cy, wb, cz, wc;
+        wrap_axis(iy + dy, ny, cy, wb);
+        wrap_axis(iz + dz, nz, cz, wc);
+        rowbase = (cz * ny + cy) * nx;
+        const uint32_t *o = b.off + cb + rowbase;
+        const int xl = ix + dxl, xh = ix + dxh;
+        startA = int(o[max(xl, 0)]);
+        lenA = int(o[min(xh, nx - 1) + 1]) - startA;
+        int wrapB = 0;
+        if (xl < 0) {
+          startB = int(o[xl + nx]);
+          lenB = int(o[nx]) - startB;
+          wrapB = -1;
+        } else if (xh >= nx) {
+          startB = int(o[0]);
+          lenB = int(o[xh - nx + 1]) - startB;
+          wrapB = 1;
         }
+        const float fdy = float(dy), fdz = float(dz);
+        Dx = fdy * fr.ev[3] + fdz * fr.ev[6];
+        Dy = fdy * fr.ev[4] + fdz * fr.ev[7];
+        Dz = fdy * fr.ev[5] + fdz * fr.ev[8];
+        meta = (dy + 16) | ((dz + 16) << 5) | ((wb + 1) << 10) | ((wc + 1) << 12) |
+               ((wrapB + 1) << 14);
+      } else {
+        cnt.pruned += unsigned(W);
       }
     }
-    int incl = nc;
+    const int len = lenA + lenB;
+    const unsigned ne = __ballot_sync(kFull, len > 0);
+    if (!ne) continue;
+    int incl = len;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int y = __shfl_up_sync(kFull, incl, o);
       if (lane >= o) incl += y;
     }
     const int tot = __shfl_sync(kFull, incl, 31);
-    const int excl = incl - nc;
+    const int excl = incl - len;
+    __syncwarp();
+    if (len > 0) {
+      SelRow &R = sh.rows[__popc(ne & lanemask_lt())];
+      R.excl = excl;
+      R.startA = startA;
+      R.lenA = lenA;
+      R.startB = startB;
+      R.rowbase = rowbase;
+      R.meta = meta;
+      R.Dx = Dx;
+      R.Dy = Dy;
+      R.Dz = Dz;
+    }
+    __syncwarp();
+    int before = 0;  // non-empty rows that start before the window
     for (int g0 = 0; g0 < tot; g0 += 32) {
+      const unsigned bit =
+          (len > 0 && excl >= g0 && excl < g0 + 32) ? (1u << (excl - g0)) : 0u;
+      const unsigned starts = __reduce_or_sync(kFull, bit);
       const int g = g0 + lane;
-      int owner = 0;
-#pragma unroll
-      for (int step = 16; step > 0; step >>= 1) {
-        const int v = __shfl_sync(kFull, incl, owner + step - 1);
-        if (v <= g) owner += step;
-      }
-      owner &= 31;
-      const int oa0 = __shfl_sync(kFull, a0, owner);
-      const int oex = __shfl_sync(kFull, excl, owner);
-      const uint32_t om = __shfl_sync(kFull, meta, owner);
-      const float oDx = __shfl_sync(kFull, Dx, owner);
-      const float oDy = __shfl_sync(kFull, Dy, owner);
-      const float oDz = __shfl_sync(kFull, Dz, owner);
-      const int t = oa0 + (g - oex);
+      const int owner = before + __popc(starts & (lanemask_lt() | (1u << lane))) - 1;
+      before += __popc(starts);
       bool keep = false;
       float d32 = 0.f;
-      if (g < tot && (long long)t != p) {
-        ++cnt.v[kCntPairs];
-        const float4 q = b.rec[t];
-        const float ex = (q.x - plx) + oDx;
-        const float ey = (q.y - ply) + oDy;
-        const float ez = (q.z - plz) + oDz;
-        d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-        keep = !(d32 > thr);  // beyond the proposed bound: never in the row
+      int t = 0;
+      uint32_t mm = 0;
+      if (g < tot) {
+        const SelRow &R = sh.rows[owner];
+        const int loc = g - R.excl;
+        const bool inA = loc < R.lenA;
+        t = inA ? R.startA + loc : R.startB + (loc - R.lenA);
+        if ((long long)t != p) {
+          ++cnt.pairs;
+          const float4 q = b.rec[t];
+          const int rm = R.meta;
+          const int wa = inA ? 0 : ((rm >> 14) & 3) - 1;
+          const int dx = int(b.scell[t]) - R.rowbase + wa * nx - ix;
+          const float fdx = float(dx);
+          const float ex = (q.x - plx) + fmaf(fdx, ev0, R.Dx);
+          const float ey = (q.y - ply) + fmaf(fdx, ev1, R.Dy);
+          const float ez = (q.z - plz) + fmaf(fdx, ev2, R.Dz);
+          d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+          keep = !(d32 > thr);
+          const int dy = (rm & 31) - 16, dz = ((rm >> 5) & 31) - 16;
+          const int s = max(1, max(abs(dx), max(abs(dy), abs(dz))));
+          mm = uint32_t(s) | (uint32_t(wa + 1) << 8) | (uint32_t((rm >> 10) & 15) << 10);
+        }
       }
       const unsigned km = __ballot_sync(kFull, keep);
-      if (total + __popc(km) > CAP) return false;  // too many candidates for the buffer
+      if (total + __popc(km) > kSelCap) return false;
       if (keep) {
-        const int pos = total + __popc(km & ((1u << lane) - 1u));
-        bd[pos] = d32;
-        bt[pos] = t;
-        bm[pos] = om;
+        const int pos = total + __popc(km & lanemask_lt());
+        sh.d[pos] = d32;
+        sh.t[pos] = t;
+        sh.m[pos] = mm;
       }
       total += __popc(km);
     }
@@ -1159,180 +1238,192 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, int 
 
   const double px = b.sx[p], py = b.sy[p], pz = b.sz[p];
   auto exact = [&](int i) -> double {
-    const int t = bt[i];
-    const uint32_t m = bm[i];
+    const int t = sh.t[i];
+    const uint32_t m = sh.m[i];
     double shx, shy, shz;
     lattice_shift(fr, int((m >> 8) & 3u) - 1, int((m >> 10) & 3u) - 1, int((m >> 12) & 3u) - 1, shx,
                   shy, shz);
     return dist2_shifted(px, py, pz, b.sx[t], b.sy[t], b.sz[t], shx, shy, shz);
   };
 
-  // 2. stop reach: count[R] = #{key <= R}, key = max(shell, b(d))
-  int key_cnt[9];
-#pragma unroll
-  for (int R = 0; R < 9; ++R) key_cnt[R] = 0;
+  // 2. stop reach: key counts packed 16 bits per reach (reaches 1-4 | 5-8)
+  const float inv_c = 1.f / float(cell_min);
+  const float eps_r =
+      band32(Bp, beta) / (2.f * float(cell_min) * float(cell_min)) + 16.f * kU32 * float(Rp + 2);
+  unsigned long long klo = 0, khi = 0;
   for (int i = lane; i < total; i += 32) {
-    const float d32 = bd[i];
-    if (!(d32 < __int_as_float(0x7f800000))) continue;
-    const int s = int(bm[i] & 255u);
-    int bR = Rp + 1;
-    double dex = -1.0;
-    for (int R = 1; R <= Rp; ++R) {
-      const double BR = stop_bound(R, cell_min);
-      const float band = band32(BR, beta);
-      const float hi = __double2float_ru(BR) + 2.f * band;
-      const float lo = __double2float_rd(BR) - band;
-      bool within;
-      if (d32 <= lo) {
-        within = true;
-      } else if (d32 > hi) {
-        within = false;
-      } else {
-        if (dex < 0.0) {
-          dex = exact(i);
-          ++cnt.v[kCntRerank];
-        }
-        within = dex <= BR;
-      }
-      if (within) {
-        bR = R;
-        break;
-      }
+    const float d32 = sh.d[i];
+    const int s = int(sh.m[i] & 255u);
+    const float rr = sqrtf(d32) * inv_c;
+    const float rc = ceilf(rr);
+    int bR;
+    if (rr <= 1.f - eps_r) {
+      bR = 1;
+    } else if (rc - rr < eps_r || rr - (rc - 1.f) < eps_r) {
+      const double dex = exact(i);
+      ++cnt.rerank;
+      int R = max(1, int(rc) - 1);
+      while (R <= Rp && !(dex <= stop_bound(R, cell_min))) ++R;
+      bR = R;
+    } else {
+      bR = int(rc);
     }
     const int key = max(s, bR);
-#pragma unroll
-    for (int R = 1; R <= 8; ++R) key_cnt[R] += (key <= R) ? 1 : 0;
+    if (key <= Rp) {
+      const unsigned long long one = 1ull << (16 * ((key - 1) & 3));
+      if (key <= 4)
+        klo += one;
+      else
+        khi += one;
+    }
   }
+  const unsigned c12 = __reduce_add_sync(kFull, unsigned(klo));
+  const unsigned c34 = __reduce_add_sync(kFull, unsigned(klo >> 32));
+  const unsigned c56 = __reduce_add_sync(kFull, unsigned(khi));
+  const unsigned c78 = __reduce_add_sync(kFull, unsigned(khi >> 32));
   int Rs = 0;
-  for (int R = 1; R <= Rp; ++R) {
-    int c = key_cnt[R];
+  {
+    unsigned cum = 0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
-    if (c >= k) {
-      Rs = R;
-      break;
+    for (int R = 1; R <= 8; ++R) {
+      const unsigned w = R <= 2 ? c12 : (R <= 4 ? c34 : (R <= 6 ? c56 : c78));
+      cum += (R & 1) ? (w & 0xffffu) : (w >> 16);
+      if (Rs == 0 && R <= Rp && cum >= unsigned(k)) Rs = R;
     }
   }
-  if (Rs == 0) {  // proposal too short: the incremental walk takes over
-    if (lane == 0) {
-      ++cnt.v[kCntPropUnder];
-      cnt.v[kCntRevisit] += Rp;
-    }
+  if (Rs == 0) {
+    ++cnt.under;
     return false;
   }
-  if (lane == 0) ++cnt.v[Rs < Rp ? kCntPropOver : kCntPropExact];
-  if (lane == 0) cnt.v[kCntShells] += Rs;
+  if (Rs < Rp)
+    ++cnt.over;
+  else
+    ++cnt.exact;
+  cnt.shells += unsigned(Rs);
 
-  // 3. select: histogram of shells <= R* over [0, B(R*)]
+  // 3. select: two-level histogram over candidates of shells <= R* within B(R*)
   const double Bs = stop_bound(Rs, cell_min);
-  const float Bs32 = float(Bs);
   const float Bs_hi = __double2float_ru(Bs) + 2.f * band32(Bs, beta);
-  bk[lane] = 0;
+  const float scale = 32.f / Bs_hi;
+  sh.hist[lane] = 0;
+  sh.hmax[lane] = 0u;
   __syncwarp();
   for (int i = lane; i < total; i += 32) {
-    const float d32 = bd[i];
-    if (int(bm[i] & 255u) > Rs || !(d32 <= Bs_hi)) continue;
-    const float x = fminf(d32 / Bs32, 1.f);
-    const int bucket = min(31, int(32.f * x * sqrtf(x)));
-    atomicAdd(&bk[bucket], 1);
+    const float d32 = sh.d[i];
+    if (int(sh.m[i] & 255u) <= Rs && d32 <= Bs_hi) atomicAdd(&sh.hist[min(31, int(d32 * scale))], 1);
   }
   __syncwarp();
-  int c = bk[lane];
-  int incl = c;
+  int bstar, need;
+  {
+    const int c = sh.hist[lane];
+    int incl = c;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(kFull, incl, o);
-    if (lane >= o) incl += y;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const unsigned reach = __ballot_sync(kFull, incl >= k);
+    if (!reach) return false;  // cannot happen: R* guarantees k candidates within B(R*)
+    bstar = __ffs(reach) - 1;
+    need = k - (__shfl_sync(kFull, incl, bstar) - __shfl_sync(kFull, c, bstar));
   }
-  const unsigned reach = __ballot_sync(kFull, incl >= k);
-  if (!reach) return false;  // cannot happen: R* guarantees k candidates within B(R*)
-  const int bstar = __ffs(reach) - 1;
-  // T = the largest d32 in buckets <= bstar
-  float T = 0.f;
+  __syncwarp();
+  sh.hist[lane] = 0;
+  __syncwarp();
   for (int i = lane; i < total; i += 32) {
-    const float d32 = bd[i];
-    if (int(bm[i] & 255u) > Rs || !(d32 <= Bs_hi)) continue;
-    const float x = fminf(d32 / Bs32, 1.f);
-    const int bucket = min(31, int(32.f * x * sqrtf(x)));
-    if (bucket <= bstar) T = fmaxf(T, d32);
+    const float d32 = sh.d[i];
+    if (int(sh.m[i] & 255u) > Rs || !(d32 <= Bs_hi)) continue;
+    const float x = d32 * scale;
+    if (min(31, int(x)) != bstar) continue;
+    const int sub = min(31, int((x - float(bstar)) * 32.f));
+    atomicAdd(&sh.hist[sub], 1);
+    atomicMax(&sh.hmax[sub], __float_as_uint(d32));
   }
+  __syncwarp();
+  float T;
+  {
+    const int c = sh.hist[lane];
+    int incl = c;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) T = fmaxf(T, __shfl_xor_sync(kFull, T, o));
-  const float TS = T + 3.f * band32(double(T), beta);
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const unsigned reach = __ballot_sync(kFull, incl >= need);
+    if (!reach) return false;  // cannot happen
+    const int b2 = __ffs(reach) - 1;
+    // buckets below bstar hold smaller values than every value of bstar
+    T = __uint_as_float(__reduce_max_sync(kFull, lane <= b2 ? sh.hmax[lane] : 0u));
+  }
+  const float TS = fminf(T + 3.f * band32(double(T), beta), Bs_hi);
 
-  // S = shells <= R*, d32 <= TS, compacted into two slots per lane
-  // (position q: lane q % 32, slot q / 32)
-  double sd[2] = {pinf(), pinf()};
-  int sj[2] = {0x7fffffff, 0x7fffffff};
+  // S = shells <= R*, d32 <= TS, staged in shared memory in candidate order
   int nS = 0;
   for (int i0 = 0; i0 < total; i0 += 32) {
     const int i = i0 + lane;
-    bool in = false;
-    if (i < total) in = int(bm[i] & 255u) <= Rs && bd[i] <= TS;
+    const bool in = i < total && int(sh.m[i] & 255u) <= Rs && sh.d[i] <= TS;
     const unsigned m = __ballot_sync(kFull, in);
-    const int cntm = __popc(m);
-    if (cntm == 0) continue;
-    if (nS + cntm > 64) return false;  // S larger than the sort
-    double dd = 0.0;
-    int jj = 0;
+    if (nS + __popc(m) > 64) return false;  // S larger than the sort
     if (in) {
-      dd = exact(i);
-      jj = b.sidx[bt[i]];
+      const int q = nS + __popc(m & lanemask_lt());
+      sh.sd[q] = exact(i);
+      sh.sj[q] = b.sidx[sh.t[i]];
     }
-    // this round fills positions nS .. nS + cntm - 1; lane L takes position
-    // nS + ((L - nS) & 31) from the source lane holding the r-th set bit
-    const int r = (lane - nS) & 31;
-    const int src = r < cntm ? int(__fns(m, 0, r + 1)) : lane;
-    const double vd = shfl_d(dd, src);
-    const int vj = __shfl_sync(kFull, jj, src);
-    if (r < cntm) {
-      const int q = nS + r;
-      if (q < 32) {
-        sd[0] = vd;
-        sj[0] = vj;
-      } else {
-        sd[1] = vd;
-        sj[1] = vj;
-      }
-    }
-    nS += cntm;
+    nS += __popc(m);
   }
-  if (lane == 0) cnt.v[kCntRerank] += nS;
-  warp_sort64(sd, sj, lane);
-
-  // 4. tie across the k-th slot: (k-1)-th and k-th sorted values
-  const double vk = __shfl_sync(kFull, sd[(k - 1) >> 5], (k - 1) & 31);
-  const double vn = k < 64 ? __shfl_sync(kFull, sd[k >> 5], k & 31) : pinf();
-  if (nS > k && vn == vk) {
-    if (lane == 0) {
-      push_replay(b, p);
-      ++cnt.v[kCntReplays];
-    }
-    return true;
-  }
-  if (b.stop_log && lane == 0) b.stop_log[p] = int8_t(Rs);
+  __syncwarp();
+  if (nS < k) return false;  // cannot happen: T bounds k candidates
+  if (lane == 0) cnt.rerank += unsigned(nS);
   const int i = b.sidx[p];
   int *row = b.out_nn + fr.out_base + (long long)i * k;
   double *drow = b.out_d2 ? b.out_d2 + fr.out_base + (long long)i * k : nullptr;
+  if (nS <= 32) {
+    double d = lane < nS ? sh.sd[lane] : pinf();
+    int j = lane < nS ? sh.sj[lane] : 0x7fffffff;
+    warp_sort32(d, j, lane);
+    // 4. a tie across the k-th slot: (k-1)-th and k-th sorted values
+    const double vk = __shfl_sync(kFull, d, k - 1);
+    const double vn = __shfl_sync(kFull, d, k & 31);
+    if (nS > k && vn == vk) {
+      ++cnt.replays;
+      return false;
+    }
+    if (lane < k) {
+      row[lane] = j;
+      if (drow) drow[lane] = d;
+    }
+  } else {
+    double sd[2];
+    int sj[2];
 #pragma unroll
-  for (int s = 0; s < 2; ++s) {
-    const int pos = s * 32 + lane;
-    if (pos < k) {
-      row[pos] = sj[s];
-      if (drow) drow[pos] = sd[s];
+    for (int s = 0; s < 2; ++s) {
+      const int q = s * 32 + lane;
+      sd[s] = q < nS ? sh.sd[q] : pinf();
+      sj[s] = q < nS ? sh.sj[q] : 0x7fffffff;
+    }
+    warp_sort64(sd, sj, lane);
+    const double vk = __shfl_sync(kFull, sd[(k - 1) >> 5], (k - 1) & 31);
+    const double vn = __shfl_sync(kFull, sd[k >> 5], k & 31);
+    if (nS > k && vn == vk) {
+      ++cnt.replays;
+      return false;
+    }
+    if (lane < k) {
+      row[lane] = sj[0];
+      if (drow) drow[lane] = sd[0];
     }
   }
-  if (lane == 0) cnt.v[kCntInserts] += k;
+  if (b.stop_log && lane == 0) b.stop_log[p] = int8_t(Rs);
+  cnt.inserts += unsigned(k);
   return true;
 }
 
-template <int KPL>
-__global__ void __launch_bounds__(kSelectWarps * 32, 2) k_select_walk(BatchBuffers b) {
-  __shared__ SelectShared<KPL> sh;
+__global__ void __launch_bounds__(kSelWarps * 32, 2) k_select_walk(BatchBuffers b) {
+  extern __shared__ __align__(16) unsigned char sel_smem[];
+  SelShared &sh = reinterpret_cast<SelShared *>(sel_smem)[threadIdx.x >> 5];
   const long long total = b.off[b.ncells];
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  LocalCounters cnt;
+  SelCounters cnt;
   constexpr int kGrab = 4;
   for (;;) {
     uint32_t base = 0;
@@ -1342,15 +1433,34 @@ __global__ void __launch_bounds__(kSelectWarps * 32, 2) k_select_walk(BatchBuffe
     for (int q = 0; q < kGrab; ++q) {
       const long long p = (long long)base + q;
       if (p >= total) break;
-      if (!select_source<KPL>(b, p, lane, warp, cnt, sh))
-        team_source<kModeFastF32, KPL>(b, p, lane, cnt);
+      const unsigned tie = cnt.replays;
+      if (!select_source(b, p, lane, sh, cnt)) {
+        if (cnt.replays == tie) ++cnt.fallback;
+        if (lane == 0) push_replay(b, p);
+      }
       __syncwarp();
     }
   }
-  flush_counters(b, cnt);
+  const unsigned pairs = __reduce_add_sync(kFull, cnt.pairs);
+  const unsigned pruned = __reduce_add_sync(kFull, cnt.pruned);
+  const unsigned rerank = __reduce_add_sync(kFull, cnt.rerank);
+  if (lane == 0) {
+    unsigned long long *c = reinterpret_cast<unsigned long long *>(b.counters);
+    atomicAdd(&c[kCntPairs], pairs);
+    atomicAdd(&c[kCntPruned], pruned);
+    atomicAdd(&c[kCntRerank], rerank);
+    atomicAdd(&c[kCntInserts], cnt.inserts);
+    atomicAdd(&c[kCntShells], cnt.shells);
+    atomicAdd(&c[kCntReplays], cnt.replays + cnt.fallback);
+    atomicAdd(&c[kCntPropUnder], cnt.under);
+    atomicAdd(&c[kCntPropOver], cnt.over);
+    atomicAdd(&c[kCntPropExact], cnt.exact);
+    atomicAdd(&c[kCntFallback], cnt.fallback);
+  }
 }
 
-// ------------------------------------------------------------------------
+size_t select_smem_bytes() { return sizeof(SelShared) * kSelWarps; }
+
 // Warp-parallel literal replay of the reference heap for one source (finite
 // coordinates). The warp evaluates the reference visit sequence 32
 // candidates at a time -- shells ascending, offsets in lexicographic order
@@ -1741,12 +1851,16 @@ cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t
     k_queue_all<<<sm_count() * 4, 256, 0, s>>>(b);
     return cudaGetLastError();
   }
-  if (w.tpp == 32 && w.mode == kModeLearned && b.kmax <= 32 && b.proposal && b.shell_table) {
+  if (w.tpp == 32 && w.mode == kModeLearned && b.kmax <= 32 && b.proposal) {
+    const size_t smem = select_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(k_select_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(smem));
+    if (e != cudaSuccess) return e;
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk<1>, kSelectWarps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk, kSelWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
     const int grid = w.grid > 0 ? w.grid : sm_count() * per_sm;
-    k_select_walk<1><<<grid, kSelectWarps * 32, 0, s>>>(b);
+    k_select_walk<<<grid, kSelWarps * 32, smem, s>>>(b);
     return cudaGetLastError();
   }
   if (w.tpp == 32 && b.kmax <= 256) {

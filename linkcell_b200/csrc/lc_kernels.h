@@ -64,6 +64,7 @@ enum WalkCounters : int {
   kCntPropOver = 7,   // learned proposal too long
   kCntPropExact = 8,  // learned proposal equal to the settled shell
   kCntRevisit = 9,    // shells walked again after a short proposal
+  kCntFallback = 10,  // cube-select sources sent to the literal replay (not ties)
   kNumCounters = 16
 };
 

@@ -52,8 +52,8 @@ def test_graph_replay_follows_new_cells(gpu, lib, oracle_mod, mode):
         buf = Fixed(lib, ws, n, k)
         for step in range(4):
             L = 14.0 + step
-            cell = [L, 0.3, -0.2, 0.0, L - 1.0, 0.4, 0.0, 0.0, L + 0.5]
-            xyz = (rng.random((n, 3)) @ np.asarray(cell).reshape(3, 3))
+            cell = np.array([[L, 0.3, -0.2], [0.0, L - 1.0, 0.4], [0.0, 0.0, L + 0.5]])
+            xyz = rng.random((n, 3)) @ cell
             want = oracle_mod.knearest(xyz, cell, k)
             assert_same(buf.run(xyz, cell), want, f"graph step {step}")
         assert lib.lc_gpu_graph_captures(ws) == 1
