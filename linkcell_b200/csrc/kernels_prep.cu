@@ -181,45 +181,22 @@ __global__ void __launch_bounds__(kScanBlock)
   if (base <= ncells - 1 && ncells - 1 < base + kScanItems) off[ncells] = run;
 }
 
-// Arrival slots: tmp[off[c] + arank[g]] = g.
+// Arrival slots: tmp[off[c] + arank[g]] = g. The output rows of masked
+// points are filled here with -1 / NaN (src/knearest.rs:293-296).
 __global__ void __launch_bounds__(256)
-    k_place_slots(const uint32_t *__restrict__ cell_of, const uint32_t *__restrict__ arank,
+    k_place_slots(const FrameDesc *__restrict__ frames, int nframes,
+                  const uint32_t *__restrict__ cell_of, const uint32_t *__restrict__ arank,
                   const uint32_t *__restrict__ off, uint32_t *__restrict__ tmp, long long npts,
-                  long long ncells, int *__restrict__ status) {
+                  long long ncells, int *__restrict__ out_nn, double *__restrict__ out_d2,
+                  int *__restrict__ status) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long total = off[ncells];
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += stride) {
-    const uint32_t c = cell_of[g];
-    if (c == kInactive) continue;
-    const long long pos = (long long)off[c] + arank[g];
-    if (pos >= total || c >= ncells) {
-      atomicOr(status, kStatusBadIndex);
-      continue;
-    }
-    tmp[pos] = uint32_t(g);
-  }
-}
-
-// Stable placement: a point's slot in its cell is the number of points of
-// the same cell with a smaller id. Writes the sorted SoA records and fills
-// the output rows of masked points with -1 / NaN (src/knearest.rs:293-296).
-__global__ void __launch_bounds__(256)
-    k_place_records(const double *__restrict__ xyz, const FrameDesc *__restrict__ frames,
-                    int nframes, long long npts, long long ncells,
-                    const uint32_t *__restrict__ cell_of, const uint32_t *__restrict__ off,
-                    const uint32_t *__restrict__ tmp, double *__restrict__ sx,
-                    double *__restrict__ sy, double *__restrict__ sz, int *__restrict__ sidx,
-                    uint32_t *__restrict__ scell, float4 *__restrict__ rec,
-                    int *__restrict__ out_nn, double *__restrict__ out_d2,
-                    int *__restrict__ status) {
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  const long long total = off[ncells];
-  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += stride) {
-    const int f = nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
-    const FrameDesc &fr = frames[f];
-    const long long i = g - fr.pt_base;
     const uint32_t c = cell_of[g];
     if (c == kInactive) {
+      const int f = nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
+      const FrameDesc &fr = frames[f];
+      const long long i = g - fr.pt_base;
       int *row = out_nn + fr.out_base + i * fr.k;
       for (int s = 0; s < fr.k; ++s) row[s] = -1;
       if (out_d2) {
@@ -229,27 +206,60 @@ __global__ void __launch_bounds__(256)
       }
       continue;
     }
+    const long long pos = (long long)off[c] + arank[g];
+    if (pos >= total || c >= ncells) {
+      atomicOr(status, kStatusBadIndex);
+      continue;
+    }
+    tmp[pos] = uint32_t(g);
+  }
+}
+
+// Stable placement, one thread per sorted slot: the point g arriving at
+// slot pos of cell c lands at off[c] + (number of points of c with a
+// smaller id), so the order inside a cell is by point id (the reference
+// bins points in id order). The reads of g's coordinates are gathers; the
+// writes of the sorted SoA records stay within the cell's few slots, so a
+// warp's stores remain coalesced.
+__global__ void __launch_bounds__(256)
+    k_place_records(const double *__restrict__ xyz, const FrameDesc *__restrict__ frames,
+                    int nframes, long long npts, long long ncells,
+                    const uint32_t *__restrict__ cell_of, const uint32_t *__restrict__ off,
+                    const uint32_t *__restrict__ tmp, double *__restrict__ sx,
+                    double *__restrict__ sy, double *__restrict__ sz, int *__restrict__ sidx,
+                    uint32_t *__restrict__ scell, float4 *__restrict__ rec,
+                    int *__restrict__ status) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long total = off[ncells];
+  for (long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x; pos < total;
+       pos += stride) {
+    const uint32_t g = tmp[pos];
+    const uint32_t c = (long long)g < npts ? cell_of[g] : kInactive;
     if (c >= ncells) {
       atomicOr(status, kStatusBadIndex);
       continue;
     }
-    const uint32_t a = off[c], b = off[c + 1];
+    const uint32_t a = off[c], e = off[c + 1];
     uint32_t r = 0;
-    for (uint32_t q = a; q < b; ++q) r += tmp[q] < uint32_t(g) ? 1u : 0u;
-    const long long pos = (long long)a + r;
-    if (pos >= total) {
+    for (uint32_t q = a; q < e; ++q) r += tmp[q] < g ? 1u : 0u;
+    const long long dst = (long long)a + r;
+    if (dst >= (long long)e) {
       atomicOr(status, kStatusBadIndex);
       continue;
     }
+    const int f = nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
+    const FrameDesc &fr = frames[f];
     double s0, s1, s2, q0, q1, q2;
-    fractional(fr, xyz[3 * g + 0], xyz[3 * g + 1], xyz[3 * g + 2], s0, s1, s2);
+    fractional(fr, xyz[3 * (long long)g + 0], xyz[3 * (long long)g + 1], xyz[3 * (long long)g + 2],
+               s0, s1, s2);
     cartesian(fr, s0, s1, s2, q0, q1, q2);
-    sx[pos] = q0;
-    sy[pos] = q1;
-    sz[pos] = q2;
-    sidx[pos] = int(i);
+    sx[dst] = q0;
+    sy[dst] = q1;
+    sz[dst] = q2;
+    const int i = int((long long)g - fr.pt_base);
+    sidx[dst] = i;
     const uint32_t lc = uint32_t(c - fr.cell_base);
-    scell[pos] = lc;
+    scell[dst] = lc;
     // FP32 offset from the lower cell corner H (c / n) + origin.
     const int cx = int(lc % uint32_t(fr.nx));
     const int cy = int((lc / uint32_t(fr.nx)) % uint32_t(fr.ny));
@@ -258,7 +268,7 @@ __global__ void __launch_bounds__(256)
     const double c0 = fr.h[0] * f0 + fr.h[3] * f1 + fr.h[6] * f2 + fr.origin[0];
     const double c1 = fr.h[1] * f0 + fr.h[4] * f1 + fr.h[7] * f2 + fr.origin[1];
     const double c2 = fr.h[2] * f0 + fr.h[5] * f1 + fr.h[8] * f2 + fr.origin[2];
-    rec[pos] = make_float4(float(q0 - c0), float(q1 - c1), float(q2 - c2), __int_as_float(int(i)));
+    rec[dst] = make_float4(float(q0 - c0), float(q1 - c1), float(q2 - c2), __int_as_float(i));
   }
 }
 
@@ -303,12 +313,12 @@ cudaError_t launch_scan(const BatchBuffers &b, cudaStream_t s) {
 cudaError_t launch_place(const BatchBuffers &b, cudaStream_t s) {
   if (b.npts <= 0) return cudaSuccess;
   const int g = grid_for(b.npts, 256);
-  k_place_slots<<<g, 256, 0, s>>>(b.cell_of, b.arank, b.off, b.tmp, b.npts, b.ncells, b.status);
+  k_place_slots<<<g, 256, 0, s>>>(b.frames, b.nframes, b.cell_of, b.arank, b.off, b.tmp, b.npts,
+                                  b.ncells, b.out_nn, b.out_d2, b.status);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_place_records<<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.npts, b.ncells, b.cell_of, b.off,
-                                    b.tmp, b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec, b.out_nn,
-                                    b.out_d2, b.status);
+                                    b.tmp, b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec, b.status);
   return cudaGetLastError();
 }
 

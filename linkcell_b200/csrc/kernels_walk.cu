@@ -996,11 +996,11 @@ constexpr int kSelWarps = 8;   // warps per block
 struct __align__(16) SelRow {  // one non-empty row of the cube
   int excl;                    // first candidate position of the row
   int startA, lenA;            // sorted range of the cells inside the box
-  int startB;                  // sorted range of the cells wrapped in x
-  int rowbase;                 // local cell id of (0, cy, cz)
-  int meta;                    // dy + 16 | dz + 16 << 5 | wb + 1 << 10 | wc + 1 << 12 | wrapB + 1 << 14
+  int startB;                  // sorted range of the cells wrapped in x, minus lenA
+  int xoffA, xoffB;            // dx = scell + xoff (A: no x wrap, B: wrapped)
+  int metaA, metaB;            // wrap counts of a candidate (A / B) in SelShared::m layout
   float Dx, Dy, Dz;            // dy e_b + dz e_c (FP32)
-  int pad[3];
+  int syz;                     // max(1, |dy|, |dz|)
 };
 
 struct SelShared {
@@ -1091,6 +1091,14 @@ struct SelCounters {
   unsigned under = 0, over = 0, exact = 0, fallback = 0;
 };
 
+// Exact quotient of x by n from a double reciprocal estimate (x < 2^32).
+__device__ __forceinline__ uint32_t quot(uint32_t x, uint32_t n, double inv) {
+  uint32_t q = uint32_t(__double2uint_rz(double(x) * inv));
+  if (q * n > x) --q;
+  else if ((q + 1) * n <= x) ++q;
+  return q;
+}
+
 // One source; false: the source must go to the literal replay.
 __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelShared &sh,
                               SelCounters &cnt) {
@@ -1103,9 +1111,11 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
       2 * Rp + 1 > nx || 2 * Rp + 1 > ny || 2 * Rp + 1 > nz)
     return false;
   const uint32_t lc = b.scell[p];
-  const int ix = int(lc % uint32_t(nx));
-  const int iy = int((lc / uint32_t(nx)) % uint32_t(ny));
-  const int iz = int(lc / (uint32_t(nx) * uint32_t(ny)));
+  const uint32_t qy = quot(lc, uint32_t(nx), fr.inv_nx);
+  const uint32_t iz_ = quot(lc, uint32_t(nx) * uint32_t(ny), fr.inv_nxy);
+  const int ix = int(lc - qy * uint32_t(nx));
+  const int iy = int(qy - iz_ * uint32_t(ny));
+  const int iz = int(iz_);
   const long long cb = fr.cell_base;
   const double cell_min = fr.cell_min;
   const float4 r = b.rec[p];
@@ -1114,21 +1124,21 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   const float fb = fr.nhinv[3] * plx + fr.nhinv[4] * ply + fr.nhinv[5] * plz;
   const float fc = fr.nhinv[6] * plx + fr.nhinv[7] * ply + fr.nhinv[8] * plz;
   const float ev0 = fr.ev[0], ev1 = fr.ev[1], ev2 = fr.ev[2];
-  const double beta = fp32_beta(fr, Rp);
-  const double Bp = stop_bound(Rp, cell_min);
-  const float thr = fp32_threshold(Bp, beta);
-  const float qlim = thr / (float(fr.lam_min) * 0.99f) * 1.0001f;
+  const float thr = fr.sel_thr[Rp];
+  const float qlim = fr.sel_qlim[Rp];
 
   // 1. gather
   const int W = 2 * Rp + 1;
+  const float invW = 1.f / float(W);
   const int nrow = W * W;
   int total = 0;
   for (int r0 = 0; r0 < nrow; r0 += 32) {
     const int row = r0 + lane;
-    int lenA = 0, lenB = 0, startA = 0, startB = 0, rowbase = 0, meta = 0;
-    float Dx = 0.f, Dy = 0.f, Dz = 0.f;
+    int lenA = 0, lenB = 0;
+    SelRow rw;
     if (row < nrow) {
-      const int dy = row % W - Rp, dz = row / W - Rp;
+      const int qz = int((float(row) + 0.5f) * invW);  // exact: row < 289, W <= 17
+      const int dy = row - qz * W - Rp, dz = qz - Rp;
       const float gb = fmaxf(axis_gap(dy, fb), 0.f), gc = fmaxf(axis_gap(dz, fc), 0.f);
       const float Q = qlim - (gb * gb + gc * gc);
       if (Q >= 0.f) {
@@ -1136,30 +1146,36 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
         const int dxh = int(floorf(fminf(fa + gm, float(Rp))));
         const int dxl = -int(floorf(fminf(gm + 1.f - fa, float(Rp))));
         cnt.pruned += unsigned(W - (dxh - dxl + 1));
-        int cy, wb, cz, wc;
-        wrap_axis(iy + dy, ny, cy, wb);
-        wrap_axis(iz + dz, nz, cz, wc);
-        rowbase = (cz * ny + cy) * nx;
+        int cy = iy + dy, wb = 0, cz = iz + dz, wc = 0;
+        if (cy < 0) { cy += ny; wb = -1; } else if (cy >= ny) { cy -= ny; wb = 1; }
+        if (cz < 0) { cz += nz; wc = -1; } else if (cz >= nz) { cz -= nz; wc = 1; }
+        const int rowbase = (cz * ny + cy) * nx;
         const uint32_t *o = b.off + cb + rowbase;
         const int xl = ix + dxl, xh = ix + dxh;
-        startA = int(o[max(xl, 0)]);
-        lenA = int(o[min(xh, nx - 1) + 1]) - startA;
-        int wrapB = 0;
+        rw.startA = int(o[max(xl, 0)]);
+        lenA = int(o[min(xh, nx - 1) + 1]) - rw.startA;
+        int wrapB = 0, sB = 0;
         if (xl < 0) {
-          startB = int(o[xl + nx]);
-          lenB = int(o[nx]) - startB;
+          sB = int(o[xl + nx]);
+          lenB = int(o[nx]) - sB;
           wrapB = -1;
         } else if (xh >= nx) {
-          startB = int(o[0]);
-          lenB = int(o[xh - nx + 1]) - startB;
+          sB = int(o[0]);
+          lenB = int(o[xh - nx + 1]) - sB;
           wrapB = 1;
         }
+        rw.lenA = lenA;
+        rw.startB = sB - lenA;
+        rw.xoffA = -rowbase - ix;
+        rw.xoffB = -rowbase - ix + wrapB * nx;
+        const int wbc = ((wb + 1) << 10) | ((wc + 1) << 12);
+        rw.metaA = (1 << 8) | wbc;
+        rw.metaB = ((wrapB + 1) << 8) | wbc;
         const float fdy = float(dy), fdz = float(dz);
-        Dx = fdy * fr.ev[3] + fdz * fr.ev[6];
-        Dy = fdy * fr.ev[4] + fdz * fr.ev[7];
-        Dz = fdy * fr.ev[5] + fdz * fr.ev[8];
-        meta = (dy + 16) | ((dz + 16) << 5) | ((wb + 1) << 10) | ((wc + 1) << 12) |
-               ((wrapB + 1) << 14);
+        rw.Dx = fdy * fr.ev[3] + fdz * fr.ev[6];
+        rw.Dy = fdy * fr.ev[4] + fdz * fr.ev[7];
+        rw.Dz = fdy * fr.ev[5] + fdz * fr.ev[8];
+        rw.syz = max(1, max(abs(dy), abs(dz)));
       } else {
         cnt.pruned += unsigned(W);
       }
@@ -1177,16 +1193,8 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
     const int excl = incl - len;
     __syncwarp();
     if (len > 0) {
-      SelRow &R = sh.rows[__popc(ne & lanemask_lt())];
-      R.excl = excl;
-      R.startA = startA;
-      R.lenA = lenA;
-      R.startB = startB;
-      R.rowbase = rowbase;
-      R.meta = meta;
-      R.Dx = Dx;
-      R.Dy = Dy;
-      R.Dz = Dz;
+      rw.excl = excl;
+      sh.rows[__popc(ne & lanemask_lt())] = rw;
     }
     __syncwarp();
     int before = 0;  // non-empty rows that start before the window
@@ -1205,22 +1213,18 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
         const SelRow &R = sh.rows[owner];
         const int loc = g - R.excl;
         const bool inA = loc < R.lenA;
-        t = inA ? R.startA + loc : R.startB + (loc - R.lenA);
+        t = (inA ? R.startA : R.startB) + loc;
         if ((long long)t != p) {
           ++cnt.pairs;
           const float4 q = b.rec[t];
-          const int rm = R.meta;
-          const int wa = inA ? 0 : ((rm >> 14) & 3) - 1;
-          const int dx = int(b.scell[t]) - R.rowbase + wa * nx - ix;
+          const int dx = int(b.scell[t]) + (inA ? R.xoffA : R.xoffB);
           const float fdx = float(dx);
           const float ex = (q.x - plx) + fmaf(fdx, ev0, R.Dx);
           const float ey = (q.y - ply) + fmaf(fdx, ev1, R.Dy);
           const float ez = (q.z - plz) + fmaf(fdx, ev2, R.Dz);
           d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
           keep = !(d32 > thr);
-          const int dy = (rm & 31) - 16, dz = ((rm >> 5) & 31) - 16;
-          const int s = max(1, max(abs(dx), max(abs(dy), abs(dz))));
-          mm = uint32_t(s) | (uint32_t(wa + 1) << 8) | (uint32_t((rm >> 10) & 15) << 10);
+          mm = uint32_t(max(abs(dx), R.syz)) | uint32_t(inA ? R.metaA : R.metaB);
         }
       }
       const unsigned km = __ballot_sync(kFull, keep);
@@ -1248,8 +1252,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
 
   // 2. stop reach: key counts packed 16 bits per reach (reaches 1-4 | 5-8)
   const float inv_c = 1.f / float(cell_min);
-  const float eps_r =
-      band32(Bp, beta) / (2.f * float(cell_min) * float(cell_min)) + 16.f * kU32 * float(Rp + 2);
+  const float eps_r = fr.sel_epsr[Rp];
   unsigned long long klo = 0, khi = 0;
   for (int i = lane; i < total; i += 32) {
     const float d32 = sh.d[i];
@@ -1302,8 +1305,8 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   cnt.shells += unsigned(Rs);
 
   // 3. select: two-level histogram over candidates of shells <= R* within B(R*)
-  const double Bs = stop_bound(Rs, cell_min);
-  const float Bs_hi = __double2float_ru(Bs) + 2.f * band32(Bs, beta);
+  const float Bs_hi = fr.sel_bhi[Rs];
+  const float beta_s = fr.sel_beta[Rs];  // candidates of shells <= R* have offsets <= R*
   const float scale = 32.f / Bs_hi;
   sh.hist[lane] = 0;
   sh.hmax[lane] = 0u;
@@ -1355,7 +1358,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
     // buckets below bstar hold smaller values than every value of bstar
     T = __uint_as_float(__reduce_max_sync(kFull, lane <= b2 ? sh.hmax[lane] : 0u));
   }
-  const float TS = fminf(T + 3.f * band32(double(T), beta), Bs_hi);
+  const float TS = fminf(__fadd_ru(T, __fmul_ru(3.f, __fmaf_ru(T, 8.f * kU32, beta_s))), Bs_hi);
 
   // S = shells <= R*, d32 <= TS, staged in shared memory in candidate order
   int nS = 0;
@@ -1418,13 +1421,13 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   return true;
 }
 
-__global__ void __launch_bounds__(kSelWarps * 32, 2) k_select_walk(BatchBuffers b) {
+__global__ void __launch_bounds__(kSelWarps * 32, 3) k_select_walk(BatchBuffers b) {
   extern __shared__ __align__(16) unsigned char sel_smem[];
   SelShared &sh = reinterpret_cast<SelShared *>(sel_smem)[threadIdx.x >> 5];
   const long long total = b.off[b.ncells];
   const int lane = threadIdx.x & 31;
   SelCounters cnt;
-  constexpr int kGrab = 4;
+  constexpr int kGrab = 16;  // consecutive sources share most candidates (L1 reuse)
   for (;;) {
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(b.work, uint32_t(kGrab));

@@ -44,12 +44,11 @@ cudaError_t mlp_grad(const float *params, const float *X, const int *y, int B, M
                      float *grad, float *loss, cudaStream_t s);
 cudaError_t mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr,
                      cudaStream_t s);
-// Proposed shell per non-empty cell (tensor-core inference over the list
-// of non-empty cells; cell_list holds up to ncells ids), then per sorted
-// source.
+// Proposed shell per occupied cell (tensor-core inference over 16-cell row
+// tiles, the first layer as a 5x5x5 convolution of the occupancy grid),
+// then per sorted source.
 cudaError_t mlp_propose(const float *params, const BatchBuffers &b, int8_t *cell_prop,
-                        int8_t *source_prop, float tau, uint32_t *cell_list, uint32_t *list_count,
-                        cudaStream_t s);
+                        int8_t *source_prop, float tau, cudaStream_t s);
 // Training rows from a logged search: features of the cell of every
 // stride-th sorted source and its settled shell class (min(R*, 8) - 1).
 cudaError_t mlp_training_rows(const BatchBuffers &b, const int8_t *stop_log, long long stride,

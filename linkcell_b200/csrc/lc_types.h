@@ -58,6 +58,17 @@ struct FrameDesc {
   long long cell_base;  // first cell of the frame in the batch
   long long out_base;   // first output element (row 0, slot 0)
   long long mask_base;  // offset of the frame's mask (shared masks repeat 0)
+  long long row_tile_base;  // first 16-cell row tile of the frame (shell proposals)
+  // Cube select walk, per reach R = 1..8 (index R): the FP32 filter at
+  // B(R) = (R cell_min)^2, the row-trimming limit thr / (0.99 lam_min), the
+  // FP32 error offset beta (rounded up), B(R) + 2 band(B(R)) rounded up,
+  // and the error band of sqrt(d32) / cell_min near an integer.
+  float sel_thr[9];
+  float sel_qlim[9];
+  float sel_beta[9];
+  float sel_bhi[9];
+  float sel_epsr[9];
+  double inv_nx, inv_nxy;  // 1 / nx, 1 / (nx ny) for exact quotient estimates
 };
 
 // ------------------------------------------------------------ exact FP64

@@ -8,10 +8,11 @@
 //   - forward (k_dense: tiled FP32 GEMM with bias and optional SiLU),
 //     softmax cross-entropy, backward (GEMMs for input and weight
 //     gradients, SiLU derivative), and Adam;
-//   - k_cell_proposal_tc: inference per non-empty cell on the tensor cores
-//     (mma.sync TF32, FP32 accumulation), writing the proposed shell of
-//     every cell (the smallest R with P(settled shell <= R) >= tau); the
-//     walk reads it for each source.
+//   - k_cell_proposal_tc: inference over 16-cell row tiles on the tensor
+//     cores (mma.sync TF32, FP32 accumulation; layer 1 as a 5x5x5
+//     convolution of the staged occupancy halo), writing the proposed shell
+//     of every occupied cell (the smallest R with P(settled shell <= R) >=
+//     tau); the walk reads it for each source.
 //
 // Parameter layout (floats): W1[64][126] b1[64] W2[64][64] b2[64]
 // W3[8][64] b3[8].
@@ -251,21 +252,30 @@ __global__ void k_training_rows(BatchBuffers b, const int8_t *__restrict__ stop_
 
 // ---------------------------------------------------------------------
 // Tensor-core inference: mma.sync m16n8k8 TF32 (FP32 accumulate). One warp
-// evaluates 16 cells at a time: layer 1 is [16 x 128] x [128 x 64] (126
-// features padded with zeros), layer 2 [16 x 64] x [64 x 64], layer 3
-// [16 x 64] x [64 x 8]. Features are gathered straight into the A
-// fragments; the hidden layer goes through shared memory to change from
+// evaluates a row tile of 16 consecutive cells along x: layer 1 is
+// [16 x 128] x [128 x 64] (126 features padded with zeros), layer 2
+// [16 x 64] x [64 x 64], layer 3 [16 x 64] x [64 x 8]. The 125 occupancy
+// features of the tile's cells all come from one 20 x 5 x 5 halo of
+// log(1 + occupancy) values staged in shared memory, so layer 1 is a 5x5x5
+// convolution: A[m][f] = halo[yz(f)][m + dx(f)], read through a 128-entry
+// offset table. The hidden layers go through shared memory to change from
 // the accumulator layout to the A-operand layout.
 constexpr int kW1Stride = 132;  // padded rows: conflict-free B-fragment loads
 constexpr int kW2Stride = 68;
-constexpr int kTcWarps = 4;
+constexpr int kTcWarps = 8;
+constexpr int kHaloX = 24;      // 20 used; 24 keeps the A-fragment loads conflict-free
+constexpr int kHaloK = 25 * kHaloX;        // the constant feature k / 64
+constexpr int kHaloZero = kHaloK + 16;     // zero padding features
+constexpr int kHaloSize = kHaloZero + 32;
 
 struct TcShared {
   float w1[kMlpHidden * kW1Stride];
   float w2[kMlpHidden * kW2Stride];
   float w3[kMlpOut * kW2Stride];
   float b1[kMlpHidden], b2[kMlpHidden], b3[kMlpOut];
+  int toff[128];  // halo offset of feature f for cell 0 of the tile
   float h[kTcWarps][16 * kW2Stride];
+  float halo[kTcWarps][kHaloSize];
 };
 
 __device__ __forceinline__ uint32_t to_tf32(float x) {
@@ -283,26 +293,9 @@ __device__ __forceinline__ void mma_tf32(float (&c)[4], uint32_t a0, uint32_t a1
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// Non-empty cells into a list (order does not matter).
-__global__ void k_list_cells(const uint32_t *__restrict__ off, long long ncells,
-                             uint32_t *__restrict__ list, uint32_t *__restrict__ count) {
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncells;
-       c += (long long)gridDim.x * blockDim.x) {
-    const bool has = off[c + 1] > off[c];
-    const unsigned m = __ballot_sync(0xffffffffu, has);
-    if (m == 0) continue;
-    const int lane = threadIdx.x & 31;
-    uint32_t base = 0;
-    if (lane == __ffs(m) - 1) base = atomicAdd(count, uint32_t(__popc(m)));
-    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-    if (has) list[base + __popc(m & ((1u << lane) - 1u))] = uint32_t(c);
-  }
-}
-
-__global__ void __launch_bounds__(kTcWarps * 32) k_cell_proposal_tc(
+__global__ void __launch_bounds__(kTcWarps * 32, 1) k_cell_proposal_tc(
     const float *__restrict__ params, const FrameDesc *__restrict__ frames, int nframes,
-    const uint32_t *__restrict__ off, const uint32_t *__restrict__ list,
-    const uint32_t *__restrict__ list_count, float tau, int8_t *__restrict__ cell_prop) {
+    const uint32_t *__restrict__ off, float tau, int8_t *__restrict__ cell_prop) {
   extern __shared__ float smem_raw[];
   TcShared &sh = *reinterpret_cast<TcShared *>(smem_raw);
   const float *W1 = params, *B1 = W1 + kMlpHidden * kMlpIn;
@@ -325,57 +318,59 @@ __global__ void __launch_bounds__(kTcWarps * 32) k_cell_proposal_tc(
     sh.b2[t] = B2[t];
   }
   if (threadIdx.x < kMlpOut) sh.b3[threadIdx.x] = B3[threadIdx.x];
+  if (threadIdx.x < 128) {
+    // feature f = (dx + 2) * 25 + (dy + 2) * 5 + (dz + 2); halo row (dy + 2) * 5 + (dz + 2)
+    const int f = threadIdx.x;
+    sh.toff[f] = f < 125 ? (f % 25) * kHaloX + f / 25 : (f == 125 ? kHaloK : kHaloZero);
+  }
   __syncthreads();
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, tig = lane & 3;
-  const uint32_t ncl = *list_count;
   float *hbuf = sh.h[warp];
-  const long long tiles = (ncl + 15) / 16;
+  float *halo = sh.halo[warp];
+  const FrameDesc &last = frames[nframes - 1];
+  const long long tiles = last.row_tile_base + (long long)((last.nx + 15) / 16) * last.ny * last.nz;
   for (long long tile = (long long)blockIdx.x * kTcWarps + warp; tile < tiles;
        tile += (long long)gridDim.x * kTcWarps) {
-    // the two cells (rows g and g + 8) whose features this lane gathers
-    int cxs[2], cys[2], czs[2];
-    const FrameDesc *frs[2];
-    bool valid[2];
-    long long cellid[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const long long row = tile * 16 + g + 8 * h;
-      valid[h] = row < ncl;
-      const long long c = valid[h] ? (long long)list[row] : 0;
-      cellid[h] = c;
-      int f = 0;
-      if (nframes > 1) {
-        int lo = 0, hi = nframes - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (frames[mid].cell_base <= c)
-            lo = mid;
-          else
-            hi = mid - 1;
-        }
-        f = lo;
+    int f = 0;
+    if (nframes > 1) {
+      int lo = 0, hi = nframes - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (frames[mid].row_tile_base <= tile)
+          lo = mid;
+        else
+          hi = mid - 1;
       }
-      frs[h] = &frames[f];
-      const uint32_t lc = uint32_t(c - frs[h]->cell_base);
-      cxs[h] = int(lc % uint32_t(frs[h]->nx));
-      cys[h] = int((lc / uint32_t(frs[h]->nx)) % uint32_t(frs[h]->ny));
-      czs[h] = int(lc / (uint32_t(frs[h]->nx) * uint32_t(frs[h]->ny)));
+      f = lo;
     }
-    auto feature = [&](int h, int fi) -> float {
-      if (!valid[h]) return 0.f;
-      const FrameDesc &fr = *frs[h];
-      if (fi < 125) {
-        const int dx = fi / 25 - 2, dy = (fi / 5) % 5 - 2, dz = fi % 5 - 2;
-        const int jx = rem_euclid(cxs[h] + dx, fr.nx);
-        const int jy = rem_euclid(cys[h] + dy, fr.ny);
-        const int jz = rem_euclid(czs[h] + dz, fr.nz);
-        const long long q = fr.cell_base + ((long long)jz * fr.ny + jy) * (long long)fr.nx + jx;
-        return log1pf(float(off[q + 1] - off[q]));
-      }
-      return fi == 125 ? float(fr.k) / 64.0f : 0.f;
-    };
+    const FrameDesc &fr = frames[f];
+    const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
+    const int per_row = (nx + 15) / 16;
+    const long long lt = tile - fr.row_tile_base;
+    const int row = int(lt / per_row);
+    const int x0 = int(lt - (long long)row * per_row) * 16;
+    const int cy = row % ny, cz = row / ny;
+    const int ncl = min(16, nx - x0);
+    const long long c0 = fr.cell_base + (long long)row * nx + x0;
+    if (off[c0] == off[c0 + ncl]) continue;  // no occupied cell in the tile
+    // halo: x0 - 2 .. x0 + 17, cy - 2 .. cy + 2, cz - 2 .. cz + 2 (periodic)
+    __syncwarp();
+    for (int hidx = lane; hidx < 25 * 20; hidx += 32) {
+      const int yz = hidx / 20, xx = hidx - yz * 20;
+      const int jy = rem_euclid(cy + yz / 5 - 2, ny);
+      const int jz = rem_euclid(cz + yz % 5 - 2, nz);
+      const int jx = rem_euclid(x0 + xx - 2, nx);
+      const long long q = fr.cell_base + ((long long)jz * ny + jy) * (long long)nx + jx;
+      halo[yz * kHaloX + xx] = __uint_as_float(to_tf32(log1pf(float(off[q + 1] - off[q]))));
+    }
+    if (lane < 16) {
+      halo[kHaloK + lane] = __uint_as_float(to_tf32(float(fr.k) / 64.0f));
+      halo[kHaloZero + lane] = 0.f;
+      halo[kHaloZero + 16 + lane] = 0.f;
+    }
+    __syncwarp();
     // layer 1
     float acc[8][4];
 #pragma unroll
@@ -386,11 +381,13 @@ __global__ void __launch_bounds__(kTcWarps * 32) k_cell_proposal_tc(
       acc[nt][2] = b0;
       acc[nt][3] = b1v;
     }
+#pragma unroll 2
     for (int k0 = 0; k0 < 128; k0 += 8) {
-      const uint32_t a0 = to_tf32(feature(0, k0 + tig));
-      const uint32_t a1 = to_tf32(feature(1, k0 + tig));
-      const uint32_t a2 = to_tf32(feature(0, k0 + tig + 4));
-      const uint32_t a3 = to_tf32(feature(1, k0 + tig + 4));
+      const int o0 = sh.toff[k0 + tig], o1 = sh.toff[k0 + tig + 4];
+      const uint32_t a0 = __float_as_uint(halo[o0 + g]);
+      const uint32_t a1 = __float_as_uint(halo[o0 + g + 8]);
+      const uint32_t a2 = __float_as_uint(halo[o1 + g]);
+      const uint32_t a3 = __float_as_uint(halo[o1 + g + 8]);
 #pragma unroll
       for (int nt = 0; nt < 8; ++nt) {
         const int n = nt * 8 + g;
@@ -454,7 +451,6 @@ __global__ void __launch_bounds__(kTcWarps * 32) k_cell_proposal_tc(
       const uint32_t b1 = __float_as_uint(sh.w3[g * kW2Stride + k0 + tig + 4]);
       mma_tf32(z, a0, a1, a2, a3, b0, b1);
     }
-    __syncwarp();
     // each quad holds the 8 logits of rows g (z[0], z[1]) and g + 8 (z[2], z[3])
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -464,14 +460,15 @@ __global__ void __launch_bounds__(kTcWarps * 32) k_cell_proposal_tc(
         lg[2 * q] = __shfl_sync(0xffffffffu, z[2 * h], (lane & ~3) | q);
         lg[2 * q + 1] = __shfl_sync(0xffffffffu, z[2 * h + 1], (lane & ~3) | q);
       }
-      if (tig == 0 && valid[h]) {
-        float m = lg[0];
+      const int m = g + 8 * h;
+      if (tig == 0 && m < ncl) {
+        float mx = lg[0];
 #pragma unroll
-        for (int o = 1; o < 8; ++o) m = fmaxf(m, lg[o]);
+        for (int o = 1; o < 8; ++o) mx = fmaxf(mx, lg[o]);
         float e[8], sum = 0.f;
 #pragma unroll
         for (int o = 0; o < 8; ++o) {
-          e[o] = __expf(lg[o] - m);
+          e[o] = __expf(lg[o] - mx);
           sum += e[o];
         }
         int prop = kMlpOut;
@@ -481,7 +478,7 @@ __global__ void __launch_bounds__(kTcWarps * 32) k_cell_proposal_tc(
           cum += e[o] / sum;
           if (cum >= tau && prop == kMlpOut) prop = o + 1;
         }
-        cell_prop[cellid[h]] = int8_t(prop >= kMlpOut ? 0 : prop);
+        cell_prop[c0 + m] = int8_t(prop >= kMlpOut ? 0 : prop);
       }
     }
     __syncwarp();
@@ -573,20 +570,19 @@ cudaError_t mlp_training_rows(const BatchBuffers &b, const int8_t *stop_log, lon
 }
 
 cudaError_t mlp_propose(const float *params, const BatchBuffers &b, int8_t *cell_prop,
-                        int8_t *source_prop, float tau, uint32_t *cell_list, uint32_t *list_count,
-                        cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(list_count, 0, sizeof(uint32_t), s);
-  if (e != cudaSuccess) return e;
-  k_list_cells<<<grid_of(b.ncells, 256), 256, 0, s>>>(b.off, b.ncells, cell_list, list_count);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+                        int8_t *source_prop, float tau, cudaStream_t s) {
+  if (b.nframes <= 0 || b.ncells <= 0) return cudaSuccess;
   const size_t sm = sizeof(TcShared);
-  e = cudaFuncSetAttribute(k_cell_proposal_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+  cudaError_t e =
+      cudaFuncSetAttribute(k_cell_proposal_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
   if (e != cudaSuccess) return e;
-  int dev = 0, sms = 148;
+  int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_cell_proposal_tc<<<sms * 3, kTcWarps * 32, sm, s>>>(params, b.frames, b.nframes, b.off,
-                                                         cell_list, list_count, tau, cell_prop);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_proposal_tc, kTcWarps * 32, sm);
+  if (per_sm < 1) per_sm = 1;
+  k_cell_proposal_tc<<<sms * per_sm, kTcWarps * 32, sm, s>>>(params, b.frames, b.nframes, b.off,
+                                                              tau, cell_prop);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_source_proposal<<<grid_of(b.npts, 256), 256, 0, s>>>(b.frames, b.nframes, b.off, b.ncells,
                                                          b.scell, cell_prop, source_prop);

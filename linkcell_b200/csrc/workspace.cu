@@ -168,7 +168,43 @@ Code plan_frame(const double *rows, const double *origin, double cell_hint, int 
   for (int t = 0; t < 9; ++t) mag += std::fabs(fd.h[t]);
   // generous: 2^-36 of the largest coordinate / shift magnitude per unit wrap
   fd.eps64 = std::ldexp(mag, -36);
+  fill_select_tables(fd);
   return Code::Ok;
+}
+
+namespace {
+// Smallest float >= v.
+float float_up(double v) {
+  float f = float(v);
+  if (double(f) < v) f = std::nextafter(f, std::numeric_limits<float>::infinity());
+  return f;
+}
+}  // namespace
+
+// Per-reach constants of the cube select walk. The FP32 distance of a
+// candidate whose cell offset is at most R per axis differs from the
+// reference's FP64 value by at most band(d) = 8u d + beta(R), with
+// e = u (6R + 8) ell + eps64 (R + 2) the per-component error of the FP32
+// offset and beta(R) = 4 e^2 / u + 4 e^2 (the cross terms 2 |D| e are
+// bounded by u D^2 + e^2 / u); 1e-6 of margin on top.
+void fill_select_tables(FrameDesc &fd) {
+  const double u = 5.9604644775390625e-08;  // 2^-24
+  for (int R = 0; R <= 8; ++R) {
+    const int Ru = R < 1 ? 1 : R;
+    const double e = u * (6.0 * Ru + 8.0) * double(fd.ell) + fd.eps64 * (Ru + 2.0);
+    const double beta = (4.0 * e * e / u + 4.0 * e * e) * (1.0 + 1e-6);
+    const double b = double(Ru) * fd.cell_min;
+    const double B = b * b;
+    const double band = B * 8.0 * u + beta;
+    fd.sel_beta[R] = float_up(beta);
+    fd.sel_thr[R] = float_up(B * (1.0 + 8.0 * u) + beta);
+    fd.sel_bhi[R] = float_up(B + 2.0 * band);
+    const double lam = double(float(fd.lam_min) * 0.99f);
+    fd.sel_qlim[R] = lam > 0.0 ? float_up(double(fd.sel_thr[R]) / lam * 1.0001) : 3.0e38f;
+    fd.sel_epsr[R] = float_up(band / (2.0 * fd.cell_min * fd.cell_min) + 16.0 * u * (Ru + 2.0));
+  }
+  fd.inv_nx = 1.0 / double(fd.nx);
+  fd.inv_nxy = 1.0 / (double(fd.nx) * double(fd.ny));
 }
 
 // ------------------------------------------------------------ workspace
@@ -260,7 +296,7 @@ void WorkspaceImpl::release_all() {
   rel(sidx_); rel(replay_list_); rel(replay_i_); rel(scell_); rel(sx_); rel(sy_); rel(sz_);
   rel(replay_d_); rel(rec_); rel(frames_); rel(counters_); rel(h_xyz_); rel(h_d2_);
   rel(h_mask_); rel(h_nn_); rel(active_); rel(proposal_); rel(cell_prop_); rel(stop_log_);
-  rel(model_); rel(shell_table_); rel(cell_list_); rel(list_count_);
+  rel(model_); rel(shell_table_);
   shell_table_ready_ = false;
 }
 
@@ -276,11 +312,13 @@ void WorkspaceImpl::release_all() {
 Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const int *mask,
                         int *out_nn, double *out_d2, bool wait, std::string &detail) {
   const int nf = int(frames.size());
-  long long npts = 0, ncells = 0;
+  long long npts = 0, ncells = 0, rtiles = 0;
   int kmax = 1;
   for (auto &fd : frames) {
     fd.pt_base = npts;
     fd.cell_base = ncells;
+    fd.row_tile_base = rtiles;
+    rtiles += (long long)((fd.nx + 15) / 16) * fd.ny * fd.nz;
     npts += fd.n;
     ncells += (long long)fd.nx * fd.ny * fd.nz;
     kmax = std::max(kmax, fd.k);
@@ -320,11 +358,7 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   const bool learned = opts.mode == kModeLearned && kmax <= 256;
   if (learned) {
     LC_TRY(grow(proposal_, P));
-    if (opts.fixed_proposal <= 0 && has_model_) {
-      LC_TRY(grow(cell_prop_, C));
-      LC_TRY(grow(cell_list_, C));
-      LC_TRY(grow(list_count_, 1));
-    }
+    if (opts.fixed_proposal <= 0 && has_model_) LC_TRY(grow(cell_prop_, C));
   }
   if (!shell_table_ready_) {
     const int rmax = kShellTableRmax;
@@ -517,8 +551,7 @@ Code WorkspaceImpl::enqueue(BatchBuffers &b, const WalkLaunch &wl, int nf, size_
     if (opts.fixed_proposal > 0) {
       LC_TRY(cudaMemsetAsync(proposal_.p, std::min(opts.fixed_proposal, 127), P, s));
     } else if (has_model_) {
-      LC_TRY(mlp_propose(model_.p, b, cell_prop_.p, proposal_.p, tau_, cell_list_.p,
-                         list_count_.p, s));
+      LC_TRY(mlp_propose(model_.p, b, cell_prop_.p, proposal_.p, tau_, s));
     } else {
       LC_TRY(cudaMemsetAsync(proposal_.p, 0, P, s));
     }

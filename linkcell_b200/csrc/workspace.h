@@ -41,6 +41,8 @@ const char *gpu_message(Code c);
 // src/knearest.rs:377-397,430) into a FrameDesc. rows = a, b, c (9 doubles)
 // and origin (3 doubles). hint <= 0 or NaN selects the default edge 3.0.
 Code plan_frame(const double *rows, const double *origin, double cell_hint, int k, FrameDesc &fd);
+// Fills the per-reach constants of the cube select walk (FrameDesc::sel_*).
+void fill_select_tables(FrameDesc &fd);
 
 // Options that pick the walk.
 struct WalkOptions {
@@ -154,7 +156,7 @@ class WorkspaceImpl {
   Buf<long long> counters_;
   Buf<int8_t> proposal_, cell_prop_, stop_log_;
   Buf<float> model_;
-  Buf<uint32_t> shell_table_, cell_list_, list_count_;
+  Buf<uint32_t> shell_table_;
   bool shell_table_ready_ = false;
   bool has_model_ = false;
   float tau_ = 0.9f;

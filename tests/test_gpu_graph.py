@@ -51,7 +51,7 @@ def test_graph_replay_follows_new_cells(gpu, lib, oracle_mod, mode):
         assert lib.lc_gpu_set_graph(ws, 1) == 0
         buf = Fixed(lib, ws, n, k)
         for step in range(4):
-            L = 14.0 + step
+            L = 14.0 + 0.01 * step  # same cell grid: the graph is replayed
             cell = np.array([[L, 0.3, -0.2], [0.0, L - 1.0, 0.4], [0.0, 0.0, L + 0.5]])
             xyz = rng.random((n, 3)) @ cell
             want = oracle_mod.knearest(xyz, cell, k)
