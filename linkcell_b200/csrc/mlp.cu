@@ -9,13 +9,14 @@
 //     softmax cross-entropy, backward (GEMMs for input and weight
 //     gradients, SiLU derivative), and Adam;
 //   - k_cell_proposal_tc: inference over 16-cell row tiles on the tensor
-//     cores (mma.sync TF32, FP32 accumulation; layer 1 as a 5x5x5
+//     cores (mma.sync FP16, FP32 accumulation; layer 1 as a 5x5x5
 //     convolution of the staged occupancy halo), writing the proposed shell
 //     of every occupied cell (the smallest R with P(settled shell <= R) >=
 //     tau); the walk reads it for each source.
 //
 // Parameter layout (floats): W1[64][126] b1[64] W2[64][64] b2[64]
 // W3[8][64] b3[8].
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -251,51 +252,65 @@ __global__ void k_training_rows(BatchBuffers b, const int8_t *__restrict__ stop_
 }
 
 // ---------------------------------------------------------------------
-// Tensor-core inference: mma.sync m16n8k8 TF32 (FP32 accumulate). One warp
-// evaluates a row tile of 16 consecutive cells along x: layer 1 is
-// [16 x 128] x [128 x 64] (126 features padded with zeros), layer 2
-// [16 x 64] x [64 x 64], layer 3 [16 x 64] x [64 x 8]. The 125 occupancy
-// features of the tile's cells all come from one 20 x 5 x 5 halo of
-// log(1 + occupancy) values staged in shared memory, so layer 1 is a 5x5x5
-// convolution: A[m][f] = halo[yz(f)][m + dx(f)], read through a 128-entry
-// offset table. The hidden layers go through shared memory to change from
-// the accumulator layout to the A-operand layout.
-constexpr int kW1Stride = 132;  // padded rows: conflict-free B-fragment loads
-constexpr int kW2Stride = 68;
+// Tensor-core inference: mma.sync m16n8k16 FP16 (FP32 accumulate; FP16 keeps
+// the 10-bit significand of TF32). One warp evaluates a row tile of 16
+// consecutive cells along x: layer 1 is [16 x 128] x [128 x 64] (126
+// features padded with zeros), layer 2 [16 x 64] x [64 x 64], layer 3
+// [16 x 64] x [64 x 8]. The 125 occupancy features of the tile's cells all
+// come from one 20 x 5 x 5 halo of log(1 + occupancy) values staged in
+// shared memory, so layer 1 is a 5x5x5 convolution: A[m][f] =
+// halo[yz(f)][m + dx(f)], read through a 128-entry offset table. The hidden
+// layers go through shared memory to change from the accumulator layout to
+// the A-operand layout.
+constexpr int kW1Stride = 136;  // halves per W1 row: conflict-free B-fragment loads
+constexpr int kW2Stride = 72;   // halves per W2 / W3 / hidden row
 constexpr int kTcWarps = 8;
-constexpr int kHaloX = 24;      // 20 used; 24 keeps the A-fragment loads conflict-free
+constexpr int kHaloX = 24;      // 20 used
 constexpr int kHaloK = 25 * kHaloX;        // the constant feature k / 64
 constexpr int kHaloZero = kHaloK + 16;     // zero padding features
 constexpr int kHaloSize = kHaloZero + 32;
 
 struct TcShared {
-  float w1[kMlpHidden * kW1Stride];
-  float w2[kMlpHidden * kW2Stride];
-  float w3[kMlpOut * kW2Stride];
+  __half w1[kMlpHidden * kW1Stride];
+  __half w2[kMlpHidden * kW2Stride];
+  __half w3[kMlpOut * kW2Stride];
   float b1[kMlpHidden], b2[kMlpHidden], b3[kMlpOut];
-  int toff[128];  // halo offset of feature f for cell 0 of the tile
-  float h[kTcWarps][16 * kW2Stride];
-  float halo[kTcWarps][kHaloSize];
+  float lg1p[64];   // log(1 + c) for occupancies c < 64
+  int toff[128];    // halo offset of feature f for cell 0 of the tile
+  __half h[kTcWarps][16 * kW2Stride];
+  __half halo[kTcWarps][kHaloSize];
 };
 
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
-
-__device__ __forceinline__ void mma_tf32(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
-                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+__device__ __forceinline__ void mma_f16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                        uint32_t a3, uint32_t b0, uint32_t b1) {
   asm volatile(
-      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
       "{%8,%9}, {%0,%1,%2,%3};"
       : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+__device__ __forceinline__ uint32_t pack_h2(__half lo, __half hi) {
+  return uint32_t(__half_as_ushort(lo)) | (uint32_t(__half_as_ushort(hi)) << 16);
+}
+
+__device__ __forceinline__ uint32_t ld_h2(const __half *p) {
+  return *reinterpret_cast<const uint32_t *>(p);
+}
+
+// SiLU with the fast division (inference only).
+__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+
+// Periodic coordinate c + d for |d| <= 2.
+__device__ __forceinline__ int wrap_near(int c, int n) {
+  if (n < 3) return rem_euclid(c, n);
+  return c < 0 ? c + n : (c >= n ? c - n : c);
+}
+
 __global__ void __launch_bounds__(kTcWarps * 32, 1) k_cell_proposal_tc(
     const float *__restrict__ params, const FrameDesc *__restrict__ frames, int nframes,
-    const uint32_t *__restrict__ off, float tau, int8_t *__restrict__ cell_prop) {
+    const uint32_t *__restrict__ off, const uint32_t *__restrict__ count, float tau,
+    int8_t *__restrict__ cell_prop) {
   extern __shared__ float smem_raw[];
   TcShared &sh = *reinterpret_cast<TcShared *>(smem_raw);
   const float *W1 = params, *B1 = W1 + kMlpHidden * kMlpIn;
@@ -303,21 +318,22 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) k_cell_proposal_tc(
   const float *W3 = B2 + kMlpHidden, *B3 = W3 + kMlpOut * kMlpHidden;
   for (int t = threadIdx.x; t < kMlpHidden * kW1Stride; t += blockDim.x) {
     const int n = t / kW1Stride, kk = t % kW1Stride;
-    sh.w1[t] = kk < kMlpIn ? __uint_as_float(to_tf32(W1[n * kMlpIn + kk])) : 0.f;
+    sh.w1[t] = __float2half_rn(kk < kMlpIn ? W1[n * kMlpIn + kk] : 0.f);
   }
   for (int t = threadIdx.x; t < kMlpHidden * kW2Stride; t += blockDim.x) {
     const int n = t / kW2Stride, kk = t % kW2Stride;
-    sh.w2[t] = kk < kMlpHidden ? __uint_as_float(to_tf32(W2[n * kMlpHidden + kk])) : 0.f;
+    sh.w2[t] = __float2half_rn(kk < kMlpHidden ? W2[n * kMlpHidden + kk] : 0.f);
   }
   for (int t = threadIdx.x; t < kMlpOut * kW2Stride; t += blockDim.x) {
     const int n = t / kW2Stride, kk = t % kW2Stride;
-    sh.w3[t] = kk < kMlpHidden ? __uint_as_float(to_tf32(W3[n * kMlpHidden + kk])) : 0.f;
+    sh.w3[t] = __float2half_rn(kk < kMlpHidden ? W3[n * kMlpHidden + kk] : 0.f);
   }
   for (int t = threadIdx.x; t < kMlpHidden; t += blockDim.x) {
     sh.b1[t] = B1[t];
     sh.b2[t] = B2[t];
   }
   if (threadIdx.x < kMlpOut) sh.b3[threadIdx.x] = B3[threadIdx.x];
+  if (threadIdx.x < 64) sh.lg1p[threadIdx.x] = log1pf(float(threadIdx.x));
   if (threadIdx.x < 128) {
     // feature f = (dx + 2) * 25 + (dy + 2) * 5 + (dz + 2); halo row (dy + 2) * 5 + (dz + 2)
     const int f = threadIdx.x;
@@ -327,8 +343,8 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) k_cell_proposal_tc(
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, tig = lane & 3;
-  float *hbuf = sh.h[warp];
-  float *halo = sh.halo[warp];
+  __half *hbuf = sh.h[warp];
+  __half *halo = sh.halo[warp];
   const FrameDesc &last = frames[nframes - 1];
   const long long tiles = last.row_tile_base + (long long)((last.nx + 15) / 16) * last.ny * last.nz;
   for (long long tile = (long long)blockIdx.x * kTcWarps + warp; tile < tiles;
@@ -359,16 +375,16 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) k_cell_proposal_tc(
     __syncwarp();
     for (int hidx = lane; hidx < 25 * 20; hidx += 32) {
       const int yz = hidx / 20, xx = hidx - yz * 20;
-      const int jy = rem_euclid(cy + yz / 5 - 2, ny);
-      const int jz = rem_euclid(cz + yz % 5 - 2, nz);
-      const int jx = rem_euclid(x0 + xx - 2, nx);
-      const long long q = fr.cell_base + ((long long)jz * ny + jy) * (long long)nx + jx;
-      halo[yz * kHaloX + xx] = __uint_as_float(to_tf32(log1pf(float(off[q + 1] - off[q]))));
+      const int jy = wrap_near(cy + yz / 5 - 2, ny);
+      const int jz = wrap_near(cz + yz % 5 - 2, nz);
+      const int jx = (nx >= 20) ? wrap_near(x0 + xx - 2, nx) : rem_euclid(x0 + xx - 2, nx);
+      const uint32_t cnt = count[fr.cell_base + ((long long)jz * ny + jy) * (long long)nx + jx];
+      halo[yz * kHaloX + xx] = __float2half_rn(cnt < 64u ? sh.lg1p[cnt] : log1pf(float(cnt)));
     }
     if (lane < 16) {
-      halo[kHaloK + lane] = __uint_as_float(to_tf32(float(fr.k) / 64.0f));
-      halo[kHaloZero + lane] = 0.f;
-      halo[kHaloZero + 16 + lane] = 0.f;
+      halo[kHaloK + lane] = __float2half_rn(float(fr.k) / 64.0f);
+      halo[kHaloZero + lane] = __float2half_rn(0.f);
+      halo[kHaloZero + 16 + lane] = __float2half_rn(0.f);
     }
     __syncwarp();
     // layer 1
@@ -382,28 +398,27 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) k_cell_proposal_tc(
       acc[nt][3] = b1v;
     }
 #pragma unroll 2
-    for (int k0 = 0; k0 < 128; k0 += 8) {
-      const int o0 = sh.toff[k0 + tig], o1 = sh.toff[k0 + tig + 4];
-      const uint32_t a0 = __float_as_uint(halo[o0 + g]);
-      const uint32_t a1 = __float_as_uint(halo[o0 + g + 8]);
-      const uint32_t a2 = __float_as_uint(halo[o1 + g]);
-      const uint32_t a3 = __float_as_uint(halo[o1 + g + 8]);
+    for (int k0 = 0; k0 < 128; k0 += 16) {
+      const int o0 = sh.toff[k0 + 2 * tig], o1 = sh.toff[k0 + 2 * tig + 1];
+      const int o2 = sh.toff[k0 + 2 * tig + 8], o3 = sh.toff[k0 + 2 * tig + 9];
+      const uint32_t a0 = pack_h2(halo[o0 + g], halo[o1 + g]);
+      const uint32_t a1 = pack_h2(halo[o0 + g + 8], halo[o1 + g + 8]);
+      const uint32_t a2 = pack_h2(halo[o2 + g], halo[o3 + g]);
+      const uint32_t a3 = pack_h2(halo[o2 + g + 8], halo[o3 + g + 8]);
 #pragma unroll
       for (int nt = 0; nt < 8; ++nt) {
-        const int n = nt * 8 + g;
-        const uint32_t b0 = __float_as_uint(sh.w1[n * kW1Stride + k0 + tig]);
-        const uint32_t b1 = __float_as_uint(sh.w1[n * kW1Stride + k0 + tig + 4]);
-        mma_tf32(acc[nt], a0, a1, a2, a3, b0, b1);
+        const __half *wr = sh.w1 + (nt * 8 + g) * kW1Stride + k0 + 2 * tig;
+        mma_f16(acc[nt], a0, a1, a2, a3, ld_h2(wr), ld_h2(wr + 8));
       }
     }
-    // SiLU, then to shared memory (row-major 16 x 64)
+    // SiLU, then to shared memory (row-major 16 x 64 halves)
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
       const int col = nt * 8 + 2 * tig;
-      hbuf[g * kW2Stride + col] = silu(acc[nt][0]);
-      hbuf[g * kW2Stride + col + 1] = silu(acc[nt][1]);
-      hbuf[(g + 8) * kW2Stride + col] = silu(acc[nt][2]);
-      hbuf[(g + 8) * kW2Stride + col + 1] = silu(acc[nt][3]);
+      *reinterpret_cast<__half2 *>(hbuf + g * kW2Stride + col) =
+          __floats2half2_rn(silu_fast(acc[nt][0]), silu_fast(acc[nt][1]));
+      *reinterpret_cast<__half2 *>(hbuf + (g + 8) * kW2Stride + col) =
+          __floats2half2_rn(silu_fast(acc[nt][2]), silu_fast(acc[nt][3]));
     }
     __syncwarp();
     // layer 2
@@ -416,40 +431,37 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) k_cell_proposal_tc(
       acc[nt][3] = b1v;
     }
 #pragma unroll
-    for (int k0 = 0; k0 < 64; k0 += 8) {
-      const uint32_t a0 = to_tf32(hbuf[g * kW2Stride + k0 + tig]);
-      const uint32_t a1 = to_tf32(hbuf[(g + 8) * kW2Stride + k0 + tig]);
-      const uint32_t a2 = to_tf32(hbuf[g * kW2Stride + k0 + tig + 4]);
-      const uint32_t a3 = to_tf32(hbuf[(g + 8) * kW2Stride + k0 + tig + 4]);
+    for (int k0 = 0; k0 < 64; k0 += 16) {
+      const uint32_t a0 = ld_h2(hbuf + g * kW2Stride + k0 + 2 * tig);
+      const uint32_t a1 = ld_h2(hbuf + (g + 8) * kW2Stride + k0 + 2 * tig);
+      const uint32_t a2 = ld_h2(hbuf + g * kW2Stride + k0 + 2 * tig + 8);
+      const uint32_t a3 = ld_h2(hbuf + (g + 8) * kW2Stride + k0 + 2 * tig + 8);
 #pragma unroll
       for (int nt = 0; nt < 8; ++nt) {
-        const int n = nt * 8 + g;
-        const uint32_t b0 = __float_as_uint(sh.w2[n * kW2Stride + k0 + tig]);
-        const uint32_t b1 = __float_as_uint(sh.w2[n * kW2Stride + k0 + tig + 4]);
-        mma_tf32(acc[nt], a0, a1, a2, a3, b0, b1);
+        const __half *wr = sh.w2 + (nt * 8 + g) * kW2Stride + k0 + 2 * tig;
+        mma_f16(acc[nt], a0, a1, a2, a3, ld_h2(wr), ld_h2(wr + 8));
       }
     }
     __syncwarp();
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
       const int col = nt * 8 + 2 * tig;
-      hbuf[g * kW2Stride + col] = silu(acc[nt][0]);
-      hbuf[g * kW2Stride + col + 1] = silu(acc[nt][1]);
-      hbuf[(g + 8) * kW2Stride + col] = silu(acc[nt][2]);
-      hbuf[(g + 8) * kW2Stride + col + 1] = silu(acc[nt][3]);
+      *reinterpret_cast<__half2 *>(hbuf + g * kW2Stride + col) =
+          __floats2half2_rn(silu_fast(acc[nt][0]), silu_fast(acc[nt][1]));
+      *reinterpret_cast<__half2 *>(hbuf + (g + 8) * kW2Stride + col) =
+          __floats2half2_rn(silu_fast(acc[nt][2]), silu_fast(acc[nt][3]));
     }
     __syncwarp();
     // layer 3: 8 logits per cell
     float z[4] = {sh.b3[2 * tig], sh.b3[2 * tig + 1], sh.b3[2 * tig], sh.b3[2 * tig + 1]};
 #pragma unroll
-    for (int k0 = 0; k0 < 64; k0 += 8) {
-      const uint32_t a0 = to_tf32(hbuf[g * kW2Stride + k0 + tig]);
-      const uint32_t a1 = to_tf32(hbuf[(g + 8) * kW2Stride + k0 + tig]);
-      const uint32_t a2 = to_tf32(hbuf[g * kW2Stride + k0 + tig + 4]);
-      const uint32_t a3 = to_tf32(hbuf[(g + 8) * kW2Stride + k0 + tig + 4]);
-      const uint32_t b0 = __float_as_uint(sh.w3[g * kW2Stride + k0 + tig]);
-      const uint32_t b1 = __float_as_uint(sh.w3[g * kW2Stride + k0 + tig + 4]);
-      mma_tf32(z, a0, a1, a2, a3, b0, b1);
+    for (int k0 = 0; k0 < 64; k0 += 16) {
+      const uint32_t a0 = ld_h2(hbuf + g * kW2Stride + k0 + 2 * tig);
+      const uint32_t a1 = ld_h2(hbuf + (g + 8) * kW2Stride + k0 + 2 * tig);
+      const uint32_t a2 = ld_h2(hbuf + g * kW2Stride + k0 + 2 * tig + 8);
+      const uint32_t a3 = ld_h2(hbuf + (g + 8) * kW2Stride + k0 + 2 * tig + 8);
+      const __half *wr = sh.w3 + g * kW2Stride + k0 + 2 * tig;
+      mma_f16(z, a0, a1, a2, a3, ld_h2(wr), ld_h2(wr + 8));
     }
     // each quad holds the 8 logits of rows g (z[0], z[1]) and g + 8 (z[2], z[3])
 #pragma unroll
@@ -582,7 +594,7 @@ cudaError_t mlp_propose(const float *params, const BatchBuffers &b, int8_t *cell
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_proposal_tc, kTcWarps * 32, sm);
   if (per_sm < 1) per_sm = 1;
   k_cell_proposal_tc<<<sms * per_sm, kTcWarps * 32, sm, s>>>(params, b.frames, b.nframes, b.off,
-                                                              tau, cell_prop);
+                                                              b.count, tau, cell_prop);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_source_proposal<<<grid_of(b.npts, 256), 256, 0, s>>>(b.frames, b.nframes, b.off, b.ncells,
                                                          b.scell, cell_prop, source_prop);

@@ -77,7 +77,7 @@ def test_graph_stats_report_total_time(gpu, lib):
             buf.run(rng.random((2000, 3)) * 12.0, [12.0, 12.0, 12.0])
         counters = (ctypes.c_longlong * 16)()
         ms = ctypes.c_double()
-        assert lib.lc_gpu_stats(ws, counters, 16, ctypes.byref(ms)) == 0
+        assert lib.lc_gpu_stats(ws, counters, 16, ctypes.byref(ms)) == 16
         assert ms.value > 0.0
     finally:
         lib.lc_gpu_workspace_free(ws)

@@ -98,7 +98,7 @@ def test_learned_walk_with_network_is_exact_and_saves_work(gpu, oracle_mod):
 
 
 def test_tensor_core_proposals_match_cpu_network(gpu):
-    """The walk's proposals (tensor-core inference, TF32) agree with the CPU
+    """The walk's proposals (tensor-core inference, FP16) agree with the CPU
     reference network on the same features for nearly every source; a
     disagreement only moves work, never the result."""
     import ctypes
