@@ -984,9 +984,9 @@ __global__ void __launch_bounds__(256, 2) k_team_walk(BatchBuffers b) {
 //     value tied with the k-th, and nothing else can tie (with the FP32 error
 //     band(x) = 8u x + beta, any candidate above T + 3 band(T) has an exact
 //     distance above T + band(T), which bounds the k-th value).
-//  4. S is recomputed in exact FP64, bitonic-sorted by (d2, index), and its
-//     first k are the row; a tie across the k-th slot goes to the literal
-//     replay.
+//  4. S is recomputed in exact FP64, every element is ranked in (d2, index)
+//     order against the others, and ranks 0..k-1 are the row; a tie across
+//     the k-th slot goes to the literal replay.
 // Any proposal gives the reference result: a short proposal, a buffer
 // overflow, a cube that wraps the box, k > 32 or an S larger than 64 sends
 // the source to the literal replay.
@@ -1010,13 +1010,11 @@ struct SelShared {
   SelRow rows[32];
   double sd[64];
   int sj[64];
+  int si[64];
   int hist[32];
   unsigned hmax[32];
+  unsigned long long wc[8];  // warp-uniform counters (SelWarpCounter), lane 0 updates
 };
-
-__device__ __forceinline__ float band32(double theta, double beta) {
-  return __double2float_ru(theta * 8.0 * double(kU32) + beta);
-}
 
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
@@ -1030,66 +1028,10 @@ __device__ __forceinline__ float axis_gap(int d, float f) {
   return d > 0 ? float(d) - f : (d < 0 ? f + float(-d - 1) : 0.f);
 }
 
-// Bitonic sort of 32 (d, j) pairs, one per lane, ascending by (d2, index).
-__device__ __forceinline__ void warp_sort32(double &d, int &j, int lane) {
-#pragma unroll
-  for (int size = 2; size <= 32; size <<= 1) {
-#pragma unroll
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      const double od = __shfl_xor_sync(kFull, d, stride);
-      const int oj = __shfl_xor_sync(kFull, j, stride);
-      const bool up = (lane & size) == 0 || size == 32;
-      const bool lower = (lane & stride) == 0;
-      const bool take = (lower == up) ? lex_less(od, oj, d, j) : lex_less(d, j, od, oj);
-      if (take) {
-        d = od;
-        j = oj;
-      }
-    }
-  }
-}
-
-// Bitonic sort of 2 * 32 (d, j) pairs held two per lane: element e = s * 32 + lane.
-__device__ __forceinline__ void warp_sort64(double (&d)[2], int (&j)[2], int lane) {
-#pragma unroll
-  for (int size = 2; size <= 64; size <<= 1) {
-#pragma unroll
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      if (stride == 32) {
-        // both partners in this lane (size == 64: one ascending block)
-        if (lex_less(d[1], j[1], d[0], j[0])) {
-          const double td = d[0];
-          const int tj = j[0];
-          d[0] = d[1];
-          j[0] = j[1];
-          d[1] = td;
-          j[1] = tj;
-        }
-        continue;
-      }
-#pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        const int e = s * 32 + lane;
-        const double od = __shfl_xor_sync(kFull, d[s], stride);
-        const int oj = __shfl_xor_sync(kFull, j[s], stride);
-        const bool up = ((e & size) == 0);
-        const bool lower = (e & stride) == 0;
-        const bool take =
-            (lower == up) ? lex_less(od, oj, d[s], j[s]) : lex_less(d[s], j[s], od, oj);
-        if (take) {
-          d[s] = od;
-          j[s] = oj;
-        }
-      }
-    }
-  }
-}
-
-struct SelCounters {
-  unsigned pairs = 0, pruned = 0, rerank = 0;          // per lane
-  unsigned inserts = 0, shells = 0, replays = 0;       // warp-uniform
-  unsigned under = 0, over = 0, exact = 0, fallback = 0;
+struct SelCounters {  // per lane; the warp-uniform counters live in SelShared::wc
+  unsigned pairs = 0, pruned = 0, rerank = 0;
 };
+enum SelWarpCounter { kWcInserts, kWcShells, kWcReplays, kWcUnder, kWcOver, kWcExact, kWcFallback };
 
 // Exact quotient of x by n from a double reciprocal estimate (x < 2^32).
 __device__ __forceinline__ uint32_t quot(uint32_t x, uint32_t n, double inv) {
@@ -1197,45 +1139,71 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
       sh.rows[__popc(ne & lanemask_lt())] = rw;
     }
     __syncwarp();
+    // two 32-candidate windows per trip, so their loads are in flight together
     int before = 0;  // non-empty rows that start before the window
-    for (int g0 = 0; g0 < tot; g0 += 32) {
-      const unsigned bit =
-          (len > 0 && excl >= g0 && excl < g0 + 32) ? (1u << (excl - g0)) : 0u;
-      const unsigned starts = __reduce_or_sync(kFull, bit);
-      const int g = g0 + lane;
-      const int owner = before + __popc(starts & (lanemask_lt() | (1u << lane))) - 1;
-      before += __popc(starts);
-      bool keep = false;
-      float d32 = 0.f;
-      int t = 0;
-      uint32_t mm = 0;
-      if (g < tot) {
-        const SelRow &R = sh.rows[owner];
-        const int loc = g - R.excl;
-        const bool inA = loc < R.lenA;
-        t = (inA ? R.startA : R.startB) + loc;
-        if ((long long)t != p) {
-          ++cnt.pairs;
-          const float4 q = b.rec[t];
-          const int dx = int(b.scell[t]) + (inA ? R.xoffA : R.xoffB);
-          const float fdx = float(dx);
-          const float ex = (q.x - plx) + fmaf(fdx, ev0, R.Dx);
-          const float ey = (q.y - ply) + fmaf(fdx, ev1, R.Dy);
-          const float ez = (q.z - plz) + fmaf(fdx, ev2, R.Dz);
-          d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-          keep = !(d32 > thr);
-          mm = uint32_t(max(abs(dx), R.syz)) | uint32_t(inA ? R.metaA : R.metaB);
+    const unsigned le = lanemask_lt() | (1u << lane);
+    for (int g0 = 0; g0 < tot; g0 += 64) {
+      const unsigned sa = __reduce_or_sync(
+          kFull, (len > 0 && excl >= g0 && excl < g0 + 32) ? (1u << (excl - g0)) : 0u);
+      const unsigned sb = __reduce_or_sync(
+          kFull, (len > 0 && excl >= g0 + 32 && excl < g0 + 64) ? (1u << (excl - g0 - 32)) : 0u);
+      int t[2], xo[2], owner[2];
+      uint32_t meta[2];
+      bool live[2];
+      owner[0] = before + __popc(sa & le) - 1;
+      owner[1] = before + __popc(sa) + __popc(sb & le) - 1;
+      before += __popc(sa) + __popc(sb);
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        const int g = g0 + 32 * w + lane;
+        live[w] = g < tot;
+        t[w] = 0;
+        xo[w] = 0;
+        meta[w] = 0;
+        if (live[w]) {
+          const SelRow &R = sh.rows[owner[w]];
+          const int loc = g - R.excl;
+          const bool inA = loc < R.lenA;
+          t[w] = (inA ? R.startA : R.startB) + loc;
+          xo[w] = inA ? R.xoffA : R.xoffB;
+          meta[w] = uint32_t(inA ? R.metaA : R.metaB);
+          live[w] = (long long)t[w] != p;
         }
       }
-      const unsigned km = __ballot_sync(kFull, keep);
-      if (total + __popc(km) > kSelCap) return false;
-      if (keep) {
-        const int pos = total + __popc(km & lanemask_lt());
-        sh.d[pos] = d32;
-        sh.t[pos] = t;
-        sh.m[pos] = mm;
+      float4 q[2];
+      int sc[2];
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        q[w] = live[w] ? b.rec[t[w]] : make_float4(0.f, 0.f, 0.f, 0.f);
+        sc[w] = live[w] ? int(b.scell[t[w]]) : 0;
       }
-      total += __popc(km);
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        bool keep = false;
+        float d32 = 0.f;
+        uint32_t mm = 0;
+        if (live[w]) {
+          ++cnt.pairs;
+          const SelRow &R = sh.rows[owner[w]];
+          const int dx = sc[w] + xo[w];
+          const float fdx = float(dx);
+          const float ex = (q[w].x - plx) + fmaf(fdx, ev0, R.Dx);
+          const float ey = (q[w].y - ply) + fmaf(fdx, ev1, R.Dy);
+          const float ez = (q[w].z - plz) + fmaf(fdx, ev2, R.Dz);
+          d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+          keep = !(d32 > thr);
+          mm = uint32_t(max(abs(dx), R.syz)) | meta[w];
+        }
+        const unsigned km = __ballot_sync(kFull, keep);
+        if (total + __popc(km) > kSelCap) return false;
+        if (keep) {
+          const int pos = total + __popc(km & lanemask_lt());
+          sh.d[pos] = d32;
+          sh.t[pos] = t[w];
+          sh.m[pos] = mm;
+        }
+        total += __popc(km);
+      }
     }
   }
   __syncwarp();
@@ -1295,14 +1263,14 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
     }
   }
   if (Rs == 0) {
-    ++cnt.under;
+    if (lane == 0) ++sh.wc[kWcUnder];
     return false;
   }
   if (Rs < Rp)
-    ++cnt.over;
+    { if (lane == 0) ++sh.wc[kWcOver]; }
   else
-    ++cnt.exact;
-  cnt.shells += unsigned(Rs);
+    { if (lane == 0) ++sh.wc[kWcExact]; }
+  if (lane == 0) sh.wc[kWcShells] += unsigned(Rs);
 
   // 3. select: two-level histogram over candidates of shells <= R* within B(R*)
   const float Bs_hi = fr.sel_bhi[Rs];
@@ -1360,64 +1328,70 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   }
   const float TS = fminf(__fadd_ru(T, __fmul_ru(3.f, __fmaf_ru(T, 8.f * kU32, beta_s))), Bs_hi);
 
-  // S = shells <= R*, d32 <= TS, staged in shared memory in candidate order
+  // S = shells <= R*, d32 <= TS: buffer positions compacted first, then every
+  // lane recomputes its S elements in exact FP64 at once
   int nS = 0;
   for (int i0 = 0; i0 < total; i0 += 32) {
     const int i = i0 + lane;
     const bool in = i < total && int(sh.m[i] & 255u) <= Rs && sh.d[i] <= TS;
     const unsigned m = __ballot_sync(kFull, in);
-    if (nS + __popc(m) > 64) return false;  // S larger than the sort
-    if (in) {
-      const int q = nS + __popc(m & lanemask_lt());
-      sh.sd[q] = exact(i);
-      sh.sj[q] = b.sidx[sh.t[i]];
-    }
+    if (nS + __popc(m) > 64) return false;  // S larger than the row buffer
+    if (in) sh.si[nS + __popc(m & lanemask_lt())] = i;
     nS += __popc(m);
   }
   __syncwarp();
   if (nS < k) return false;  // cannot happen: T bounds k candidates
   if (lane == 0) cnt.rerank += unsigned(nS);
-  const int i = b.sidx[p];
-  int *row = b.out_nn + fr.out_base + (long long)i * k;
-  double *drow = b.out_d2 ? b.out_d2 + fr.out_base + (long long)i * k : nullptr;
-  if (nS <= 32) {
-    double d = lane < nS ? sh.sd[lane] : pinf();
-    int j = lane < nS ? sh.sj[lane] : 0x7fffffff;
-    warp_sort32(d, j, lane);
-    // 4. a tie across the k-th slot: (k-1)-th and k-th sorted values
-    const double vk = __shfl_sync(kFull, d, k - 1);
-    const double vn = __shfl_sync(kFull, d, k & 31);
-    if (nS > k && vn == vk) {
-      ++cnt.replays;
-      return false;
-    }
-    if (lane < k) {
-      row[lane] = j;
-      if (drow) drow[lane] = d;
-    }
-  } else {
-    double sd[2];
-    int sj[2];
+  double ed[2];
+  int ej[2];
 #pragma unroll
-    for (int s = 0; s < 2; ++s) {
-      const int q = s * 32 + lane;
-      sd[s] = q < nS ? sh.sd[q] : pinf();
-      sj[s] = q < nS ? sh.sj[q] : 0x7fffffff;
+  for (int h = 0; h < 2; ++h) {
+    const int q = lane + 32 * h;
+    ed[h] = pinf();
+    ej[h] = 0x7fffffff;
+    if (q < nS) {
+      const int i = sh.si[q];
+      ed[h] = exact(i);
+      ej[h] = b.sidx[sh.t[i]];
+      sh.sd[q] = ed[h];
+      sh.sj[q] = ej[h];
     }
-    warp_sort64(sd, sj, lane);
-    const double vk = __shfl_sync(kFull, sd[(k - 1) >> 5], (k - 1) & 31);
-    const double vn = __shfl_sync(kFull, sd[k >> 5], k & 31);
-    if (nS > k && vn == vk) {
-      ++cnt.replays;
-      return false;
+  }
+  __syncwarp();
+  // 4. rank of each element in (d2, index) order; the first k are the row
+  int rk[2] = {0, 0};
+  for (int e = 0; e < nS; ++e) {
+    const double de = sh.sd[e];
+    const int je = sh.sj[e];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) rk[h] += lex_less(de, je, ed[h], ej[h]) ? 1 : 0;
+  }
+  const FrameDesc &frr = fr;
+  const int i = b.sidx[p];
+  int *row = b.out_nn + frr.out_base + (long long)i * k;
+  double *drow = b.out_d2 ? b.out_d2 + frr.out_base + (long long)i * k : nullptr;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    if (lane + 32 * h < nS) {
+      if (rk[h] == k - 1) sh.hmax[0] = __double2loint(ed[h]), sh.hmax[1] = __double2hiint(ed[h]);
+      if (rk[h] == k) sh.hmax[2] = __double2loint(ed[h]), sh.hmax[3] = __double2hiint(ed[h]);
     }
-    if (lane < k) {
-      row[lane] = sj[0];
-      if (drow) drow[lane] = sd[0];
+  }
+  __syncwarp();
+  // a tie across the k-th slot: the k-th and (k+1)-th values are equal
+  if (nS > k && sh.hmax[0] == sh.hmax[2] && sh.hmax[1] == sh.hmax[3]) {
+    if (lane == 0) ++sh.wc[kWcReplays];
+    return false;
+  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    if (lane + 32 * h < nS && rk[h] < k) {
+      row[rk[h]] = ej[h];
+      if (drow) drow[rk[h]] = ed[h];
     }
   }
   if (b.stop_log && lane == 0) b.stop_log[p] = int8_t(Rs);
-  cnt.inserts += unsigned(k);
+  if (lane == 0) sh.wc[kWcInserts] += unsigned(k);
   return true;
 }
 
@@ -1427,6 +1401,8 @@ __global__ void __launch_bounds__(kSelWarps * 32, 3) k_select_walk(BatchBuffers 
   const long long total = b.off[b.ncells];
   const int lane = threadIdx.x & 31;
   SelCounters cnt;
+  if (lane < 8) sh.wc[lane] = 0;
+  __syncwarp();
   constexpr int kGrab = 16;  // consecutive sources share most candidates (L1 reuse)
   for (;;) {
     uint32_t base = 0;
@@ -1436,9 +1412,9 @@ __global__ void __launch_bounds__(kSelWarps * 32, 3) k_select_walk(BatchBuffers 
     for (int q = 0; q < kGrab; ++q) {
       const long long p = (long long)base + q;
       if (p >= total) break;
-      const unsigned tie = cnt.replays;
+      const unsigned long long tie = sh.wc[kWcReplays];
       if (!select_source(b, p, lane, sh, cnt)) {
-        if (cnt.replays == tie) ++cnt.fallback;
+        if (lane == 0 && sh.wc[kWcReplays] == tie) ++sh.wc[kWcFallback];
         if (lane == 0) push_replay(b, p);
       }
       __syncwarp();
@@ -1452,13 +1428,13 @@ __global__ void __launch_bounds__(kSelWarps * 32, 3) k_select_walk(BatchBuffers 
     atomicAdd(&c[kCntPairs], pairs);
     atomicAdd(&c[kCntPruned], pruned);
     atomicAdd(&c[kCntRerank], rerank);
-    atomicAdd(&c[kCntInserts], cnt.inserts);
-    atomicAdd(&c[kCntShells], cnt.shells);
-    atomicAdd(&c[kCntReplays], cnt.replays + cnt.fallback);
-    atomicAdd(&c[kCntPropUnder], cnt.under);
-    atomicAdd(&c[kCntPropOver], cnt.over);
-    atomicAdd(&c[kCntPropExact], cnt.exact);
-    atomicAdd(&c[kCntFallback], cnt.fallback);
+    atomicAdd(&c[kCntInserts], sh.wc[kWcInserts]);
+    atomicAdd(&c[kCntShells], sh.wc[kWcShells]);
+    atomicAdd(&c[kCntReplays], sh.wc[kWcReplays] + sh.wc[kWcFallback]);
+    atomicAdd(&c[kCntPropUnder], sh.wc[kWcUnder]);
+    atomicAdd(&c[kCntPropOver], sh.wc[kWcOver]);
+    atomicAdd(&c[kCntPropExact], sh.wc[kWcExact]);
+    atomicAdd(&c[kCntFallback], sh.wc[kWcFallback]);
   }
 }
 
