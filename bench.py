@@ -42,7 +42,7 @@ MODE_NAMES = {0: "plain_f64", 1: "fast_f32", 2: "learned", 3: "replay"}
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=60)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--mode", type=int, default=-1, help="walk mode; -1 = best available")
@@ -61,6 +61,24 @@ def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
+
+
+def max_over_ranks(x: float, device: str) -> float:
+    """The largest x over the ranks of the default process group (x itself
+    without one): every multi-GPU time is the slowest rank's."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: int, steps: int, max_ms: float, world: int) -> float:
+    """Units of all ranks per second over the slowest rank's time (weak
+    scaling: every rank searches its own frame)."""
+    return world * units_per_rank * steps / (max_ms / 1000.0)
 
 
 def workload(n, k, seed):
@@ -247,7 +265,7 @@ def run_ours(args):
             torch.distributed.barrier()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(steps)]
-        walk_ms, prep_ms, replay_ms = [], [], []
+        walk_ms, prep_ms, replay_ms, prop_ms = [], [], [], []
         counters = None
         for s in range(steps):
             with torch.cuda.stream(tstream):
@@ -257,9 +275,12 @@ def run_ours(args):
             with torch.cuda.stream(tstream):
                 ev[s][1].record(tstream)
             L.lc_gpu_wait(ws)
-            pp, pw, pr = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
-            L.lc_gpu_phase_times(ws, ctypes.byref(pp), ctypes.byref(pw), ctypes.byref(pr))
-            walk_ms.append(pw.value)
+            pp, pq, pw, pr = (ctypes.c_double(), ctypes.c_double(), ctypes.c_double(),
+                              ctypes.c_double())
+            L.lc_gpu_phase_times4(ws, ctypes.byref(pp), ctypes.byref(pq), ctypes.byref(pw),
+                                  ctypes.byref(pr))
+            walk_ms.append(pw.value)  # the walk kernel alone
+            prop_ms.append(pq.value)
             prep_ms.append(pp.value)
             replay_ms.append(pr.value)
         torch.cuda.synchronize()
@@ -267,39 +288,41 @@ def run_ours(args):
         L.lc_gpu_stats(ws, buf, 16, None)
         counters = list(buf)
         counters.append(int(L.lc_gpu_get_tpp(ws)))  # walk design used (autotuned unless forced)
-        total = sum(a.elapsed_time(b) for a, b in ev)
-        if world > 1:
-            t = torch.tensor([total], dtype=torch.float64, device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            total = float(t.item())
-        return total, walk_ms, counters, prep_ms, replay_ms
+        total = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), "cuda")
+        return total, walk_ms, counters, prep_ms, replay_ms, prop_ms
 
     best_mode = args.mode if args.mode >= 0 else 2
     # plain FP64 walk (the 2x denominator), then the headline mode
-    plain_total, plain_walk, plain_cnt, _, _ = time_mode(0, max(3, args.steps // 2), args.warmup)
     sampler = ClockSampler(dev)
-    sampler.start()
-    total, walk_ms, cnt, prep_ms, replay_ms = time_mode(best_mode, args.steps, args.warmup)
+    sampler.start()  # clocks over both timed regions
+    time.sleep(0.3)  # nvidia-smi start-up
+    plain_total, plain_walk, plain_cnt, _, _, _ = time_mode(0, max(3, args.steps // 2),
+                                                            args.warmup)
+    total, walk_ms, cnt, prep_ms, replay_ms, prop_ms = time_mode(best_mode, args.steps,
+                                                                 args.warmup)
     sampler.stop()
     ms_per_step = total / args.steps
-    value = world * n * args.steps / (total / 1000.0)
-    plain_value = world * n * max(3, args.steps // 2) / (plain_total / 1000.0)
+    value = whole_job_rate(n, args.steps, total, world)
+    plain_value = whole_job_rate(n, max(3, args.steps // 2), plain_total, world)
 
     # roofline of the dominant kernel (the walk): algorithmic bytes per launch
     peak, peak_kind = measured_peaks()
-    walk_bytes = n * (32 + 12 * k)
+    # per source: FP32 record 16 B + FP64 coordinates 24 B + index and cell 8 B read,
+    # the output row (i32 + f64 per slot) written
+    walk_bytes = n * (48 + 12 * k)
     walk_avg_ms = statistics.mean(walk_ms)
     achieved = walk_bytes / (walk_avg_ms / 1000.0) / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "walk_bimodal_4M_k32_traffic.txt")
+    tname = "select_walk" if best_mode == 2 else "walk"
+    tpath = os.path.join(ROOT, "profiles", f"{tname}_bimodal_4M_k32_traffic.txt")
     if os.path.exists(tpath):
         for line in open(tpath):
             if line.startswith("traffic_bytes_per_launch:"):
                 traffic = float(line.split(":")[1])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "peak_source": f"{peak_kind} hbm_gbs", "kernel": "walk",
-                "algorithmic_bytes_per_source": 32 + 12 * k}
+                "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_select_walk" if best_mode == 2 else "walk",
+                "algorithmic_bytes_per_source": 48 + 12 * k}
 
     # end to end through the host C ABI with pinned buffers
     e2e = None
@@ -327,12 +350,8 @@ def run_ours(args):
             t0 = time.perf_counter()
             host_step()
             times.append(time.perf_counter() - t0)
-        tot = sum(times)
-        if world > 1:
-            t = torch.tensor([tot], dtype=torch.float64, device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            tot = float(t.item())
-        e2e = {"value": world * n * args.steps / tot, "unit": "sources/s",
+        tot = max_over_ranks(sum(times), "cuda")
+        e2e = {"value": whole_job_rate(n, args.steps, 1000.0 * tot, world), "unit": "sources/s",
                "h2d_bytes_per_step": n * 24, "d2h_bytes_per_step": n * k * 12,
                "ms_per_step": 1000.0 * tot / args.steps, "timer": "host wall clock around the call"}
 
@@ -343,7 +362,9 @@ def run_ours(args):
     names = ["pairs", "inserts", "replays", "shells", "pruned", "reranks", "prop_under",
              "prop_over", "prop_exact", "revisited", "fallback"]
     walk_stats = {nm: cnt[i] for i, nm in enumerate(names)}  # counters of the last step
-    launches_per_step = 6
+    # our kernels per step: fold, scan, slots, records, walk, replay; the learned
+    # mode adds the proposal network and the per-source proposal gather
+    launches_per_step = 6 + (2 if (best_mode == 2 and model_info is not None) else 0)
     out = {"metric": METRIC, "value": value, "unit": "sources/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -359,6 +380,7 @@ def run_ours(args):
                           "walk_ms": statistics.mean(plain_walk), "tpp": plain_cnt[-1]},
            "speedup_vs_plain": value / plain_value, "walk_ms": walk_avg_ms,
            "prep_ms": statistics.mean(prep_ms), "replay_ms": statistics.mean(replay_ms),
+           "propose_ms": statistics.mean(prop_ms),
            "walk_stats_last_step": walk_stats, "model": model_info,
            "plain_walk_stats_last_step": {nm: plain_cnt[i] for i, nm in enumerate(names)}}
     if rank == 0:

@@ -159,6 +159,10 @@ int lc_gpu_stats(lc_gpu_workspace *ws, long long *counters, int n_counters, doub
  * workspace stream: fold + bin + scan + placement, the walk kernel, and the
  * exact replay of tied sources. Waits for the search to finish. */
 int lc_gpu_phase_times(lc_gpu_workspace *ws, double *prep_ms, double *walk_ms, double *replay_ms);
+/* The same split with the learned mode's shell proposals apart: walk_ms is
+ * then the walk kernel alone. */
+int lc_gpu_phase_times4(lc_gpu_workspace *ws, double *prep_ms, double *propose_ms, double *walk_ms,
+                        double *replay_ms);
 
 /* One frame of a heterogeneous batch: its own point count, cell, k and
  * hint. Frames are packed back to back in xyz (3 doubles per point) and in

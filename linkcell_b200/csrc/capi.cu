@@ -612,6 +612,21 @@ int lc_gpu_phase_times(lc_gpu_workspace *ws, double *prep_ms, double *walk_ms, d
   return 0;
 }
 
+int lc_gpu_phase_times4(lc_gpu_workspace *ws, double *prep_ms, double *propose_ms, double *walk_ms,
+                        double *replay_ms) {
+  if (!ws) return gpu_fail(Code::NullPointer);
+  lc::Stats st;
+  std::string detail;
+  const Code c = ws->ws.fetch_stats(st, detail);
+  if (c != Code::Ok) return gpu_fail(c, detail);
+  if (prep_ms) *prep_ms = st.ms_prep;
+  if (propose_ms) *propose_ms = st.ms_propose;
+  if (walk_ms) *walk_ms = st.ms_walk - st.ms_propose;
+  if (replay_ms) *replay_ms = st.ms_replay;
+  gpu_ok();
+  return 0;
+}
+
 int lc_gpu_knearest_batch(lc_gpu_workspace *ws, const double *xyz, const lc_frame *fr,
                           size_t n_frames, const int *mask, int *out_nn, double *out_d2,
                           int wait) {

@@ -7,7 +7,10 @@
 
 #include "lc_mlp.h"
 
+#include <dlfcn.h>
+
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -207,6 +210,18 @@ void fill_select_tables(FrameDesc &fd) {
   fd.inv_nxy = 1.0 / (double(fd.nx) * double(fd.ny));
 }
 
+// Device address of page-locked host memory, or null (pageable, device or
+// unknown memory).
+void *mapped_host(const void *p) {
+  if (!p) return nullptr;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
 // ------------------------------------------------------------ workspace
 WorkspaceImpl::WorkspaceImpl() {
   // Environment overrides: LINKCELL_MODE (walk mode), LINKCELL_BLOCK
@@ -223,6 +238,7 @@ WorkspaceImpl::WorkspaceImpl() {
       opts.tpp_forced = true;
     }
   }
+  if (const char *z = std::getenv("LINKCELL_ZERO_COPY")) zero_copy_ = std::atoi(z) != 0;
   if (const char *b = std::getenv("LINKCELL_BLOCK")) {
     const int v = std::atoi(b);
     if (v == 32 || v == 64 || v == 128 || v == 256) opts.block = v;
@@ -355,7 +371,13 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   LC_TRY(grow(frames_, size_t(nf)));
   LC_TRY(grow(counters_, size_t(kNumCounters)));
   if (opts.log_shells) LC_TRY(grow(stop_log_, P));
-  const bool learned = opts.mode == kModeLearned && kmax <= 256;
+  if (opts.mode == kModeLearned && !has_model_ && opts.fixed_proposal <= 0 && !model_tried_) {
+    model_tried_ = true;
+    load_default_model();  // the shipped network, when it can be found
+  }
+  // without a network (or fixed proposal) the learned mode is the FP32 walk
+  const bool learned =
+      opts.mode == kModeLearned && kmax <= 256 && (opts.fixed_proposal > 0 || has_model_);
   if (learned) {
     LC_TRY(grow(proposal_, P));
     if (opts.fixed_proposal <= 0 && has_model_) LC_TRY(grow(cell_prop_, C));
@@ -556,11 +578,44 @@ Code WorkspaceImpl::enqueue(BatchBuffers &b, const WalkLaunch &wl, int nf, size_
       LC_TRY(cudaMemsetAsync(proposal_.p, 0, P, s));
     }
   }
+  if (timed) LC_TRY(cudaEventRecord(ev_[4], s));
   LC_TRY(launch_walk(b, wl, s));
   if (timed) LC_TRY(cudaEventRecord(ev_[2], s));
   LC_TRY(launch_replay(b, s));
   if (timed) LC_TRY(cudaEventRecord(ev_[3], s));
   return Code::Ok;
+}
+
+// The shipped shell-proposal network: LINKCELL_MODEL, else data/shell_mlp.f32
+// beside this shared library. File: "LCMLP001", i32 n, f32 tau, i32 meta
+// length, meta bytes, n f32 parameters (little-endian).
+bool WorkspaceImpl::load_default_model() {
+  std::string path;
+  if (const char *e = std::getenv("LINKCELL_MODEL")) {
+    path = e;
+  } else {
+    Dl_info info;
+    if (!dladdr(reinterpret_cast<void *>(&mapped_host), &info) || !info.dli_fname) return false;
+    path = info.dli_fname;
+    const size_t slash = path.rfind('/');
+    path = (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) +
+           "/data/shell_mlp.f32";
+  }
+  FILE *fh = std::fopen(path.c_str(), "rb");
+  if (!fh) return false;
+  char magic[8];
+  int32_t n = 0, ml = 0;
+  float tau = 0.f;
+  bool ok = std::fread(magic, 1, 8, fh) == 8 && std::memcmp(magic, "LCMLP001", 8) == 0 &&
+            std::fread(&n, 4, 1, fh) == 1 && std::fread(&tau, 4, 1, fh) == 1 &&
+            std::fread(&ml, 4, 1, fh) == 1 && n == kMlpParams && ml >= 0 && ml < (1 << 20) &&
+            std::fseek(fh, ml, SEEK_CUR) == 0;
+  std::vector<float> params(ok ? size_t(n) : 0);
+  ok = ok && std::fread(params.data(), 4, size_t(n), fh) == size_t(n);
+  std::fclose(fh);
+  if (!ok || !(tau > 0.f && tau <= 1.f)) return false;
+  std::string detail;
+  return set_model(params.data(), params.size(), tau, detail) == Code::Ok;
 }
 
 Code WorkspaceImpl::set_model(const float *params, size_t n, float tau, std::string &detail) {
@@ -624,13 +679,15 @@ Code WorkspaceImpl::fetch_stats(Stats &out, std::string &detail) {
     out.ms_total = t;
   } else if (timed_) {
     LC_TRY(cudaEventSynchronize(ev_[3]));
-    float a = 0.f, b = 0.f, c = 0.f, t = 0.f;
+    float a = 0.f, b = 0.f, c = 0.f, t = 0.f, q = 0.f;
     LC_TRY(cudaEventElapsedTime(&a, ev_[0], ev_[1]));
     LC_TRY(cudaEventElapsedTime(&b, ev_[1], ev_[2]));
     LC_TRY(cudaEventElapsedTime(&c, ev_[2], ev_[3]));
     LC_TRY(cudaEventElapsedTime(&t, ev_[0], ev_[3]));
+    LC_TRY(cudaEventElapsedTime(&q, ev_[1], ev_[4]));
     out.ms_prep = a;
     out.ms_walk = b;
+    out.ms_propose = q;
     out.ms_replay = c;
     out.ms_total = t;
   } else {
@@ -645,19 +702,36 @@ Code WorkspaceImpl::run_host(std::vector<FrameDesc> &frames, const double *xyz, 
                              const int *mask, size_t mask_n, int *out_nn, double *out_d2,
                              size_t out_n, std::string &detail) {
   const cudaStream_t s = stream();
+  // Output rows land in a random order, so they cannot be copied back in
+  // pieces while the walk runs. When the caller's output buffers are
+  // page-locked (mapped) host memory, the kernels write the rows straight
+  // into them over the host link instead, overlapping the transfer with the
+  // search; pageable buffers take the device copy and one copy back.
+  int *map_nn = nullptr;
+  double *map_d2 = nullptr;
+  if (zero_copy_) {
+    map_nn = static_cast<int *>(mapped_host(out_nn));
+    map_d2 = out_d2 ? static_cast<double *>(mapped_host(out_d2)) : nullptr;
+    if (!map_nn || (out_d2 && !map_d2)) map_nn = nullptr, map_d2 = nullptr;
+  }
   LC_TRY(grow(h_xyz_, xyz_n));
-  LC_TRY(grow(h_nn_, out_n));
-  if (out_d2) LC_TRY(grow(h_d2_, out_n));
+  if (!map_nn) {
+    LC_TRY(grow(h_nn_, out_n));
+    if (out_d2) LC_TRY(grow(h_d2_, out_n));
+  }
   if (mask) LC_TRY(grow(h_mask_, mask_n));
   LC_TRY(cudaMemcpyAsync(h_xyz_.p, xyz, xyz_n * sizeof(double), cudaMemcpyHostToDevice, s));
   if (mask)
     LC_TRY(cudaMemcpyAsync(h_mask_.p, mask, mask_n * sizeof(int), cudaMemcpyHostToDevice, s));
-  const Code c = run(frames, h_xyz_.p, mask ? h_mask_.p : nullptr, h_nn_.p,
-                     out_d2 ? h_d2_.p : nullptr, false, detail);
+  const Code c = run(frames, h_xyz_.p, mask ? h_mask_.p : nullptr, map_nn ? map_nn : h_nn_.p,
+                     out_d2 ? (map_nn ? map_d2 : h_d2_.p) : nullptr, false, detail);
   if (c != Code::Ok) return c;
-  LC_TRY(cudaMemcpyAsync(out_nn, h_nn_.p, out_n * sizeof(int), cudaMemcpyDeviceToHost, s));
-  if (out_d2)
-    LC_TRY(cudaMemcpyAsync(out_d2, h_d2_.p, out_n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  last_zero_copy = map_nn != nullptr;
+  if (!map_nn) {
+    LC_TRY(cudaMemcpyAsync(out_nn, h_nn_.p, out_n * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (out_d2)
+      LC_TRY(cudaMemcpyAsync(out_d2, h_d2_.p, out_n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
   LC_TRY(cudaStreamSynchronize(s));
   int st = 0;
   LC_TRY(cudaMemcpy(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost));

@@ -43,6 +43,8 @@ const char *gpu_message(Code c);
 Code plan_frame(const double *rows, const double *origin, double cell_hint, int k, FrameDesc &fd);
 // Fills the per-reach constants of the cube select walk (FrameDesc::sel_*).
 void fill_select_tables(FrameDesc &fd);
+// Device address of page-locked host memory, or null.
+void *mapped_host(const void *p);
 
 // Options that pick the walk.
 struct WalkOptions {
@@ -61,7 +63,8 @@ struct Stats {
   long long counters[kNumCounters] = {};
   double ms_total = 0.0;   // fold .. replay, device time
   double ms_prep = 0.0;    // fold + bin + scan + placement
-  double ms_walk = 0.0;    // the walk kernel(s)
+  double ms_walk = 0.0;    // shell proposals + the walk kernel(s)
+  double ms_propose = 0.0; // shell proposals alone (learned mode)
   double ms_replay = 0.0;  // exact replay of tied sources
 };
 
@@ -85,6 +88,7 @@ class WorkspaceImpl {
   WalkOptions opts;
   bool collect_stats = true;
   int last_tpp = 0;          // walk design of the last batch
+  bool last_zero_copy = false;  // the last host-pointer search wrote rows straight to host memory
   int graph_captures = 0;    // CUDA graphs captured so far
   // Counters and phase times of the last run (waits for it to finish).
   Code fetch_stats(Stats &out, std::string &detail);
@@ -137,6 +141,7 @@ class WorkspaceImpl {
   FrameDesc *h_frames_ = nullptr;
   size_t h_frames_cap_ = 0;
   cudaEvent_t ev_done_ = nullptr;
+  bool zero_copy_ = true;  // LINKCELL_ZERO_COPY=0 turns mapped output rows off
   bool done_pending_ = false;
   void release_all();
 
@@ -159,13 +164,15 @@ class WorkspaceImpl {
   Buf<uint32_t> shell_table_;
   bool shell_table_ready_ = false;
   bool has_model_ = false;
+  bool model_tried_ = false;  // the shipped network was looked for once
+  bool load_default_model();
   float tau_ = 0.9f;
   // host-pointer staging
   Buf<double> h_xyz_, h_d2_;
   Buf<int> h_mask_, h_nn_;
   Buf<unsigned long long> active_;
   BatchBuffers bb_;
-  cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // prep | propose | walk | replay
   bool timed_ = false;
 };
 
