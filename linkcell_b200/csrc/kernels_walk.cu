@@ -1081,28 +1081,44 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
     if (row < nrow) {
       const int qz = int((float(row) + 0.5f) * invW);  // exact: row < 289, W <= 17
       const int dy = row - qz * W - Rp, dz = qz - Rp;
-      const float gb = fmaxf(axis_gap(dy, fb), 0.f), gc = fmaxf(axis_gap(dz, fc), 0.f);
+      // row (dy, dz): offsets D_b in [dy - fb, dy + 1 - fb], D_c likewise
+      const float lo1 = float(dy) - fb, lo2 = float(dz) - fc;
+      const float hi1 = lo1 + 1.f, hi2 = lo2 + 1.f;
+      const float gb = fmaxf(0.f, fmaxf(lo1, -hi1)), gc = fmaxf(0.f, fmaxf(lo2, -hi2));
       const float Q = qlim - (gb * gb + gc * gc);
       if (Q >= 0.f) {
-        const float gm = sqrtf(Q) * 1.0001f + 1e-4f;
-        const int dxh = int(floorf(fminf(fa + gm, float(Rp))));
-        const int dxl = -int(floorf(fminf(gm + 1.f - fa, float(Rp))));
-        cnt.pruned += unsigned(W - (dxh - dxl + 1));
+        const float r01 = fr.sel_r01, r02 = fr.sel_r02;
+        const float cmin = -(fmaxf(r01 * lo1, r01 * hi1) + fmaxf(r02 * lo2, r02 * hi2));
+        const float cmax = -(fminf(r01 * lo1, r01 * hi1) + fminf(r02 * lo2, r02 * hi2));
+        const float hm = sqrtf(fr.sel_ls00 * Q) * 1.0001f + 1e-4f;
+        // cells dx with [dx - fa, dx + 1 - fa] meeting [cmin - hm, cmax + hm]:
+        // dx <= cmax + hm + fa and dx >= cmin - hm + fa - 1 (with margins)
+        const int dxh = int(floorf(fminf(cmax + hm + fa + 1e-4f, float(Rp))));
+        const int dxl = -int(floorf(fminf(1.f - (cmin - hm) - fa + 1e-4f, float(Rp))));
+        cnt.pruned += unsigned(W - max(0, dxh - dxl + 1));
         int cy = iy + dy, wb = 0, cz = iz + dz, wc = 0;
         if (cy < 0) { cy += ny; wb = -1; } else if (cy >= ny) { cy -= ny; wb = 1; }
         if (cz < 0) { cz += nz; wc = -1; } else if (cz >= nz) { cz -= nz; wc = 1; }
         const int rowbase = (cz * ny + cy) * nx;
         const uint32_t *o = b.off + cb + rowbase;
-        const int xl = ix + dxl, xh = ix + dxh;
-        rw.startA = int(o[max(xl, 0)]);
-        lenA = int(o[min(xh, nx - 1) + 1]) - rw.startA;
+        const int xl = ix + dxl, xh = ix + dxh;  // empty when dxl > dxh
+        // the cells inside the box, then the ones across the x boundary (one
+        // side only: the range spans at most 2 Rp + 1 <= nx cells)
+        const int a0 = max(xl, 0), a1 = min(xh, nx - 1);
+        rw.startA = 0;
+        if (a0 <= a1) {
+          rw.startA = int(o[a0]);
+          lenA = int(o[a1 + 1]) - rw.startA;
+        }
         int wrapB = 0, sB = 0;
-        if (xl < 0) {
+        if (xl < 0 && xl <= xh) {
+          const int b1 = min(xh, -1);
           sB = int(o[xl + nx]);
-          lenB = int(o[nx]) - sB;
+          lenB = int(o[b1 + nx + 1]) - sB;
           wrapB = -1;
-        } else if (xh >= nx) {
-          sB = int(o[0]);
+        } else if (xh >= nx && xl <= xh) {
+          const int b0 = max(xl, nx);
+          sB = int(o[b0 - nx]);
           lenB = int(o[xh - nx + 1]) - sB;
           wrapB = 1;
         }

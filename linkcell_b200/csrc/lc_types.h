@@ -64,7 +64,9 @@ struct FrameDesc {
   // FP32 error offset beta (rounded up), B(R) + 2 band(B(R)) rounded up,
   // and the error band of sqrt(d32) / cell_min near an integer.
   float sel_thr[9];
-  float sel_qlim[9];
+  float sel_qlim[9];       // thr / lam_s, lam_s = 0.99 x the smallest eigenvalue of the (b, c) Schur form
+  float sel_r01, sel_r02;  // M_ab / M_aa, M_ac / M_aa of the bin-unit metric M = E^T E
+  float sel_ls00;          // lam_s / M_aa
   float sel_beta[9];
   float sel_bhi[9];
   float sel_epsr[9];

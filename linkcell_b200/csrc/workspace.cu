@@ -192,6 +192,30 @@ float float_up(double v) {
 // bounded by u D^2 + e^2 / u); 1e-6 of margin on top.
 void fill_select_tables(FrameDesc &fd) {
   const double u = 5.9604644775390625e-08;  // 2^-24
+  // Row trimming: in bin units the squared distance of an offset D is
+  // D^T M D with M = E^T E. For fixed (D_b, D_c) the D_a giving at most thr
+  // lie within h of c = -(M_ab D_b + M_ac D_c) / M_aa, h^2 = (thr - S) / M_aa,
+  // S the Schur form of (D_b, D_c), bounded below by lam_s |(D_b, D_c)|^2.
+  double E[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int r = 0; r < 3; ++r) E[a][r] = fd.h[a * 3 + r] / double(a == 0 ? fd.nx : (a == 1 ? fd.ny : fd.nz));
+  double M[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) M[i][j] = E[i][0] * E[j][0] + E[i][1] * E[j][1] + E[i][2] * E[j][2];
+  const double s11 = M[1][1] - M[0][1] * M[0][1] / M[0][0];
+  const double s12 = M[1][2] - M[0][1] * M[0][2] / M[0][0];
+  const double s22 = M[2][2] - M[0][2] * M[0][2] / M[0][0];
+  const double tr = 0.5 * (s11 + s22), df = 0.5 * (s11 - s22);
+  double lam_s = std::max(0.0, tr - std::sqrt(df * df + s12 * s12)) * 0.99;
+  fd.sel_r01 = float(M[0][1] / M[0][0]);
+  fd.sel_r02 = float(M[0][2] / M[0][0]);
+  fd.sel_ls00 = float(lam_s / M[0][0]);
+  if (!(lam_s > 1e-9 * M[0][0])) {
+    // near-degenerate metric: the isotropic bound lam_min |D|^2 <= thr instead
+    lam_s = double(float(fd.lam_min) * 0.99f);
+    fd.sel_r01 = fd.sel_r02 = 0.f;
+    fd.sel_ls00 = 1.f;
+  }
   for (int R = 0; R <= 8; ++R) {
     const int Ru = R < 1 ? 1 : R;
     const double e = u * (6.0 * Ru + 8.0) * double(fd.ell) + fd.eps64 * (Ru + 2.0);
@@ -202,8 +226,7 @@ void fill_select_tables(FrameDesc &fd) {
     fd.sel_beta[R] = float_up(beta);
     fd.sel_thr[R] = float_up(B * (1.0 + 8.0 * u) + beta);
     fd.sel_bhi[R] = float_up(B + 2.0 * band);
-    const double lam = double(float(fd.lam_min) * 0.99f);
-    fd.sel_qlim[R] = lam > 0.0 ? float_up(double(fd.sel_thr[R]) / lam * 1.0001) : 3.0e38f;
+    fd.sel_qlim[R] = lam_s > 0.0 ? float_up(double(fd.sel_thr[R]) / lam_s * 1.0001) : 3.0e38f;
     fd.sel_epsr[R] = float_up(band / (2.0 * fd.cell_min * fd.cell_min) + 16.0 * u * (Ru + 2.0));
   }
   fd.inv_nx = 1.0 / double(fd.nx);
