@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--workload", default="c2", choices=["c2", "c3"],
+                   help="c2: the 4M bimodal frame (headline); c3: 256 frames of uneven n, "
+                        "cell, k and mask in one batched call")
     return p.parse_args()
 
 
@@ -390,10 +393,142 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def run_c3(args):
+    """C3: 256 frames of their own sheared cells, densities, k in {4, 8, 16, 32}
+    and masks (linkcell_b200.workloads.frames_batch, seed 3) searched by one
+    lc_gpu_knearest_batch call per step, the launch sequence captured once in
+    a CUDA graph and replayed. value = active sources of all frames per
+    second (device time); e2e adds the host copies of the coordinates in and
+    of the rows out."""
+    import torch
+    world, rank, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    from linkcell_b200 import _capi, _cell_struct, learn, workloads as W
+    from linkcell_b200 import build as B
+    B.build()
+    L = _capi.load()
+    frames = W.frames_batch(256, seed=3 + rank)
+    arr = (_capi.LcFrame * len(frames))()
+    total_out, moff, active = 0, 0, 0
+    for f, fr in enumerate(frames):
+        arr[f].n, arr[f].k = fr["n"], fr["k"]
+        arr[f].cell = _cell_struct(np.asarray(fr["cell"], dtype=np.float64))
+        arr[f].cell_hint = 3.0
+        arr[f].mask_offset = moff
+        moff += fr["n"]
+        total_out += fr["n"] * fr["k"]
+        active += int(fr["mask"].sum())
+    xyz_h = np.concatenate([fr["xyz"] for fr in frames])
+    mask_h = np.concatenate([fr["mask"] for fr in frames]).astype(np.int32)
+    x = torch.as_tensor(xyz_h, device="cuda")
+    m = torch.as_tensor(mask_h, device="cuda")
+    nn = torch.empty(total_out, dtype=torch.int32, device="cuda")
+    d2 = torch.empty(total_out, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    ws = L.lc_gpu_workspace_new()
+    assert ws, _capi.gpu_error()
+    learn.attach(ws)
+    assert L.lc_gpu_set_graph(ws, 1) == 0
+    if args.tpp:
+        assert L.lc_gpu_set_tpp(ws, args.tpp) == 0
+    tstream = torch.cuda.ExternalStream(ctypes.c_void_p(L.lc_gpu_queue(ws)).value)
+
+    def step():
+        rc = L.lc_gpu_knearest_batch(ws, x.data_ptr(), arr, len(frames), m.data_ptr(),
+                                     nn.data_ptr(), d2.data_ptr(), 0)
+        assert rc == 0, _capi.gpu_error()
+
+    def time_mode(mode, steps):
+        assert L.lc_gpu_set_mode(ws, mode) == 0
+        for _ in range(args.warmup):
+            step()
+            L.lc_gpu_wait(ws)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        for i in range(steps):
+            with torch.cuda.stream(tstream):
+                flush.fill_(i & 0xFF)
+                ev[i][0].record(tstream)
+            step()
+            with torch.cuda.stream(tstream):
+                ev[i][1].record(tstream)
+        L.lc_gpu_wait(ws)
+        torch.cuda.synchronize()
+        return max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), "cuda")
+
+    sampler = ClockSampler(dev)
+    sampler.start()
+    time.sleep(0.3)
+    plain_ms = time_mode(0, max(3, args.steps // 2))
+    total_ms = time_mode(2, args.steps)
+    sampler.stop()
+    value = whole_job_rate(active, args.steps, total_ms, world)
+    plain_value = whole_job_rate(active, max(3, args.steps // 2), plain_ms, world)
+    captures = int(L.lc_gpu_graph_captures(ws))
+
+    # end to end: pinned host coordinates in, rows out, every step
+    xh = torch.as_tensor(xyz_h).pin_memory()
+    nnh = torch.empty(total_out, dtype=torch.int32).pin_memory()
+    d2h = torch.empty(total_out, dtype=torch.float64).pin_memory()
+    times = []
+    for i in range(args.warmup + args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with torch.cuda.stream(tstream):
+            x.copy_(xh, non_blocking=True)
+        step()
+        with torch.cuda.stream(tstream):
+            nnh.copy_(nn, non_blocking=True)
+            d2h.copy_(d2, non_blocking=True)
+        tstream.synchronize()
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(sum(times), "cuda")
+    ks = sorted({fr["k"] for fr in frames})
+    out = {"metric": "kNN sources/s, C3: 256 frames of uneven n, cell, k and mask, 1 B200, "
+                     "exact indices",
+           "value": value, "unit": "sources/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "c3_256_frames", "frames": len(frames), "points": int(moff),
+                      "active_sources": active, "k": ks, "mode": "learned", "graph": True,
+                      "graph_captures": captures, "parallelism": f"replicas x{world}",
+                      "l2": "flushed between timed steps (256 MB write)"},
+           "roofline": None, "cpu_baseline": None,
+           "e2e": {"value": whole_job_rate(active, args.steps, 1000.0 * e2e_s, world),
+                   "unit": "sources/s", "h2d_bytes_per_step": int(xyz_h.nbytes),
+                   "d2h_bytes_per_step": int(total_out * 12),
+                   "timer": "host wall clock around copy in, search, copy out"},
+           "gpu_launches": None, "clocks": sampler.summary(),
+           "plain_fp64": {"value": plain_value, "unit": "sources/s"},
+           "speedup_vs_plain": value / plain_value}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    # the copies above ran on the workspace's stream: release every tensor
+    # that recorded it before the stream goes away with the workspace
+    torch.cuda.synchronize()
+    del x, m, nn, d2, xh, nnh, d2h, flush
+    L.lc_gpu_workspace_free(ws)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "c3":
+        run_c3(args)
     else:
         run_ours(args)
 

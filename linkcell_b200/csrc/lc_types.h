@@ -26,6 +26,7 @@ enum StatusBits : int {
   kStatusScanTimeout = 1,    // decoupled look-back wait ran out of iterations
   kStatusBadIndex = 2,       // a kernel saw an offset outside its buffers
   kStatusReplayOverflow = 4, // replay queue longer than its buffer
+  kStatusMmaTimeout = 8,     // a tensor-core product did not complete in bounded time
 };
 
 // Per-frame flags (frame_flags[f]).
@@ -58,7 +59,7 @@ struct FrameDesc {
   long long cell_base;  // first cell of the frame in the batch
   long long out_base;   // first output element (row 0, slot 0)
   long long mask_base;  // offset of the frame's mask (shared masks repeat 0)
-  long long row_tile_base;  // first 16-cell row tile of the frame (shell proposals)
+  long long seg_base;  // first 32-cell row segment of the frame (shell proposals)
   // Cube select walk, per reach R = 1..8 (index R): the FP32 filter at
   // B(R) = (R cell_min)^2, the row-trimming limit thr / (0.99 lam_min), the
   // FP32 error offset beta (rounded up), B(R) + 2 band(B(R)) rounded up,

@@ -8,17 +8,18 @@
 //   - forward (k_dense: tiled FP32 GEMM with bias and optional SiLU),
 //     softmax cross-entropy, backward (GEMMs for input and weight
 //     gradients, SiLU derivative), and Adam;
-//   - k_cell_proposal_tc: inference over 16-cell row tiles on the tensor
-//     cores (mma.sync FP16, FP32 accumulation; layer 1 as a 5x5x5
-//     convolution of the staged occupancy halo), writing the proposed shell
-//     of every occupied cell (the smallest R with P(settled shell <= R) >=
-//     tau); the walk reads it for each source.
+//   - k_cell_proposal_tc: inference over 128-cell tiles on the tcgen05
+//     tensor cores (FP16 operands in shared memory, FP32 accumulators in
+//     tensor memory; layer 1 as a 5x5x5 convolution of the staged occupancy
+//     halo), writing the proposed shell of every cell (the smallest R with
+//     P(settled shell <= R) >= tau); the walk reads it for each source.
 //
 // Parameter layout (floats): W1[64][126] b1[64] W2[64][64] b2[64]
 // W3[8][64] b3[8].
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "lc_kernels.h"
@@ -252,248 +253,408 @@ __global__ void k_training_rows(BatchBuffers b, const int8_t *__restrict__ stop_
 }
 
 // ---------------------------------------------------------------------
-// Tensor-core inference: mma.sync m16n8k16 FP16 (FP32 accumulate; FP16 keeps
-// the 10-bit significand of TF32). One warp evaluates a row tile of 16
-// consecutive cells along x: layer 1 is [16 x 128] x [128 x 64] (126
-// features padded with zeros), layer 2 [16 x 64] x [64 x 64], layer 3
-// [16 x 64] x [64 x 8]. The 125 occupancy features of the tile's cells all
-// come from one 20 x 5 x 5 halo of log(1 + occupancy) values staged in
-// shared memory, so layer 1 is a 5x5x5 convolution: A[m][f] =
-// halo[yz(f)][m + dx(f)], read through a 128-entry offset table. The hidden
-// layers go through shared memory to change from the accumulator layout to
-// the A-operand layout.
-constexpr int kW1Stride = 136;  // halves per W1 row: conflict-free B-fragment loads
-constexpr int kW2Stride = 72;   // halves per W2 / W3 / hidden row
-constexpr int kTcWarps = 8;
-constexpr int kHaloX = 24;      // 20 used
-constexpr int kHaloK = 25 * kHaloX;        // the constant feature k / 64
-constexpr int kHaloZero = kHaloK + 16;     // zero padding features
-constexpr int kHaloSize = kHaloZero + 32;
+// Tensor-core inference on the 5th-generation tensor cores (tcgen05). A CTA
+// of four warps evaluates 128 cells at a time -- four 32-cell row segments,
+// one per warp -- as the M = 128 rows of the three layers:
+//   D1 = A1 W1^T  (A1: [128 x 128] occupancy features, 126 used),
+//   D2 = SiLU(D1 + b1) W2^T,  D3 = SiLU(D2 + b2) W3^T  (N = 64, 64, 16 with 8 used).
+// One thread issues tcgen05.mma (kind::f16: FP16 operands that the tensor
+// cores read from shared memory through matrix descriptors, FP32
+// accumulators in tensor memory) and tcgen05.commit, which arrives on an
+// mbarrier once the products are done; every warp then reads its 32
+// accumulator lanes with tcgen05.ld, adds the bias, applies SiLU and writes
+// the next layer's A operand. Layer 1 is a 5x5x5 convolution of the
+// occupancy grid: each warp stages the 36 x 5 x 5 halo of log(1 + count) of
+// its segment and each lane writes its cell's 128 features from it.
+//
+// Operand layout (K-major, no swizzle): 8-row x 16-byte core matrices; the 8
+// rows of a core matrix are 16 B apart, 8-row groups SBO = 128 B apart, and
+// the 16-byte K chunks LBO apart (LBO = rows x 16 B).
+constexpr int kUmmaThreads = 256;   // two warps per lane quarter of tensor memory
+constexpr int kHaloW = 40;          // halves per halo row (36 used: x0 - 2 .. x0 + 33)
+constexpr uint32_t kTmemCols = 64;  // D1, D2 and D3 share the same columns
+constexpr int kMbarSpin = 1 << 22;  // bounded wait for the tensor cores
 
-struct TcShared {
-  __half w1[kMlpHidden * kW1Stride];
-  __half w2[kMlpHidden * kW2Stride];
-  __half w3[kMlpOut * kW2Stride];
-  float b1[kMlpHidden], b2[kMlpHidden], b3[kMlpOut];
-  float lg1p[64];   // log(1 + c) for occupancies c < 64
-  int toff[128];    // halo offset of feature f for cell 0 of the tile
-  __half h[kTcWarps][16 * kW2Stride];
-  __half halo[kTcWarps][kHaloSize];
+struct UmmaShared {
+  __half a[128 * 128];  // A1, then A2 and A3 (aliased): chunk c at c * 2048 B, row m at m * 16 B
+  __half w1[64 * 128];  // chunk c at c * 1024 B, row n at n * 16 B
+  __half w2[64 * 64];   // chunk c at c * 1024 B
+  __half w3[16 * 64];   // rows 8..15 zero; chunk c at c * 256 B
+  __half halo[4][25 * kHaloW];
+  float b1[64], b2[64], b3[16];
+  float lg1p[64];       // log(1 + c) for occupancies c < 64
+  unsigned long long mbar;
+  uint32_t tmem_base;
 };
 
-__device__ __forceinline__ void mma_f16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
-                                        uint32_t a3, uint32_t b0, uint32_t b1) {
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor (sm_100 format, version 1, no swizzle).
+__device__ __forceinline__ uint64_t umma_desc(const void *p, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = uint64_t((smem_u32(p) >> 4) & 0x3FFFu);
+  d |= uint64_t((lbo >> 4) & 0x3FFFu) << 16;
+  d |= uint64_t((sbo >> 4) & 0x3FFFu) << 32;
+  d |= uint64_t(1) << 46;
+  return d;
+}
+
+// Instruction descriptor of kind::f16: FP16 A and B, both K-major, FP32 D.
+__host__ __device__ constexpr uint32_t umma_idesc(int M, int N) {
+  return (1u << 4) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t idesc, uint32_t accumulate) {
   asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-      "{%8,%9}, {%0,%1,%2,%3};"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u),
+        "r"(0u), "r"(0u));
 }
 
-__device__ __forceinline__ uint32_t pack_h2(__half lo, __half hi) {
-  return uint32_t(__half_as_ushort(lo)) | (uint32_t(__half_as_ushort(hi)) << 16);
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               :
+               : "r"(mbar)
+               : "memory");
 }
 
-__device__ __forceinline__ uint32_t ld_h2(const __half *p) {
-  return *reinterpret_cast<const uint32_t *>(p);
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (int i = 0; i < kMbarSpin; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tmem_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void async_proxy_fence() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// 16 consecutive FP32 accumulator columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
 // SiLU with the fast division (inference only).
 __device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 
-// Periodic coordinate c + d for |d| <= 2.
+__device__ __forceinline__ uint32_t pack_h2(float lo, float hi) {
+  const __half2 h = __floats2half2_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+// Periodic coordinate c for |c - [0, n)| <= 2.
 __device__ __forceinline__ int wrap_near(int c, int n) {
   if (n < 3) return rem_euclid(c, n);
   return c < 0 ? c + n : (c >= n ? c - n : c);
 }
 
-__global__ void __launch_bounds__(kTcWarps * 32, 1) k_cell_proposal_tc(
+// Hidden layer epilogue: 32 of row m's 64 accumulators (columns
+// [32 h, 32 h + 32)) + bias, SiLU, as FP16 into the next A operand.
+__device__ __forceinline__ void hidden_to_a(uint32_t taddr, const float *bias, __half *a, int m,
+                                            int half) {
+#pragma unroll
+  for (int q = 2 * half; q < 2 * half + 2; ++q) {
+    float v[16];
+    tmem_ld16(taddr + 16 * q, v);
+    tmem_wait_ld();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      uint4 w;
+      w.x = pack_h2(silu_fast(v[8 * h + 0] + bias[16 * q + 8 * h + 0]),
+                    silu_fast(v[8 * h + 1] + bias[16 * q + 8 * h + 1]));
+      w.y = pack_h2(silu_fast(v[8 * h + 2] + bias[16 * q + 8 * h + 2]),
+                    silu_fast(v[8 * h + 3] + bias[16 * q + 8 * h + 3]));
+      w.z = pack_h2(silu_fast(v[8 * h + 4] + bias[16 * q + 8 * h + 4]),
+                    silu_fast(v[8 * h + 5] + bias[16 * q + 8 * h + 5]));
+      w.w = pack_h2(silu_fast(v[8 * h + 6] + bias[16 * q + 8 * h + 6]),
+                    silu_fast(v[8 * h + 7] + bias[16 * q + 8 * h + 7]));
+      *reinterpret_cast<uint4 *>(a + (2 * q + h) * 1024 + m * 8) = w;
+    }
+  }
+}
+
+// Segment geometry of row segment seg: cells inside the frame (0 past the
+// last segment), first cell, and the frame.
+struct SegInfo {
+  const FrameDesc *fr;
+  int ncl, x0, cy, cz;
+  long long c0;
+};
+
+__device__ __forceinline__ SegInfo segment_info(const FrameDesc *__restrict__ frames, int nframes,
+                                                long long seg, long long segs) {
+  SegInfo g;
+  g.fr = frames;
+  g.ncl = 0;
+  g.x0 = g.cy = g.cz = 0;
+  g.c0 = 0;
+  if (seg >= segs) return g;
+  int f = 0;
+  if (nframes > 1) {
+    int lo = 0, hi = nframes - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (frames[mid].seg_base <= seg)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    f = lo;
+  }
+  g.fr = &frames[f];
+  const FrameDesc &fr = *g.fr;
+  const int per_row = (fr.nx + 31) / 32;
+  const long long ls = seg - fr.seg_base;
+  const int row = int(ls / per_row);
+  g.x0 = int(ls - (long long)row * per_row) * 32;
+  g.cy = row % fr.ny;
+  g.cz = row / fr.ny;
+  g.ncl = min(32, fr.nx - g.x0);
+  g.c0 = fr.cell_base + (long long)row * fr.nx + g.x0;
+  return g;
+}
+
+// Rows [y0, y1) of a segment's halo of log(1 + count): 36 columns
+// x0 - 2 .. x0 + 33 of the 5 x 5 (dy, dz) rows around it.
+__device__ __forceinline__ void stage_halo(const SegInfo &g, const uint32_t *__restrict__ count,
+                                           const float *lg1p, __half *halo, int y0, int y1,
+                                           int lane) {
+  if (g.ncl == 0) {
+    for (int yz = y0; yz < y1; ++yz)
+      for (int x = lane; x < 36; x += 32) halo[yz * kHaloW + x] = __float2half_rn(0.f);
+    return;
+  }
+  const FrameDesc &fr = *g.fr;
+  const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
+  const int xa = (nx >= 36) ? wrap_near(g.x0 + lane - 2, nx) : rem_euclid(g.x0 + lane - 2, nx);
+  const int xb = (nx >= 36) ? wrap_near(g.x0 + lane + 30, nx) : rem_euclid(g.x0 + lane + 30, nx);
+  for (int yz = y0; yz < y1; ++yz) {
+    const int jy = wrap_near(g.cy + yz / 5 - 2, ny);
+    const int jz = wrap_near(g.cz + yz % 5 - 2, nz);
+    const uint32_t *crow = count + fr.cell_base + ((long long)jz * ny + jy) * (long long)nx;
+    const uint32_t ca = crow[xa];
+    halo[yz * kHaloW + lane] = __float2half_rn(ca < 64u ? lg1p[ca] : log1pf(float(ca)));
+    if (lane < 4) {
+      const uint32_t cb = crow[xb];
+      halo[yz * kHaloW + 32 + lane] = __float2half_rn(cb < 64u ? lg1p[cb] : log1pf(float(cb)));
+    }
+  }
+}
+
+// Feature chunks [c0, c1) (8 features each) of row m = the lane's cell:
+// f = (dx + 2) * 25 + (dy + 2) * 5 + (dz + 2) is halo row f % 25, column
+// lane + f / 25; then k / 64 and two zeros.
+template <int C0, int C1>
+__device__ __forceinline__ void build_a1(const __half *halo, __half *a, int m, int lane,
+                                         unsigned short kfeat) {
+  const unsigned short *hs = reinterpret_cast<const unsigned short *>(halo) + lane;
+#pragma unroll
+  for (int c = C0; c < C1; ++c) {
+    uint32_t v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int f = 8 * c + i;
+      v[i] = f < 125 ? uint32_t(hs[(f % 25) * kHaloW + f / 25]) : (f == 125 ? kfeat : 0u);
+    }
+    uint4 w;
+    w.x = v[0] | (v[1] << 16);
+    w.y = v[2] | (v[3] << 16);
+    w.z = v[4] | (v[5] << 16);
+    w.w = v[6] | (v[7] << 16);
+    *reinterpret_cast<uint4 *>(a + c * 1024 + m * 8) = w;
+  }
+}
+
+// Layer L (0, 1, 2) of one tile: products of A (128 x K) and the layer's
+// weights into tensor-memory columns [tcol, tcol + N), then a commit to mbar.
+// Called by one thread.
+__device__ __forceinline__ void issue_layer(int layer, const UmmaShared &sh, const __half *a,
+                                            uint32_t tcol, uint32_t mbar) {
+  tmem_fence_after();
+  if (layer == 0) {
+#pragma unroll
+    for (int s2 = 0; s2 < 8; ++s2)
+      umma_f16(tcol, umma_desc(a + s2 * 2 * 1024, 2048, 128),
+               umma_desc(sh.w1 + s2 * 2 * 512, 1024, 128), umma_idesc(128, 64), s2 > 0);
+  } else if (layer == 1) {
+#pragma unroll
+    for (int s2 = 0; s2 < 4; ++s2)
+      umma_f16(tcol, umma_desc(a + s2 * 2 * 1024, 2048, 128),
+               umma_desc(sh.w2 + s2 * 2 * 512, 1024, 128), umma_idesc(128, 64), s2 > 0);
+  } else {
+#pragma unroll
+    for (int s2 = 0; s2 < 4; ++s2)
+      umma_f16(tcol, umma_desc(a + s2 * 2 * 1024, 2048, 128),
+               umma_desc(sh.w3 + s2 * 2 * 128, 256, 128), umma_idesc(128, 16), s2 > 0);
+  }
+  umma_commit(mbar);
+}
+
+// Softmax of row m's 8 logits and the proposal (smallest R with P >= tau).
+__device__ __forceinline__ void write_proposal(uint32_t taddr, const float *b3, float tau,
+                                               int8_t *cell_prop, long long cell, bool valid) {
+  float z[16];
+  tmem_ld16(taddr, z);
+  tmem_wait_ld();
+  if (!valid) return;
+  float lg[8], mx = -3.0e38f;
+#pragma unroll
+  for (int o = 0; o < 8; ++o) {
+    lg[o] = z[o] + b3[o];
+    mx = fmaxf(mx, lg[o]);
+  }
+  float e[8], sum = 0.f;
+#pragma unroll
+  for (int o = 0; o < 8; ++o) {
+    e[o] = __expf(lg[o] - mx);
+    sum += e[o];
+  }
+  int prop = kMlpOut;
+  float cum = 0.f;
+#pragma unroll
+  for (int o = 0; o < 8; ++o) {
+    cum += e[o] / sum;
+    if (cum >= tau && prop == kMlpOut) prop = o + 1;
+  }
+  cell_prop[cell] = int8_t(prop >= kMlpOut ? 0 : prop);
+}
+
+// Eight warps per CTA: warps w and w + 4 share lane quarter w of tensor
+// memory (rows 32 w .. 32 w + 31, one 32-cell row segment): each stages half
+// of the segment's halo and features, and takes half of the accumulator
+// columns in the epilogues.
+__global__ void __launch_bounds__(kUmmaThreads, 1) k_cell_proposal_tc(
     const float *__restrict__ params, const FrameDesc *__restrict__ frames, int nframes,
-    const uint32_t *__restrict__ off, const uint32_t *__restrict__ count, float tau,
-    int8_t *__restrict__ cell_prop) {
-  extern __shared__ float smem_raw[];
-  TcShared &sh = *reinterpret_cast<TcShared *>(smem_raw);
+    const uint32_t *__restrict__ count, float tau, int8_t *__restrict__ cell_prop,
+    int *__restrict__ status) {
+  extern __shared__ __align__(1024) unsigned char umma_smem[];
+  UmmaShared &sh = *reinterpret_cast<UmmaShared *>(umma_smem);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int quarter = warp & 3, half = warp >> 2;
   const float *W1 = params, *B1 = W1 + kMlpHidden * kMlpIn;
   const float *W2 = B1 + kMlpHidden, *B2 = W2 + kMlpHidden * kMlpHidden;
   const float *W3 = B2 + kMlpHidden, *B3 = W3 + kMlpOut * kMlpHidden;
-  for (int t = threadIdx.x; t < kMlpHidden * kW1Stride; t += blockDim.x) {
-    const int n = t / kW1Stride, kk = t % kW1Stride;
-    sh.w1[t] = __float2half_rn(kk < kMlpIn ? W1[n * kMlpIn + kk] : 0.f);
+  // weights as FP16 K-major operands
+  for (int t = threadIdx.x; t < 64 * 128; t += kUmmaThreads) {
+    const int n = t >> 7, k = t & 127;
+    sh.w1[(k >> 3) * 512 + n * 8 + (k & 7)] = __float2half_rn(k < kMlpIn ? W1[n * kMlpIn + k] : 0.f);
   }
-  for (int t = threadIdx.x; t < kMlpHidden * kW2Stride; t += blockDim.x) {
-    const int n = t / kW2Stride, kk = t % kW2Stride;
-    sh.w2[t] = __float2half_rn(kk < kMlpHidden ? W2[n * kMlpHidden + kk] : 0.f);
+  for (int t = threadIdx.x; t < 64 * 64; t += kUmmaThreads) {
+    const int n = t >> 6, k = t & 63;
+    sh.w2[(k >> 3) * 512 + n * 8 + (k & 7)] = __float2half_rn(W2[n * kMlpHidden + k]);
   }
-  for (int t = threadIdx.x; t < kMlpOut * kW2Stride; t += blockDim.x) {
-    const int n = t / kW2Stride, kk = t % kW2Stride;
-    sh.w3[t] = __float2half_rn(kk < kMlpHidden ? W3[n * kMlpHidden + kk] : 0.f);
+  for (int t = threadIdx.x; t < 16 * 64; t += kUmmaThreads) {
+    const int n = t >> 6, k = t & 63;
+    sh.w3[(k >> 3) * 128 + n * 8 + (k & 7)] =
+        __float2half_rn(n < kMlpOut ? W3[n * kMlpHidden + k] : 0.f);
   }
-  for (int t = threadIdx.x; t < kMlpHidden; t += blockDim.x) {
-    sh.b1[t] = B1[t];
-    sh.b2[t] = B2[t];
+  if (threadIdx.x < 64) {
+    sh.b1[threadIdx.x] = B1[threadIdx.x];
+    sh.b2[threadIdx.x] = B2[threadIdx.x];
+    sh.lg1p[threadIdx.x] = log1pf(float(threadIdx.x));
   }
-  if (threadIdx.x < kMlpOut) sh.b3[threadIdx.x] = B3[threadIdx.x];
-  if (threadIdx.x < 64) sh.lg1p[threadIdx.x] = log1pf(float(threadIdx.x));
-  if (threadIdx.x < 128) {
-    // feature f = (dx + 2) * 25 + (dy + 2) * 5 + (dz + 2); halo row (dy + 2) * 5 + (dz + 2)
-    const int f = threadIdx.x;
-    sh.toff[f] = f < 125 ? (f % 25) * kHaloX + f / 25 : (f == 125 ? kHaloK : kHaloZero);
+  if (threadIdx.x < 16) sh.b3[threadIdx.x] = threadIdx.x < kMlpOut ? B3[threadIdx.x] : 0.f;
+  const uint32_t mbar = smem_u32(&sh.mbar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&sh.tmem_base)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  async_proxy_fence();
+  tmem_fence_before();
+  __syncthreads();
+  tmem_fence_after();
+  const uint32_t tmem = sh.tmem_base;
+  const uint32_t tlane = tmem + (uint32_t(quarter * 32) << 16);  // this warp's lane quarter
+  const int m = quarter * 32 + lane;                              // A row = accumulator lane
+  __half *halo = sh.halo[quarter];
+  uint32_t phase = 0;
+  bool ok = true;
+  auto sync_issue = [&](int layer) {
+    async_proxy_fence();
+    tmem_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0) issue_layer(layer, sh, sh.a, tmem, mbar);
+  };
+  auto wait_products = [&]() -> bool {
+    const bool w = mbar_wait(mbar, phase);
+    phase ^= 1u;
+    const bool all = __syncthreads_and(w);
+    tmem_fence_after();
+    return all;
+  };
+
+  const FrameDesc &last = frames[nframes - 1];
+  const long long segs = last.seg_base + (long long)((last.nx + 31) / 32) * last.ny * last.nz;
+  const long long ctas = (segs + 3) / 4;
+  for (long long ct = blockIdx.x; ct < ctas; ct += gridDim.x) {
+    const SegInfo g = segment_info(frames, nframes, ct * 4 + quarter, segs);
+    stage_halo(g, count, sh.lg1p, halo, half ? 13 : 0, half ? 25 : 13, lane);
+    __syncthreads();  // both halves of every halo are in place
+    const unsigned short kfeat = __half_as_ushort(__float2half_rn(float(g.fr->k) / 64.0f));
+    if (half)
+      build_a1<8, 16>(halo, sh.a, m, lane, kfeat);
+    else
+      build_a1<0, 8>(halo, sh.a, m, lane, kfeat);
+    sync_issue(0);
+    if (!(ok = wait_products())) break;
+    hidden_to_a(tlane, sh.b1, sh.a, m, half);
+    sync_issue(1);
+    if (!(ok = wait_products())) break;
+    hidden_to_a(tlane, sh.b2, sh.a, m, half);
+    sync_issue(2);
+    if (!(ok = wait_products())) break;
+    if (half == 0) write_proposal(tlane, sh.b3, tau, cell_prop, g.c0 + lane, lane < g.ncl);
+    // the next tile rewrites the halos, A and the accumulators
+    tmem_fence_before();
+    __syncthreads();
+    tmem_fence_after();
+  }
+  if (!ok && threadIdx.x == 0) {
+    atomicOr(status, kStatusMmaTimeout);
+    mbar_wait(mbar, phase ^ 1u);  // give the products in flight a last bounded wait
   }
   __syncthreads();
-
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, tig = lane & 3;
-  __half *hbuf = sh.h[warp];
-  __half *halo = sh.halo[warp];
-  const FrameDesc &last = frames[nframes - 1];
-  const long long tiles = last.row_tile_base + (long long)((last.nx + 15) / 16) * last.ny * last.nz;
-  for (long long tile = (long long)blockIdx.x * kTcWarps + warp; tile < tiles;
-       tile += (long long)gridDim.x * kTcWarps) {
-    int f = 0;
-    if (nframes > 1) {
-      int lo = 0, hi = nframes - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (frames[mid].row_tile_base <= tile)
-          lo = mid;
-        else
-          hi = mid - 1;
-      }
-      f = lo;
-    }
-    const FrameDesc &fr = frames[f];
-    const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
-    const int per_row = (nx + 15) / 16;
-    const long long lt = tile - fr.row_tile_base;
-    const int row = int(lt / per_row);
-    const int x0 = int(lt - (long long)row * per_row) * 16;
-    const int cy = row % ny, cz = row / ny;
-    const int ncl = min(16, nx - x0);
-    const long long c0 = fr.cell_base + (long long)row * nx + x0;
-    if (off[c0] == off[c0 + ncl]) continue;  // no occupied cell in the tile
-    // halo: x0 - 2 .. x0 + 17, cy - 2 .. cy + 2, cz - 2 .. cz + 2 (periodic)
-    __syncwarp();
-    for (int hidx = lane; hidx < 25 * 20; hidx += 32) {
-      const int yz = hidx / 20, xx = hidx - yz * 20;
-      const int jy = wrap_near(cy + yz / 5 - 2, ny);
-      const int jz = wrap_near(cz + yz % 5 - 2, nz);
-      const int jx = (nx >= 20) ? wrap_near(x0 + xx - 2, nx) : rem_euclid(x0 + xx - 2, nx);
-      const uint32_t cnt = count[fr.cell_base + ((long long)jz * ny + jy) * (long long)nx + jx];
-      halo[yz * kHaloX + xx] = __float2half_rn(cnt < 64u ? sh.lg1p[cnt] : log1pf(float(cnt)));
-    }
-    if (lane < 16) {
-      halo[kHaloK + lane] = __float2half_rn(float(fr.k) / 64.0f);
-      halo[kHaloZero + lane] = __float2half_rn(0.f);
-      halo[kHaloZero + 16 + lane] = __float2half_rn(0.f);
-    }
-    __syncwarp();
-    // layer 1
-    float acc[8][4];
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      const float b0 = sh.b1[nt * 8 + 2 * tig], b1v = sh.b1[nt * 8 + 2 * tig + 1];
-      acc[nt][0] = b0;
-      acc[nt][1] = b1v;
-      acc[nt][2] = b0;
-      acc[nt][3] = b1v;
-    }
-#pragma unroll 2
-    for (int k0 = 0; k0 < 128; k0 += 16) {
-      const int o0 = sh.toff[k0 + 2 * tig], o1 = sh.toff[k0 + 2 * tig + 1];
-      const int o2 = sh.toff[k0 + 2 * tig + 8], o3 = sh.toff[k0 + 2 * tig + 9];
-      const uint32_t a0 = pack_h2(halo[o0 + g], halo[o1 + g]);
-      const uint32_t a1 = pack_h2(halo[o0 + g + 8], halo[o1 + g + 8]);
-      const uint32_t a2 = pack_h2(halo[o2 + g], halo[o3 + g]);
-      const uint32_t a3 = pack_h2(halo[o2 + g + 8], halo[o3 + g + 8]);
-#pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
-        const __half *wr = sh.w1 + (nt * 8 + g) * kW1Stride + k0 + 2 * tig;
-        mma_f16(acc[nt], a0, a1, a2, a3, ld_h2(wr), ld_h2(wr + 8));
-      }
-    }
-    // SiLU, then to shared memory (row-major 16 x 64 halves)
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      const int col = nt * 8 + 2 * tig;
-      *reinterpret_cast<__half2 *>(hbuf + g * kW2Stride + col) =
-          __floats2half2_rn(silu_fast(acc[nt][0]), silu_fast(acc[nt][1]));
-      *reinterpret_cast<__half2 *>(hbuf + (g + 8) * kW2Stride + col) =
-          __floats2half2_rn(silu_fast(acc[nt][2]), silu_fast(acc[nt][3]));
-    }
-    __syncwarp();
-    // layer 2
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      const float b0 = sh.b2[nt * 8 + 2 * tig], b1v = sh.b2[nt * 8 + 2 * tig + 1];
-      acc[nt][0] = b0;
-      acc[nt][1] = b1v;
-      acc[nt][2] = b0;
-      acc[nt][3] = b1v;
-    }
-#pragma unroll
-    for (int k0 = 0; k0 < 64; k0 += 16) {
-      const uint32_t a0 = ld_h2(hbuf + g * kW2Stride + k0 + 2 * tig);
-      const uint32_t a1 = ld_h2(hbuf + (g + 8) * kW2Stride + k0 + 2 * tig);
-      const uint32_t a2 = ld_h2(hbuf + g * kW2Stride + k0 + 2 * tig + 8);
-      const uint32_t a3 = ld_h2(hbuf + (g + 8) * kW2Stride + k0 + 2 * tig + 8);
-#pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
-        const __half *wr = sh.w2 + (nt * 8 + g) * kW2Stride + k0 + 2 * tig;
-        mma_f16(acc[nt], a0, a1, a2, a3, ld_h2(wr), ld_h2(wr + 8));
-      }
-    }
-    __syncwarp();
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      const int col = nt * 8 + 2 * tig;
-      *reinterpret_cast<__half2 *>(hbuf + g * kW2Stride + col) =
-          __floats2half2_rn(silu_fast(acc[nt][0]), silu_fast(acc[nt][1]));
-      *reinterpret_cast<__half2 *>(hbuf + (g + 8) * kW2Stride + col) =
-          __floats2half2_rn(silu_fast(acc[nt][2]), silu_fast(acc[nt][3]));
-    }
-    __syncwarp();
-    // layer 3: 8 logits per cell
-    float z[4] = {sh.b3[2 * tig], sh.b3[2 * tig + 1], sh.b3[2 * tig], sh.b3[2 * tig + 1]};
-#pragma unroll
-    for (int k0 = 0; k0 < 64; k0 += 16) {
-      const uint32_t a0 = ld_h2(hbuf + g * kW2Stride + k0 + 2 * tig);
-      const uint32_t a1 = ld_h2(hbuf + (g + 8) * kW2Stride + k0 + 2 * tig);
-      const uint32_t a2 = ld_h2(hbuf + g * kW2Stride + k0 + 2 * tig + 8);
-      const uint32_t a3 = ld_h2(hbuf + (g + 8) * kW2Stride + k0 + 2 * tig + 8);
-      const __half *wr = sh.w3 + g * kW2Stride + k0 + 2 * tig;
-      mma_f16(z, a0, a1, a2, a3, ld_h2(wr), ld_h2(wr + 8));
-    }
-    // each quad holds the 8 logits of rows g (z[0], z[1]) and g + 8 (z[2], z[3])
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      float lg[8];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        lg[2 * q] = __shfl_sync(0xffffffffu, z[2 * h], (lane & ~3) | q);
-        lg[2 * q + 1] = __shfl_sync(0xffffffffu, z[2 * h + 1], (lane & ~3) | q);
-      }
-      const int m = g + 8 * h;
-      if (tig == 0 && m < ncl) {
-        float mx = lg[0];
-#pragma unroll
-        for (int o = 1; o < 8; ++o) mx = fmaxf(mx, lg[o]);
-        float e[8], sum = 0.f;
-#pragma unroll
-        for (int o = 0; o < 8; ++o) {
-          e[o] = __expf(lg[o] - mx);
-          sum += e[o];
-        }
-        int prop = kMlpOut;
-        float cum = 0.f;
-#pragma unroll
-        for (int o = 0; o < 8; ++o) {
-          cum += e[o] / sum;
-          if (cum >= tau && prop == kMlpOut) prop = o + 1;
-        }
-        cell_prop[c0 + m] = int8_t(prop >= kMlpOut ? 0 : prop);
-      }
-    }
-    __syncwarp();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
+                 : "memory");
   }
 }
 
@@ -584,17 +745,19 @@ cudaError_t mlp_training_rows(const BatchBuffers &b, const int8_t *stop_log, lon
 cudaError_t mlp_propose(const float *params, const BatchBuffers &b, int8_t *cell_prop,
                         int8_t *source_prop, float tau, cudaStream_t s) {
   if (b.nframes <= 0 || b.ncells <= 0) return cudaSuccess;
-  const size_t sm = sizeof(TcShared);
+  const size_t sm = sizeof(UmmaShared) + 1024;  // room to align the base to 1024 B
   cudaError_t e =
       cudaFuncSetAttribute(k_cell_proposal_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
   if (e != cudaSuccess) return e;
-  int dev = 0, sms = 148, per_sm = 1;
+  int dev = 0, sms = 148, smem_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cell_proposal_tc, kTcWarps * 32, sm);
-  if (per_sm < 1) per_sm = 1;
-  k_cell_proposal_tc<<<sms * per_sm, kTcWarps * 32, sm, s>>>(params, b.frames, b.nframes, b.off,
-                                                              b.count, tau, cell_prop);
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  // resident CTAs: shared memory (1 KB of it reserved per CTA) and the
+  // kTmemCols each CTA holds of the SM's 512 tensor-memory columns
+  const int per_sm = std::max(1, std::min(smem_sm / int(sm + 1024), int(512 / kTmemCols)));
+  k_cell_proposal_tc<<<sms * per_sm, kUmmaThreads, sm, s>>>(params, b.frames, b.nframes, b.count,
+                                                            tau, cell_prop, b.status);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_source_proposal<<<grid_of(b.npts, 256), 256, 0, s>>>(b.frames, b.nframes, b.off, b.ncells,
                                                          b.scell, cell_prop, source_prop);

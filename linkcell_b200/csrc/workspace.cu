@@ -351,13 +351,13 @@ void WorkspaceImpl::release_all() {
 Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const int *mask,
                         int *out_nn, double *out_d2, bool wait, std::string &detail) {
   const int nf = int(frames.size());
-  long long npts = 0, ncells = 0, rtiles = 0;
+  long long npts = 0, ncells = 0, segs = 0;
   int kmax = 1;
   for (auto &fd : frames) {
     fd.pt_base = npts;
     fd.cell_base = ncells;
-    fd.row_tile_base = rtiles;
-    rtiles += (long long)((fd.nx + 15) / 16) * fd.ny * fd.nz;
+    fd.seg_base = segs;
+    segs += (long long)((fd.nx + 31) / 32) * fd.ny * fd.nz;
     npts += fd.n;
     ncells += (long long)fd.nx * fd.ny * fd.nz;
     kmax = std::max(kmax, fd.k);
