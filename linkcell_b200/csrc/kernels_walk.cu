@@ -988,7 +988,8 @@ __global__ void __launch_bounds__(256, 2) k_team_walk(BatchBuffers b) {
 //     order against the others, and ranks 0..k-1 are the row; a tie across
 //     the k-th slot goes to the literal replay.
 // Any proposal gives the reference result: a short proposal, a buffer
-// overflow, a cube that wraps the box, k > 32 or an S larger than 64 sends
+// overflow, a cube that wraps the box, k > 64 or an S larger than its buffer
+// (64 entries for k <= 32, 128 for k <= 64) sends
 // the source to the literal replay.
 constexpr int kSelCap = 512;   // FP32-filtered candidates per warp
 constexpr int kSelWarps = 8;   // warps per block
@@ -1003,14 +1004,16 @@ struct __align__(16) SelRow {  // one non-empty row of the cube
   int syz;                     // max(1, |dy|, |dz|)
 };
 
+// SN: elements of S per lane (S holds at most 32 SN; k <= 16 SN).
+template <int SN>
 struct SelShared {
   float d[kSelCap];
   int t[kSelCap];
   uint32_t m[kSelCap];  // shell | wa + 1 << 8 | wb + 1 << 10 | wc + 1 << 12
   SelRow rows[32];
-  double sd[64];
-  int sj[64];
-  int si[64];
+  double sd[32 * SN];
+  int sj[32 * SN];
+  int si[32 * SN];
   int hist[32];
   unsigned hmax[32];
   unsigned long long wc[8];  // warp-uniform counters (SelWarpCounter), lane 0 updates
@@ -1042,14 +1045,15 @@ __device__ __forceinline__ uint32_t quot(uint32_t x, uint32_t n, double inv) {
 }
 
 // One source; false: the source must go to the literal replay.
-__device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelShared &sh,
+template <int SN>
+__device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelShared<SN> &sh,
                               SelCounters &cnt) {
   const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
   const FrameDesc &fr = b.frames[f];
   const int Rp = b.proposal[p];
   const int k = fr.k;
   const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
-  if ((b.frame_flags[f] & kFrameNaN) || Rp <= 0 || Rp > 8 || Rp > fr.max_reach || k > 32 ||
+  if ((b.frame_flags[f] & kFrameNaN) || Rp <= 0 || Rp > 8 || Rp > fr.max_reach || k > 16 * SN ||
       2 * Rp + 1 > nx || 2 * Rp + 1 > ny || 2 * Rp + 1 > nz)
     return false;
   const uint32_t lc = b.scell[p];
@@ -1351,17 +1355,17 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
     const int i = i0 + lane;
     const bool in = i < total && int(sh.m[i] & 255u) <= Rs && sh.d[i] <= TS;
     const unsigned m = __ballot_sync(kFull, in);
-    if (nS + __popc(m) > 64) return false;  // S larger than the row buffer
+    if (nS + __popc(m) > 32 * SN) return false;  // S larger than the row buffer
     if (in) sh.si[nS + __popc(m & lanemask_lt())] = i;
     nS += __popc(m);
   }
   __syncwarp();
   if (nS < k) return false;  // cannot happen: T bounds k candidates
   if (lane == 0) cnt.rerank += unsigned(nS);
-  double ed[2];
-  int ej[2];
+  double ed[SN];
+  int ej[SN];
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
+  for (int h = 0; h < SN; ++h) {
     const int q = lane + 32 * h;
     ed[h] = pinf();
     ej[h] = 0x7fffffff;
@@ -1375,19 +1379,25 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   }
   __syncwarp();
   // 4. rank of each element in (d2, index) order; the first k are the row
-  int rk[2] = {0, 0};
-  for (int e = 0; e < nS; ++e) {
-    const double de = sh.sd[e];
-    const int je = sh.sj[e];
+  int rk[SN];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) rk[h] += lex_less(de, je, ed[h], ej[h]) ? 1 : 0;
+  for (int h = 0; h < SN; ++h) rk[h] = 0;
+  if (nS <= 32) {  // the common case: one element per lane
+    for (int e = 0; e < nS; ++e) rk[0] += lex_less(sh.sd[e], sh.sj[e], ed[0], ej[0]) ? 1 : 0;
+  } else {
+    for (int e = 0; e < nS; ++e) {
+      const double de = sh.sd[e];
+      const int je = sh.sj[e];
+#pragma unroll
+      for (int h = 0; h < SN; ++h) rk[h] += lex_less(de, je, ed[h], ej[h]) ? 1 : 0;
+    }
   }
   const FrameDesc &frr = fr;
   const int i = b.sidx[p];
   int *row = b.out_nn + frr.out_base + (long long)i * k;
   double *drow = b.out_d2 ? b.out_d2 + frr.out_base + (long long)i * k : nullptr;
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
+  for (int h = 0; h < SN; ++h) {
     if (lane + 32 * h < nS) {
       if (rk[h] == k - 1) sh.hmax[0] = __double2loint(ed[h]), sh.hmax[1] = __double2hiint(ed[h]);
       if (rk[h] == k) sh.hmax[2] = __double2loint(ed[h]), sh.hmax[3] = __double2hiint(ed[h]);
@@ -1400,7 +1410,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
     return false;
   }
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
+  for (int h = 0; h < SN; ++h) {
     if (lane + 32 * h < nS && rk[h] < k) {
       row[rk[h]] = ej[h];
       if (drow) drow[rk[h]] = ed[h];
@@ -1411,9 +1421,10 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   return true;
 }
 
-__global__ void __launch_bounds__(kSelWarps * 32, 3) k_select_walk(BatchBuffers b) {
+template <int SN>
+__global__ void __launch_bounds__(kSelWarps * 32, SN == 2 ? 3 : 2) k_select_walk(BatchBuffers b) {
   extern __shared__ __align__(16) unsigned char sel_smem[];
-  SelShared &sh = reinterpret_cast<SelShared *>(sel_smem)[threadIdx.x >> 5];
+  SelShared<SN> &sh = reinterpret_cast<SelShared<SN> *>(sel_smem)[threadIdx.x >> 5];
   const long long total = b.off[b.ncells];
   const int lane = threadIdx.x & 31;
   SelCounters cnt;
@@ -1429,7 +1440,7 @@ __global__ void __launch_bounds__(kSelWarps * 32, 3) k_select_walk(BatchBuffers 
       const long long p = (long long)base + q;
       if (p >= total) break;
       const unsigned long long tie = sh.wc[kWcReplays];
-      if (!select_source(b, p, lane, sh, cnt)) {
+      if (!select_source<SN>(b, p, lane, sh, cnt)) {
         if (lane == 0 && sh.wc[kWcReplays] == tie) ++sh.wc[kWcFallback];
         if (lane == 0) push_replay(b, p);
       }
@@ -1454,7 +1465,21 @@ __global__ void __launch_bounds__(kSelWarps * 32, 3) k_select_walk(BatchBuffers 
   }
 }
 
-size_t select_smem_bytes() { return sizeof(SelShared) * kSelWarps; }
+int sm_count();
+
+template <int SN>
+cudaError_t launch_select(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
+  const size_t smem = sizeof(SelShared<SN>) * kSelWarps;
+  cudaError_t e = cudaFuncSetAttribute(k_select_walk<SN>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk<SN>, kSelWarps * 32, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int grid = w.grid > 0 ? w.grid : sm_count() * per_sm;
+  k_select_walk<SN><<<grid, kSelWarps * 32, smem, s>>>(b);
+  return cudaGetLastError();
+}
 
 // Warp-parallel literal replay of the reference heap for one source (finite
 // coordinates). The warp evaluates the reference visit sequence 32
@@ -1846,18 +1871,8 @@ cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t
     k_queue_all<<<sm_count() * 4, 256, 0, s>>>(b);
     return cudaGetLastError();
   }
-  if (w.tpp == 32 && w.mode == kModeLearned && b.kmax <= 32 && b.proposal) {
-    const size_t smem = select_smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_select_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(smem));
-    if (e != cudaSuccess) return e;
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk, kSelWarps * 32, smem);
-    if (per_sm < 1) per_sm = 1;
-    const int grid = w.grid > 0 ? w.grid : sm_count() * per_sm;
-    k_select_walk<<<grid, kSelWarps * 32, smem, s>>>(b);
-    return cudaGetLastError();
-  }
+  if (w.tpp == 32 && w.mode == kModeLearned && b.kmax <= 64 && b.proposal)
+    return b.kmax <= 32 ? launch_select<2>(b, w, s) : launch_select<4>(b, w, s);
   if (w.tpp == 32 && b.kmax <= 256) {
     switch (w.mode) {
       case kModeFastF32: return launch_team_k<kModeFastF32>(b, w, s);

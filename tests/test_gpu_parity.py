@@ -219,6 +219,23 @@ def test_learned_walk_any_proposal_is_exact(runner, oracle_mod, shell):
         runner.set_mode(0)
 
 
+@pytest.mark.parametrize("k", [1, 17, 48, 64])
+@pytest.mark.parametrize("shell", [2, 4])
+def test_learned_walk_k_up_to_64(runner, oracle_mod, k, shell):
+    """The cube select walk serves k up to 64 (S buffer of 128); smaller and
+    larger k, any proposal, same rows as the reference."""
+    from linkcell_b200 import workloads as W
+    w = W.bimodal_triclinic(n=40000, seed=57 + k, k=k)
+    want = _oracle(oracle_mod, w["xyz"], w["cell"], k, hint=3.0)
+    runner.set_mode(2)
+    runner.set_proposal(shell)
+    try:
+        assert_same(runner.run(w["xyz"], w["cell"], k, hint=3.0), want, f"k={k} proposal {shell}")
+    finally:
+        runner.set_proposal(0)
+        runner.set_mode(0)
+
+
 def test_fp32_counters_show_filtering(runner, oracle_mod):
     from linkcell_b200 import workloads as W
     w = W.bimodal_triclinic(n=100000, seed=41, k=16)
