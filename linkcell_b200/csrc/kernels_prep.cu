@@ -27,31 +27,60 @@ __device__ __forceinline__ int frame_of_point(const FrameDesc *__restrict__ fr, 
   return lo;
 }
 
-// fold + bin + histogram: one thread per point, grid-stride.
+// fold + bin + histogram: grid-stride over points, two per thread per trip
+// (their coordinate loads and histogram atomics in flight together).
 __global__ void __launch_bounds__(256)
     k_fold_bin(const double *__restrict__ xyz, const int *__restrict__ mask,
                const FrameDesc *__restrict__ frames, int nframes, long long npts,
                uint32_t *__restrict__ cell_of, uint32_t *__restrict__ arank,
                uint32_t *__restrict__ count, int *__restrict__ frame_flags) {
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += stride) {
-    const int f = nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
-    const FrameDesc &fr = frames[f];
-    const long long i = g - fr.pt_base;
-    if (fr.has_mask && mask[fr.mask_base + i] == 0) {
-      cell_of[g] = kInactive;
-      continue;
+  for (long long g0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; g0 < npts;
+       g0 += 2 * stride) {
+    const long long gg[2] = {g0, g0 + stride};
+    double r[2][3];
+    bool act[2];
+    int fi[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const long long g = gg[u];
+      act[u] = g < npts;
+      fi[u] = 0;
+      if (!act[u]) continue;
+      fi[u] = nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
+      const FrameDesc &fr = frames[fi[u]];
+      if (fr.has_mask && mask[fr.mask_base + (g - fr.pt_base)] == 0) {
+        cell_of[g] = kInactive;
+        act[u] = false;
+        continue;
+      }
+      r[u][0] = xyz[3 * g + 0];
+      r[u][1] = xyz[3 * g + 1];
+      r[u][2] = xyz[3 * g + 2];
     }
-    double s0, s1, s2;
-    fractional(fr, xyz[3 * g + 0], xyz[3 * g + 1], xyz[3 * g + 2], s0, s1, s2);
-    if (s0 != s0 || s1 != s1 || s2 != s2) atomicOr(&frame_flags[f], kFrameNaN);
-    const int cx = bin_of(s0, fr.nx);
-    const int cy = bin_of(s1, fr.ny);
-    const int cz = bin_of(s2, fr.nz);
-    const uint32_t c =
-        uint32_t(fr.cell_base + ((long long)cz * fr.ny + cy) * (long long)fr.nx + cx);
-    cell_of[g] = c;
-    arank[g] = atomicAdd(&count[c], 1u);
+    uint32_t c[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      c[u] = 0;
+      if (!act[u]) continue;
+      const FrameDesc &fr = frames[fi[u]];
+      double s0, s1, s2;
+      fractional(fr, r[u][0], r[u][1], r[u][2], s0, s1, s2);
+      if (s0 != s0 || s1 != s1 || s2 != s2) atomicOr(&frame_flags[fi[u]], kFrameNaN);
+      const int cx = bin_of(s0, fr.nx);
+      const int cy = bin_of(s1, fr.ny);
+      const int cz = bin_of(s2, fr.nz);
+      c[u] = uint32_t(fr.cell_base + ((long long)cz * fr.ny + cy) * (long long)fr.nx + cx);
+    }
+    uint32_t rk[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) rk[u] = act[u] ? atomicAdd(&count[c[u]], 1u) : 0u;
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (!act[u]) continue;
+      cell_of[gg[u]] = c[u];
+      arank[gg[u]] = rk[u];
+    }
   }
 }
 
@@ -220,8 +249,10 @@ __global__ void __launch_bounds__(256)
 // smaller id), so the order inside a cell is by point id (the reference
 // bins points in id order). The reads of g's coordinates are gathers; the
 // writes of the sorted SoA records stay within the cell's few slots, so a
-// warp's stores remain coalesced.
-__global__ void __launch_bounds__(256)
+// warp's stores remain coalesced. Two slots per thread and the coordinate
+// gathers issued first keep more loads in flight (the kernel is bound by the
+// latency of its dependent gathers).
+__global__ void __launch_bounds__(256, 3)
     k_place_records(const double *__restrict__ xyz, const FrameDesc *__restrict__ frames,
                     int nframes, long long npts, long long ncells,
                     const uint32_t *__restrict__ cell_of, const uint32_t *__restrict__ off,
@@ -231,44 +262,63 @@ __global__ void __launch_bounds__(256)
                     int *__restrict__ status) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long total = off[ncells];
-  for (long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x; pos < total;
-       pos += stride) {
-    const uint32_t g = tmp[pos];
-    const uint32_t c = (long long)g < npts ? cell_of[g] : kInactive;
-    if (c >= ncells) {
-      atomicOr(status, kStatusBadIndex);
-      continue;
+  for (long long p0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; p0 < total;
+       p0 += 2 * stride) {
+    long long pos[2] = {p0, p0 + stride};
+    bool live[2];
+    uint32_t g[2], c[2];
+    double r[2][3];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      live[u] = pos[u] < total;
+      g[u] = live[u] ? tmp[pos[u]] : 0u;
     }
-    const uint32_t a = off[c], e = off[c + 1];
-    uint32_t r = 0;
-    for (uint32_t q = a; q < e; ++q) r += tmp[q] < g ? 1u : 0u;
-    const long long dst = (long long)a + r;
-    if (dst >= (long long)e) {
-      atomicOr(status, kStatusBadIndex);
-      continue;
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const bool ok = live[u] && (long long)g[u] < npts;
+      const long long b3 = 3 * (long long)g[u];
+      r[u][0] = ok ? xyz[b3 + 0] : 0.0;
+      r[u][1] = ok ? xyz[b3 + 1] : 0.0;
+      r[u][2] = ok ? xyz[b3 + 2] : 0.0;
+      c[u] = ok ? cell_of[g[u]] : kInactive;
     }
-    const int f = nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
-    const FrameDesc &fr = frames[f];
-    double s0, s1, s2, q0, q1, q2;
-    fractional(fr, xyz[3 * (long long)g + 0], xyz[3 * (long long)g + 1], xyz[3 * (long long)g + 2],
-               s0, s1, s2);
-    cartesian(fr, s0, s1, s2, q0, q1, q2);
-    sx[dst] = q0;
-    sy[dst] = q1;
-    sz[dst] = q2;
-    const int i = int((long long)g - fr.pt_base);
-    sidx[dst] = i;
-    const uint32_t lc = uint32_t(c - fr.cell_base);
-    scell[dst] = lc;
-    // FP32 offset from the lower cell corner H (c / n) + origin.
-    const int cx = int(lc % uint32_t(fr.nx));
-    const int cy = int((lc / uint32_t(fr.nx)) % uint32_t(fr.ny));
-    const int cz = int(lc / (uint32_t(fr.nx) * uint32_t(fr.ny)));
-    const double f0 = double(cx) / fr.nx, f1 = double(cy) / fr.ny, f2 = double(cz) / fr.nz;
-    const double c0 = fr.h[0] * f0 + fr.h[3] * f1 + fr.h[6] * f2 + fr.origin[0];
-    const double c1 = fr.h[1] * f0 + fr.h[4] * f1 + fr.h[7] * f2 + fr.origin[1];
-    const double c2 = fr.h[2] * f0 + fr.h[5] * f1 + fr.h[8] * f2 + fr.origin[2];
-    rec[dst] = make_float4(float(q0 - c0), float(q1 - c1), float(q2 - c2), __int_as_float(i));
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (!live[u]) continue;
+      if (c[u] >= ncells) {
+        atomicOr(status, kStatusBadIndex);
+        continue;
+      }
+      const uint32_t a = off[c[u]], e = off[c[u] + 1];
+      uint32_t rk = 0;
+      for (uint32_t q = a; q < e; ++q) rk += tmp[q] < g[u] ? 1u : 0u;
+      const long long dst = (long long)a + rk;
+      if (dst >= (long long)e) {
+        atomicOr(status, kStatusBadIndex);
+        continue;
+      }
+      const int f = nframes == 1 ? 0 : frame_of_point(frames, nframes, g[u]);
+      const FrameDesc &fr = frames[f];
+      double s0, s1, s2, q0, q1, q2;
+      fractional(fr, r[u][0], r[u][1], r[u][2], s0, s1, s2);
+      cartesian(fr, s0, s1, s2, q0, q1, q2);
+      sx[dst] = q0;
+      sy[dst] = q1;
+      sz[dst] = q2;
+      const int i = int((long long)g[u] - fr.pt_base);
+      sidx[dst] = i;
+      const uint32_t lc = uint32_t(c[u] - fr.cell_base);
+      scell[dst] = lc;
+      // FP32 offset from the lower cell corner H (c / n) + origin.
+      const int cx = int(lc % uint32_t(fr.nx));
+      const int cy = int((lc / uint32_t(fr.nx)) % uint32_t(fr.ny));
+      const int cz = int(lc / (uint32_t(fr.nx) * uint32_t(fr.ny)));
+      const double f0 = double(cx) / fr.nx, f1 = double(cy) / fr.ny, f2 = double(cz) / fr.nz;
+      const double c0 = fr.h[0] * f0 + fr.h[3] * f1 + fr.h[6] * f2 + fr.origin[0];
+      const double c1 = fr.h[1] * f0 + fr.h[4] * f1 + fr.h[7] * f2 + fr.origin[1];
+      const double c2 = fr.h[2] * f0 + fr.h[5] * f1 + fr.h[8] * f2 + fr.origin[2];
+      rec[dst] = make_float4(float(q0 - c0), float(q1 - c1), float(q2 - c2), __int_as_float(i));
+    }
   }
 }
 
