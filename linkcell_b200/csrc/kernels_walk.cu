@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(BLOCK, 65536 / (128 * BLOCK)) k_walk(BatchBuff
   extern __shared__ double smem[];
   double *hd = smem + threadIdx.x;
   int *hi = reinterpret_cast<int *>(smem + (size_t)b.kmax * BLOCK) + threadIdx.x;
-  const long long total = b.off[b.ncells];
+  const long long total = walk_sources(b);
   const int lane = threadIdx.x & 31;
   LocalCounters cnt;
   for (;;) {
@@ -482,8 +482,9 @@ __global__ void __launch_bounds__(BLOCK, 65536 / (128 * BLOCK)) k_walk(BatchBuff
     if (lane == 0) base = atomicAdd(b.work, 32u);
     base = __shfl_sync(kFull, base, 0);
     if ((long long)base >= total) break;
-    const long long p = (long long)base + lane;
-    if (p < total) walk_source<MODE>(b, p, hd, hi, BLOCK, cnt);
+    const long long q = (long long)base + lane;
+    const long long p = q < total ? walk_source_at(b, q) : -1;
+    if (p >= 0) walk_source<MODE>(b, p, hd, hi, BLOCK, cnt);
     __syncwarp();
   }
   flush_counters(b, cnt);
@@ -507,11 +508,12 @@ __global__ void __launch_bounds__(128) k_replay(BatchBuffers b) {
 }
 
 __global__ void k_queue_all(BatchBuffers b) {
-  const long long total = b.off[b.ncells];
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < total;
-       p += (long long)gridDim.x * blockDim.x)
-    b.replay_list[p] = int(p);
-  if (blockIdx.x == 0 && threadIdx.x == 0) *b.replay_count = uint32_t(total);
+  const long long total = walk_sources(b);
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const long long p = walk_source_at(b, q);
+    if (p >= 0) push_replay(b, p);
+  }
 }
 
 // ------------------------------------------------------------------------
@@ -940,7 +942,7 @@ __device__ void team_source(const BatchBuffers &b, long long p, int lane, LocalC
 
 template <int MODE, int KPL>
 __global__ void __launch_bounds__(256, 2) k_team_walk(BatchBuffers b) {
-  const long long total = b.off[b.ncells];
+  const long long total = walk_sources(b);
   const int lane = threadIdx.x & 31;
   LocalCounters cnt;
   constexpr int kGrab = 4;  // sources per work-queue grab (consecutive, share candidates)
@@ -950,9 +952,9 @@ __global__ void __launch_bounds__(256, 2) k_team_walk(BatchBuffers b) {
     base = __shfl_sync(kFull, base, 0);
     if ((long long)base >= total) break;
     for (int q = 0; q < kGrab; ++q) {
-      const long long p = (long long)base + q;
-      if (p >= total) break;
-      team_source<MODE, KPL>(b, p, lane, cnt);
+      if ((long long)base + q >= total) break;
+      const long long p = walk_source_at(b, (long long)base + q);
+      if (p >= 0) team_source<MODE, KPL>(b, p, lane, cnt);
     }
   }
   flush_counters(b, cnt);
@@ -1425,7 +1427,7 @@ template <int SN>
 __global__ void __launch_bounds__(kSelWarps * 32, SN == 2 ? 3 : 2) k_select_walk(BatchBuffers b) {
   extern __shared__ __align__(16) unsigned char sel_smem[];
   SelShared<SN> &sh = reinterpret_cast<SelShared<SN> *>(sel_smem)[threadIdx.x >> 5];
-  const long long total = b.off[b.ncells];
+  const long long total = walk_sources(b);
   const int lane = threadIdx.x & 31;
   SelCounters cnt;
   if (lane < 8) sh.wc[lane] = 0;
@@ -1437,8 +1439,9 @@ __global__ void __launch_bounds__(kSelWarps * 32, SN == 2 ? 3 : 2) k_select_walk
     base = __shfl_sync(kFull, base, 0);
     if ((long long)base >= total) break;
     for (int q = 0; q < kGrab; ++q) {
-      const long long p = (long long)base + q;
-      if (p >= total) break;
+      if ((long long)base + q >= total) break;
+      const long long p = walk_source_at(b, (long long)base + q);
+      if (p < 0) continue;
       const unsigned long long tie = sh.wc[kWcReplays];
       if (!select_source<SN>(b, p, lane, sh, cnt)) {
         if (lane == 0 && sh.wc[kWcReplays] == tie) ++sh.wc[kWcFallback];
@@ -1885,6 +1888,22 @@ cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t
     case kModeLearned: return launch_block<kModeLearned>(b, w, s);
     default: return launch_block<kModePlainF64>(b, w, s);
   }
+}
+
+namespace {
+__global__ void k_source_order(BatchBuffers b, int *__restrict__ order) {
+  const long long total = b.off[b.ncells];
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < total;
+       p += (long long)gridDim.x * blockDim.x) {
+    const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
+    order[b.frames[f].pt_base + b.sidx[p]] = int(p);
+  }
+}
+}  // namespace
+
+cudaError_t launch_source_order(const BatchBuffers &b, int *order, cudaStream_t s) {
+  k_source_order<<<sm_count() * 8, 256, 0, s>>>(b, order);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s) {

@@ -50,7 +50,19 @@ struct BatchBuffers {
   int8_t *stop_log = nullptr;        // optional: settled shell per sorted source (training)
   const uint32_t *shell_table = nullptr;  // near-first shell offsets, shells 1..shell_rmax
   int shell_rmax = 0;
+  // optional source order: when set, the walk visits sorted positions
+  // src_order[src_begin .. src_end) (-1 entries skipped) instead of all of them
+  const int *src_order = nullptr;
+  long long src_begin = 0, src_end = 0;
 };
+
+// Sources a walk launch visits, and the sorted position of the q-th.
+__device__ __forceinline__ long long walk_sources(const BatchBuffers &b) {
+  return b.src_order ? b.src_end - b.src_begin : (long long)b.off[b.ncells];
+}
+__device__ __forceinline__ long long walk_source_at(const BatchBuffers &b, long long q) {
+  return b.src_order ? (long long)b.src_order[b.src_begin + q] : q;
+}
 
 // Walk statistics accumulated on the device (counters[...]).
 enum WalkCounters : int {
@@ -103,6 +115,17 @@ struct WalkLaunch {
 
 cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s);
 cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s);
+// order[pt_base + index] = sorted position of each active source (order is
+// pre-filled with -1 for masked points).
+cudaError_t launch_source_order(const BatchBuffers &b, int *order, cudaStream_t s);
+// CSR of the entries within a cutoff of n x k rows (sorted ascending, -1 /
+// NaN padded): counts and row_off are rows + 1 scratch words, tile_state /
+// tile_counter the scan's scratch; row_ptr gets rows + 1 offsets, col /
+// dist2 the first cap kept entries.
+cudaError_t launch_csr(const int *nn, const double *d2, long long rows, int k, double cutoff,
+                       uint32_t *counts, uint32_t *row_off, unsigned long long *tile_state,
+                       uint32_t *tile_counter, int *status, int *row_ptr, int *col,
+                       double *dist2, long long cap, cudaStream_t s);
 size_t walk_smem_bytes(int mode, int block, int kmax);
 // Near-first shell-offset table for shells 1..rmax ((2 rmax + 1)^3 entries).
 void build_shell_table(int rmax, uint32_t *out);

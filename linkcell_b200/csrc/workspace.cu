@@ -261,7 +261,10 @@ WorkspaceImpl::WorkspaceImpl() {
       opts.tpp_forced = true;
     }
   }
-  if (const char *z = std::getenv("LINKCELL_ZERO_COPY")) zero_copy_ = std::atoi(z) != 0;
+  if (const char *z = std::getenv("LINKCELL_HOST_ROWS")) {
+    const int v = std::atoi(z);
+    if (v >= 0 && v <= 2) host_rows_ = v;
+  }
   if (const char *b = std::getenv("LINKCELL_BLOCK")) {
     const int v = std::atoi(b);
     if (v == 32 || v == 64 || v == 128 || v == 256) opts.block = v;
@@ -276,6 +279,12 @@ WorkspaceImpl::~WorkspaceImpl() {
   if (own_) cudaStreamSynchronize(own_);
   if (user_set_ && user_) cudaStreamSynchronize(user_);
   if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  if (copy_stream_) {
+    cudaStreamSynchronize(copy_stream_);
+    cudaStreamDestroy(copy_stream_);
+  }
+  for (auto &e : range_ev_)
+    if (e) cudaEventDestroy(e);
   release_all();
   if (h_frames_) cudaFreeHost(h_frames_);
   if (ev_done_) cudaEventDestroy(ev_done_);
@@ -335,6 +344,7 @@ void WorkspaceImpl::release_all() {
   rel(sidx_); rel(replay_list_); rel(replay_i_); rel(scell_); rel(sx_); rel(sy_); rel(sz_);
   rel(replay_d_); rel(rec_); rel(frames_); rel(counters_); rel(h_xyz_); rel(h_d2_);
   rel(h_mask_); rel(h_nn_); rel(active_); rel(proposal_); rel(cell_prop_); rel(stop_log_);
+  rel(order_); rel(csr_counts_); rel(csr_off_);
   rel(model_); rel(shell_table_);
   shell_table_ready_ = false;
 }
@@ -502,6 +512,8 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
     // identical) and keep the faster one for every later batch of this kind
     const int cand[2] = {32, 1};
     float ms[2] = {0.f, 0.f};
+    const bool piping = pipe_.on;
+    pipe_.on = false;  // the trials run whole searches
     for (int c = 0; c < 2; ++c) {
       set_tpp(cand[c]);
       const Code rc = enqueue(b, wl, nf, C, tiles, s, true, detail);
@@ -509,6 +521,7 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
       LC_TRY(cudaEventSynchronize(ev_[3]));
       LC_TRY(cudaEventElapsedTime(&ms[c], ev_[1], ev_[2]));
     }
+    pipe_.on = piping;
     const int best = ms[1] < ms[0] ? 1 : 0;
     tuned_[tkey] = cand[best];
     set_tpp(cand[best]);
@@ -532,6 +545,12 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
                        wl.block, has_model_ ? 1 : 0, opts.fixed_proposal, opts.log_shells};
     if (!graph_exec_ || !(key == graph_key_)) {
       if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  if (copy_stream_) {
+    cudaStreamSynchronize(copy_stream_);
+    cudaStreamDestroy(copy_stream_);
+  }
+  for (auto &e : range_ev_)
+    if (e) cudaEventDestroy(e);
       graph_exec_ = nullptr;
       cudaGraph_t g = nullptr;
       LC_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -601,6 +620,7 @@ Code WorkspaceImpl::enqueue(BatchBuffers &b, const WalkLaunch &wl, int nf, size_
       LC_TRY(cudaMemsetAsync(proposal_.p, 0, P, s));
     }
   }
+  if (pipe_.on && !pipe_.done) return walk_in_row_ranges(b, wl, s, timed, detail);
   if (timed) LC_TRY(cudaEventRecord(ev_[4], s));
   LC_TRY(launch_walk(b, wl, s));
   if (timed) LC_TRY(cudaEventRecord(ev_[2], s));
@@ -725,17 +745,21 @@ Code WorkspaceImpl::run_host(std::vector<FrameDesc> &frames, const double *xyz, 
                              const int *mask, size_t mask_n, int *out_nn, double *out_d2,
                              size_t out_n, std::string &detail) {
   const cudaStream_t s = stream();
-  // Output rows land in a random order, so they cannot be copied back in
-  // pieces while the walk runs. When the caller's output buffers are
-  // page-locked (mapped) host memory, the kernels write the rows straight
-  // into them over the host link instead, overlapping the transfer with the
-  // search; pageable buffers take the device copy and one copy back.
+  // Output rows land in a random order, so a finished search cannot be
+  // copied back in pieces while it runs. With page-locked output buffers
+  // the search is cut into row ranges instead: the walk visits the sources
+  // of one range of output rows at a time (in the order of their rows) and
+  // a copy engine brings each finished range back while the next one is
+  // searched (host_rows 1, the default). host_rows 2 has the kernels write
+  // the rows straight into the mapped host buffers; pageable buffers (or
+  // host_rows 0) take one copy back at the end.
+  const bool locked = mapped_host(out_nn) && (!out_d2 || mapped_host(out_d2));
+  const int how = locked ? host_rows_ : 0;
   int *map_nn = nullptr;
   double *map_d2 = nullptr;
-  if (zero_copy_) {
+  if (how == 2) {
     map_nn = static_cast<int *>(mapped_host(out_nn));
     map_d2 = out_d2 ? static_cast<double *>(mapped_host(out_d2)) : nullptr;
-    if (!map_nn || (out_d2 && !map_d2)) map_nn = nullptr, map_d2 = nullptr;
   }
   LC_TRY(grow(h_xyz_, xyz_n));
   if (!map_nn) {
@@ -746,11 +770,20 @@ Code WorkspaceImpl::run_host(std::vector<FrameDesc> &frames, const double *xyz, 
   LC_TRY(cudaMemcpyAsync(h_xyz_.p, xyz, xyz_n * sizeof(double), cudaMemcpyHostToDevice, s));
   if (mask)
     LC_TRY(cudaMemcpyAsync(h_mask_.p, mask, mask_n * sizeof(int), cudaMemcpyHostToDevice, s));
+  pipe_ = Pipe();
+  if (how == 1 && !opts.graph) {
+    pipe_.on = true;
+    pipe_.host_nn = out_nn;
+    pipe_.host_d2 = out_d2;
+    pipe_.k = frames.empty() ? 0 : frames[0].k;
+  }
   const Code c = run(frames, h_xyz_.p, mask ? h_mask_.p : nullptr, map_nn ? map_nn : h_nn_.p,
                      out_d2 ? (map_nn ? map_d2 : h_d2_.p) : nullptr, false, detail);
+  const bool piped = pipe_.done;
+  pipe_ = Pipe();
   if (c != Code::Ok) return c;
-  last_zero_copy = map_nn != nullptr;
-  if (!map_nn) {
+  last_host_rows = map_nn ? 2 : (piped ? 1 : 0);
+  if (!map_nn && !piped) {
     LC_TRY(cudaMemcpyAsync(out_nn, h_nn_.p, out_n * sizeof(int), cudaMemcpyDeviceToHost, s));
     if (out_d2)
       LC_TRY(cudaMemcpyAsync(out_d2, h_d2_.p, out_n * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -762,6 +795,76 @@ Code WorkspaceImpl::run_host(std::vector<FrameDesc> &frames, const double *xyz, 
     detail = "device status " + std::to_string(st);
     return Code::DeviceStatus;
   }
+  return Code::Ok;
+}
+
+Code WorkspaceImpl::neighbors_within(const int *nn, const double *d2, size_t rows, size_t k,
+                                     double cutoff, int *row_ptr, int *col, double *dist2,
+                                     size_t cap, size_t &nnz, std::string &detail) {
+  nnz = 0;
+  if (rows == 0) return Code::Ok;
+  if (rows * k >= size_t(0x7fffffff)) return Code::TooLarge;
+  const cudaStream_t s = stream();
+  LC_TRY(grow(csr_counts_, rows));
+  LC_TRY(grow(csr_off_, rows + 1));
+  LC_TRY(grow(tile_state_, size_t(scan_tiles((long long)rows))));
+  LC_TRY(grow(tile_counter_, 1));
+  LC_TRY(grow(status_, 1));
+  LC_TRY(cudaMemsetAsync(status_.p, 0, sizeof(int), s));
+  LC_TRY(launch_csr(nn, d2, (long long)rows, int(k), cutoff, csr_counts_.p, csr_off_.p,
+                    tile_state_.p, tile_counter_.p, status_.p, row_ptr, col, dist2,
+                    (long long)cap, s));
+  int total = 0, st = 0;
+  LC_TRY(cudaMemcpyAsync(&total, row_ptr + rows, sizeof(int), cudaMemcpyDeviceToHost, s));
+  LC_TRY(cudaMemcpyAsync(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  LC_TRY(cudaStreamSynchronize(s));
+  if (st != 0) {
+    detail = "device status " + std::to_string(st);
+    return Code::DeviceStatus;
+  }
+  nnz = size_t(total);
+  return Code::Ok;
+}
+
+// The walk and replay of run_host's pipelined path: row range r of the
+// output goes back on the copy stream as soon as its sources are done.
+Code WorkspaceImpl::walk_in_row_ranges(BatchBuffers &b, const WalkLaunch &wl, cudaStream_t s,
+                                       bool timed, std::string &detail) {
+  const long long rows = b.npts;
+  LC_TRY(grow(order_, size_t(rows)));
+  if (!copy_stream_) LC_TRY(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+  for (auto &e : range_ev_)
+    if (!e) LC_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  LC_TRY(cudaMemsetAsync(order_.p, 0xFF, size_t(rows) * sizeof(int), s));
+  LC_TRY(launch_source_order(b, order_.p, s));
+  if (timed) LC_TRY(cudaEventRecord(ev_[4], s));
+  const size_t k = size_t(pipe_.k);
+  for (int r = 0; r < kRowRanges; ++r) {
+    const long long r0 = rows * r / kRowRanges, r1 = rows * (r + 1) / kRowRanges;
+    BatchBuffers br = b;
+    br.src_order = order_.p;
+    br.src_begin = r0;
+    br.src_end = r1;
+    LC_TRY(cudaMemsetAsync(work_.p, 0, sizeof(uint32_t), s));
+    LC_TRY(cudaMemsetAsync(replay_count_.p, 0, sizeof(uint32_t), s));
+    LC_TRY(launch_walk(br, wl, s));
+    LC_TRY(launch_replay(br, s));
+    LC_TRY(cudaEventRecord(range_ev_[r], s));
+    LC_TRY(cudaStreamWaitEvent(copy_stream_, range_ev_[r], 0));
+    const size_t e0 = size_t(r0) * k, ne = size_t(r1 - r0) * k;
+    LC_TRY(cudaMemcpyAsync(pipe_.host_nn + e0, b.out_nn + e0, ne * sizeof(int),
+                           cudaMemcpyDeviceToHost, copy_stream_));
+    if (pipe_.host_d2)
+      LC_TRY(cudaMemcpyAsync(pipe_.host_d2 + e0, b.out_d2 + e0, ne * sizeof(double),
+                             cudaMemcpyDeviceToHost, copy_stream_));
+  }
+  if (timed) LC_TRY(cudaEventRecord(ev_[2], s));
+  if (timed) LC_TRY(cudaEventRecord(ev_[3], s));
+  // the caller's stream finishes only once every range is back
+  LC_TRY(cudaEventRecord(range_ev_[kRowRanges], copy_stream_));
+  LC_TRY(cudaStreamWaitEvent(s, range_ev_[kRowRanges], 0));
+  pipe_.done = true;
+  (void)detail;
   return Code::Ok;
 }
 

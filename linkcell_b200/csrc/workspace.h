@@ -88,7 +88,7 @@ class WorkspaceImpl {
   WalkOptions opts;
   bool collect_stats = true;
   int last_tpp = 0;          // walk design of the last batch
-  bool last_zero_copy = false;  // the last host-pointer search wrote rows straight to host memory
+  int last_host_rows = 0;  // how the last host-pointer search returned its rows (0 copy, 1 ranges, 2 mapped)
   int graph_captures = 0;    // CUDA graphs captured so far
   // Counters and phase times of the last run (waits for it to finish).
   Code fetch_stats(Stats &out, std::string &detail);
@@ -141,7 +141,32 @@ class WorkspaceImpl {
   FrameDesc *h_frames_ = nullptr;
   size_t h_frames_cap_ = 0;
   cudaEvent_t ev_done_ = nullptr;
-  bool zero_copy_ = true;  // LINKCELL_ZERO_COPY=0 turns mapped output rows off
+  // host-pointer searches with page-locked outputs: 1 = row ranges copied back
+  // while the next range is searched, 2 = rows written to mapped host memory,
+  // 0 = one copy at the end (LINKCELL_HOST_ROWS)
+  int host_rows_ = 1;
+  static constexpr int kRowRanges = 8;
+  struct Pipe {
+    bool on = false, done = false;
+    int *host_nn = nullptr;
+    double *host_d2 = nullptr;
+    int k = 0;
+  };
+  Pipe pipe_;
+  Buf<int> order_;
+  cudaStream_t copy_stream_ = nullptr;
+  cudaEvent_t range_ev_[kRowRanges + 1] = {};
+  Code walk_in_row_ranges(BatchBuffers &b, const WalkLaunch &wl, cudaStream_t s, bool timed,
+                          std::string &detail);
+  Buf<uint32_t> csr_counts_, csr_off_;
+
+ public:
+  // CSR of the entries of n x k rows (device) within cutoff; waits.
+  Code neighbors_within(const int *nn, const double *d2, size_t rows, size_t k, double cutoff,
+                        int *row_ptr, int *col, double *dist2, size_t cap, size_t &nnz,
+                        std::string &detail);
+
+ private:
   bool done_pending_ = false;
   void release_all();
 

@@ -1,9 +1,10 @@
 """The host-pointer C ABI (lc_knearest*) on the GPU: page-locked output
-buffers take the mapped-row path (rows written straight to host memory),
-pageable ones the device copy; both must give the reference rows. A fresh
-host thread reads LINKCELL_MODE when its workspace is made, so the learned
-mode (with the shipped network found beside the library) is checked the
-same way."""
+buffers take the row-range path (each range of rows copied back while the
+next is searched) or, with LINKCELL_HOST_ROWS=2, the mapped-row path (rows
+written straight to host memory); pageable ones the device copy. All must
+give the reference rows. A fresh host thread reads LINKCELL_MODE and
+LINKCELL_HOST_ROWS when its workspace is made, so the learned mode (with the
+shipped network found beside the library) is checked the same way."""
 
 from __future__ import annotations
 
@@ -38,9 +39,22 @@ def _in_thread(fn):
     return out["v"]
 
 
-@pytest.mark.parametrize("pinned", [True, False])
+def _with_env(env, fn):
+    old = {key: os.environ.get(key) for key in env}
+    os.environ.update(env)
+    try:
+        return _in_thread(fn)
+    finally:
+        for key, v in old.items():
+            if v is None:
+                os.environ.pop(key, None)
+            else:
+                os.environ[key] = v
+
+
+@pytest.mark.parametrize("pinned,rows", [(True, "1"), (True, "2"), (False, "1")])
 @pytest.mark.parametrize("mode", ["0", "2"])
-def test_host_abi_pinned_and_pageable_outputs(gpu, lib, oracle_mod, pinned, mode):
+def test_host_abi_pinned_and_pageable_outputs(gpu, lib, oracle_mod, pinned, rows, mode):
     import torch
     rng = np.random.default_rng(21)
     n, k = 30000, 16
@@ -55,15 +69,38 @@ def test_host_abi_pinned_and_pageable_outputs(gpu, lib, oracle_mod, pinned, mode
         nn_a = np.full((n, k), -9, dtype=np.int32)
         d2_a = np.zeros((n, k))
         nn_p, d2_p = nn_a.ctypes.data, d2_a.ctypes.data
-    old = os.environ.get("LINKCELL_MODE")
-    os.environ["LINKCELL_MODE"] = mode
-    try:
-        rc = _in_thread(lambda: _host_call(lib, xyz, cell, k, nn_p, d2_p))
-    finally:
-        if old is None:
-            os.environ.pop("LINKCELL_MODE", None)
-        else:
-            os.environ["LINKCELL_MODE"] = old
-    assert rc == 0
+    # two calls: the first one tunes the walk (whole searches), the second
+    # takes the configured host-row path
+    for _ in range(2):
+        rc = _with_env({"LINKCELL_MODE": mode, "LINKCELL_HOST_ROWS": rows},
+                       lambda: [_host_call(lib, xyz, cell, k, nn_p, d2_p) for _ in range(2)])
+        assert rc == [0, 0]
     got = (nn_t.numpy(), d2_t.numpy()) if pinned else (nn_a, d2_a)
-    assert_same(got, want, f"host abi pinned={pinned} mode={mode}")
+    assert_same(got, want, f"host abi pinned={pinned} rows={rows} mode={mode}")
+
+
+@pytest.mark.parametrize("rows", ["1", "2"])
+def test_host_abi_many_frames_with_mask_pinned(gpu, lib, oracle_mod, rows):
+    """lc_knearest_many (shared cell and mask, three frames) through the
+    row-range and mapped paths: masked rows keep -1 / NaN, every frame's
+    rows match the reference."""
+    import torch
+    rng = np.random.default_rng(8)
+    n, nf, k = 9000, 3, 12
+    cell = np.array([[28.0, 0.0, 0.0], [5.0, 27.0, 0.0], [-3.0, 4.0, 29.0]])
+    xyz = np.ascontiguousarray(rng.random((n * nf, 3)) @ cell)
+    mask = (rng.random(n) < 0.9).astype(np.int32)
+    want = oracle_mod.knearest(xyz, cell, k, mask=mask, n_frames=nf)
+    nn_t = torch.full((n * nf, k), -9, dtype=torch.int32).pin_memory()
+    d2_t = torch.zeros((n * nf, k), dtype=torch.float64).pin_memory()
+    c = lc_cell_of(cell)
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+
+    def call():
+        return [lib.lc_knearest_many(ctypes.cast(xyz.ctypes.data, dp), n, nf, ctypes.byref(c), k,
+                                     ctypes.cast(mask.ctypes.data, ip), 0.0,
+                                     ctypes.cast(nn_t.data_ptr(), ip),
+                                     ctypes.cast(d2_t.data_ptr(), dp)) for _ in range(3)]
+    assert _with_env({"LINKCELL_MODE": "2", "LINKCELL_HOST_ROWS": rows}, call) == [0, 0, 0]
+    assert_same((nn_t.numpy(), d2_t.numpy()), want, f"many frames rows={rows}")
