@@ -159,6 +159,19 @@ int lc_gpu_stats(lc_gpu_workspace *ws, long long *counters, int n_counters, doub
  * workspace stream: fold + bin + scan + placement, the walk kernel, and the
  * exact replay of tied sources. Waits for the search to finish. */
 int lc_gpu_phase_times(lc_gpu_workspace *ws, double *prep_ms, double *walk_ms, double *replay_ms);
+/* Neighbour lists within a cutoff, as CSR, from the rows of a finished
+ * search (no counterpart in the reference; its downstream consumers filter
+ * the n * k list by a cutoff themselves). out_nn / out_d2: the search's
+ * device output, rows x k, each row sorted ascending with -1 / NaN padding.
+ * Entry j of row i is kept when out_nn[i*k + j] >= 0 and
+ * out_d2[i*k + j] <= cutoff^2, in row order. row_ptr: rows + 1 device ints;
+ * col and dist2 (dist2 may be NULL): device arrays of capacity cap. Waits,
+ * stores the number of kept entries in *nnz, and fails (with row_ptr and
+ * *nnz complete, the first cap entries written) when *nnz > cap. */
+int lc_gpu_neighbors_within(lc_gpu_workspace *ws, const int *out_nn, const double *out_d2,
+                            size_t rows, size_t k, double cutoff, int *row_ptr, int *col,
+                            double *dist2, size_t cap, size_t *nnz);
+
 /* The same split with the learned mode's shell proposals apart: walk_ms is
  * then the walk kernel alone. */
 int lc_gpu_phase_times4(lc_gpu_workspace *ws, double *prep_ms, double *propose_ms, double *walk_ms,

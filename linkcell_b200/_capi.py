@@ -35,7 +35,7 @@ EXPORTS = (
     "lc_gpu_wait", "lc_gpu_alloc", "lc_gpu_free", "lc_gpu_fill_i32", "lc_gpu_memcpy",
     "lc_gpu_set_mode", "lc_gpu_get_mode", "lc_gpu_set_proposal", "lc_gpu_set_tpp",
     "lc_gpu_get_tpp", "lc_gpu_set_graph", "lc_gpu_graph_captures", "lc_gpu_set_stream", "lc_gpu_stats",
-    "lc_gpu_phase_times", "lc_gpu_phase_times4", "lc_gpu_set_model", "lc_gpu_log_shells", "lc_gpu_training_rows",
+    "lc_gpu_phase_times", "lc_gpu_phase_times4", "lc_gpu_neighbors_within", "lc_gpu_set_model", "lc_gpu_log_shells", "lc_gpu_training_rows",
     "lc_gpu_proposals",
     "lc_gpu_mlp_params", "lc_gpu_mlp_scratch_floats", "lc_gpu_mlp_forward", "lc_gpu_mlp_grad",
     "lc_gpu_mlp_adam",
@@ -94,6 +94,8 @@ def load():
     L.lc_gpu_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), i, dp]
     L.lc_gpu_phase_times.argtypes = [vp, dp, dp, dp]
     L.lc_gpu_phase_times4.argtypes = [vp, dp, dp, dp, dp]
+    L.lc_gpu_neighbors_within.argtypes = [vp, vp, vp, sz, sz, ctypes.c_double, vp, vp, vp, sz,
+                                          ctypes.POINTER(sz)]
     fp = ctypes.POINTER(ctypes.c_float)
     ll = ctypes.c_longlong
     L.lc_gpu_set_model.argtypes = [vp, fp, sz, ctypes.c_float]

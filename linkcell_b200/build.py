@@ -19,7 +19,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblinkcell_b200.so")
-SOURCES = ["kernels_prep.cu", "kernels_walk.cu", "workspace.cu", "capi.cu", "mlp.cu", "noalloc.cu"]
+SOURCES = ["kernels_prep.cu", "kernels_walk.cu", "workspace.cu", "capi.cu", "mlp.cu", "noalloc.cu",
+           "neighbors.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -612,6 +612,22 @@ int lc_gpu_phase_times(lc_gpu_workspace *ws, double *prep_ms, double *walk_ms, d
   return 0;
 }
 
+int lc_gpu_neighbors_within(lc_gpu_workspace *ws, const int *out_nn, const double *out_d2,
+                            size_t rows, size_t k, double cutoff, int *row_ptr, int *col,
+                            double *dist2, size_t cap, size_t *nnz) {
+  if (!ws || !out_nn || !out_d2 || !row_ptr || !nnz || (cap > 0 && !col))
+    return gpu_fail(Code::NullPointer);
+  if (k == 0) return gpu_fail(Code::ZeroK);
+  if (!(cutoff >= 0.0)) return gpu_fail_msg("cutoff must be a non-negative number");
+  std::string detail;
+  const Code c = ws->ws.neighbors_within(out_nn, out_d2, rows, k, cutoff, row_ptr, col, dist2, cap,
+                                         *nnz, detail);
+  if (c != Code::Ok) return gpu_fail(c, detail);
+  if (*nnz > cap) return gpu_fail_msg("neighbour list longer than its buffer");
+  gpu_ok();
+  return 0;
+}
+
 int lc_gpu_phase_times4(lc_gpu_workspace *ws, double *prep_ms, double *propose_ms, double *walk_ms,
                         double *replay_ms) {
   if (!ws) return gpu_fail(Code::NullPointer);
