@@ -1018,7 +1018,7 @@ struct SelShared {
   int si[32 * SN];
   int hist[32];
   unsigned hmax[32];
-  unsigned long long wc[8];  // warp-uniform counters (SelWarpCounter), lane 0 updates
+  unsigned long long wc[16];  // warp-uniform counters (SelWarpCounter), lane 0 updates
 };
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -1033,10 +1033,12 @@ __device__ __forceinline__ float axis_gap(int d, float f) {
   return d > 0 ? float(d) - f : (d < 0 ? f + float(-d - 1) : 0.f);
 }
 
-struct SelCounters {  // per lane; the warp-uniform counters live in SelShared::wc
-  unsigned pairs = 0, pruned = 0, rerank = 0;
+// Walk statistics of a warp, kept in shared memory (lane 0 or shared
+// atomics update them) so that they hold no registers.
+enum SelWarpCounter {
+  kWcInserts, kWcShells, kWcReplays, kWcUnder, kWcOver, kWcExact, kWcFallback, kWcRegather,
+  kWcPairs, kWcPruned, kWcRerank, kWcSlots
 };
-enum SelWarpCounter { kWcInserts, kWcShells, kWcReplays, kWcUnder, kWcOver, kWcExact, kWcFallback };
 
 // Exact quotient of x by n from a double reciprocal estimate (x < 2^32).
 __device__ __forceinline__ uint32_t quot(uint32_t x, uint32_t n, double inv) {
@@ -1048,8 +1050,7 @@ __device__ __forceinline__ uint32_t quot(uint32_t x, uint32_t n, double inv) {
 
 // One source; false: the source must go to the literal replay.
 template <int SN>
-__device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelShared<SN> &sh,
-                              SelCounters &cnt) {
+__device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelShared<SN> &sh) {
   const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
   const FrameDesc &fr = b.frames[f];
   const int Rp = b.proposal[p];
@@ -1072,17 +1073,36 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   const float fb = fr.nhinv[3] * plx + fr.nhinv[4] * ply + fr.nhinv[5] * plz;
   const float fc = fr.nhinv[6] * plx + fr.nhinv[7] * ply + fr.nhinv[8] * plz;
   const float ev0 = fr.ev[0], ev1 = fr.ev[1], ev2 = fr.ev[2];
-  const float thr = fr.sel_thr[Rp];
-  const float qlim = fr.sel_qlim[Rp];
+  // exact distance of buffer entry i (the source's coordinates read when
+  // needed: they stay out of the registers the gather uses)
+  auto exact = [&](int i) -> double {
+    const int t = sh.t[i];
+    const uint32_t m = sh.m[i];
+    double shx, shy, shz;
+    lattice_shift(fr, int((m >> 8) & 3u) - 1, int((m >> 10) & 3u) - 1, int((m >> 12) & 3u) - 1, shx,
+                  shy, shz);
+    return dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], shx, shy, shz);
+  };
+  // The first gather covers only rho2 = max(B(R_p - 1), q B(R_p)): every
+  // candidate of the reaches below R_p, and usually the k nearest. It
+  // settles R* = R_p when at least k candidates lie within rho2 (their
+  // distances are then at most rho2, and everything within rho2 is here);
+  // otherwise the whole ball B(R_p) is gathered again.
+  int total = 0, Rs = 0;
+  bool partial = false;
+  for (int pass = fr.sel_rho_thr[Rp] < fr.sel_thr[Rp] ? 0 : 1; pass < 2; ++pass) {
+  partial = pass == 0;
+  const float thr = partial ? fr.sel_rho_thr[Rp] : fr.sel_thr[Rp];
+  const float qlim = partial ? fr.sel_rho_qlim[Rp] : fr.sel_qlim[Rp];
 
   // 1. gather
   const int W = 2 * Rp + 1;
   const float invW = 1.f / float(W);
   const int nrow = W * W;
-  int total = 0;
+  total = 0;
   for (int r0 = 0; r0 < nrow; r0 += 32) {
     const int row = r0 + lane;
-    int lenA = 0, lenB = 0;
+    int lenA = 0, lenB = 0, pruned = 0;
     SelRow rw;
     if (row < nrow) {
       const int qz = int((float(row) + 0.5f) * invW);  // exact: row < 289, W <= 17
@@ -1101,7 +1121,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
         // dx <= cmax + hm + fa and dx >= cmin - hm + fa - 1 (with margins)
         const int dxh = int(floorf(fminf(cmax + hm + fa + 1e-4f, float(Rp))));
         const int dxl = -int(floorf(fminf(1.f - (cmin - hm) - fa + 1e-4f, float(Rp))));
-        cnt.pruned += unsigned(W - max(0, dxh - dxl + 1));
+        pruned = W - max(0, dxh - dxl + 1);
         int cy = iy + dy, wb = 0, cz = iz + dz, wc = 0;
         if (cy < 0) { cy += ny; wb = -1; } else if (cy >= ny) { cy -= ny; wb = 1; }
         if (cz < 0) { cz += nz; wc = -1; } else if (cz >= nz) { cz -= nz; wc = 1; }
@@ -1141,10 +1161,14 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
         rw.Dz = fdy * fr.ev[5] + fdz * fr.ev[8];
         rw.syz = max(1, max(abs(dy), abs(dz)));
       } else {
-        cnt.pruned += unsigned(W);
+        pruned = W;
       }
     }
     const int len = lenA + lenB;
+    {
+      const unsigned pr = __reduce_add_sync(kFull, unsigned(pruned));
+      if (lane == 0) sh.wc[kWcPruned] += pr;
+    }
     const unsigned ne = __ballot_sync(kFull, len > 0);
     if (!ne) continue;
     int incl = len;
@@ -1155,6 +1179,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
     }
     const int tot = __shfl_sync(kFull, incl, 31);
     const int excl = incl - len;
+    if (lane == 0) sh.wc[kWcPairs] += unsigned(tot);  // the source itself included
     __syncwarp();
     if (len > 0) {
       rw.excl = excl;
@@ -1205,7 +1230,6 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
         float d32 = 0.f;
         uint32_t mm = 0;
         if (live[w]) {
-          ++cnt.pairs;
           const SelRow &R = sh.rows[owner[w]];
           const int dx = sc[w] + xo[w];
           const float fdx = float(dx);
@@ -1230,36 +1254,39 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   }
   __syncwarp();
 
-  const double px = b.sx[p], py = b.sy[p], pz = b.sz[p];
-  auto exact = [&](int i) -> double {
-    const int t = sh.t[i];
-    const uint32_t m = sh.m[i];
-    double shx, shy, shz;
-    lattice_shift(fr, int((m >> 8) & 3u) - 1, int((m >> 10) & 3u) - 1, int((m >> 12) & 3u) - 1, shx,
-                  shy, shz);
-    return dist2_shifted(px, py, pz, b.sx[t], b.sy[t], b.sz[t], shx, shy, shz);
-  };
-
   // 2. stop reach: key counts packed 16 bits per reach (reaches 1-4 | 5-8)
   const float inv_c = 1.f / float(cell_min);
   const float eps_r = fr.sel_epsr[Rp];
   unsigned long long klo = 0, khi = 0;
+  unsigned in_rho = 0;  // first gather: candidates with exact distance <= rho2
   for (int i = lane; i < total; i += 32) {
     const float d32 = sh.d[i];
     const int s = int(sh.m[i] & 255u);
     const float rr = sqrtf(d32) * inv_c;
     const float rc = ceilf(rr);
     int bR;
+    double dex = -1.0;
     if (rr <= 1.f - eps_r) {
       bR = 1;
     } else if (rc - rr < eps_r || rr - (rc - 1.f) < eps_r) {
-      const double dex = exact(i);
-      ++cnt.rerank;
+      dex = exact(i);
+      atomicAdd(&sh.wc[kWcRerank], 1ull);
       int R = max(1, int(rc) - 1);
       while (R <= Rp && !(dex <= stop_bound(R, cell_min))) ++R;
       bR = R;
     } else {
       bR = int(rc);
+    }
+    if (partial) {
+      if (d32 <= fr.sel_rho_lo[Rp]) {
+        ++in_rho;
+      } else if (!(d32 > fr.sel_rho_hi[Rp])) {
+        if (dex < 0.0) {
+          dex = exact(i);
+          atomicAdd(&sh.wc[kWcRerank], 1ull);
+        }
+        in_rho += dex <= fr.sel_rho2[Rp] ? 1u : 0u;
+      }
     }
     const int key = max(s, bR);
     if (key <= Rp) {
@@ -1274,28 +1301,35 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   const unsigned c34 = __reduce_add_sync(kFull, unsigned(klo >> 32));
   const unsigned c56 = __reduce_add_sync(kFull, unsigned(khi));
   const unsigned c78 = __reduce_add_sync(kFull, unsigned(khi >> 32));
-  int Rs = 0;
   {
+    // reaches below R_p are exact in both gathers; R_p itself from the
+    // whole ball, or from the candidates within rho2 after the first
     unsigned cum = 0;
 #pragma unroll
     for (int R = 1; R <= 8; ++R) {
       const unsigned w = R <= 2 ? c12 : (R <= 4 ? c34 : (R <= 6 ? c56 : c78));
       cum += (R & 1) ? (w & 0xffffu) : (w >> 16);
-      if (Rs == 0 && R <= Rp && cum >= unsigned(k)) Rs = R;
+      if (Rs == 0 && (partial ? R < Rp : R <= Rp) && cum >= unsigned(k)) Rs = R;
     }
   }
-  if (Rs == 0) {
+  if (Rs == 0 && partial && __reduce_add_sync(kFull, in_rho) >= unsigned(k)) Rs = Rp;
+  if (Rs != 0) break;
+  if (!partial) {
     if (lane == 0) ++sh.wc[kWcUnder];
     return false;
   }
+  if (lane == 0) ++sh.wc[kWcRegather];
+  __syncwarp();
+  }  // gathers
   if (Rs < Rp)
     { if (lane == 0) ++sh.wc[kWcOver]; }
   else
     { if (lane == 0) ++sh.wc[kWcExact]; }
   if (lane == 0) sh.wc[kWcShells] += unsigned(Rs);
 
-  // 3. select: two-level histogram over candidates of shells <= R* within B(R*)
-  const float Bs_hi = fr.sel_bhi[Rs];
+  // 3. select: two-level histogram over candidates of shells <= R* within
+  // B(R*) (within rho2 when the first gather settled R* = R_p)
+  const float Bs_hi = (partial && Rs == Rp) ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rs];
   const float beta_s = fr.sel_beta[Rs];  // candidates of shells <= R* have offsets <= R*
   const float scale = 32.f / Bs_hi;
   sh.hist[lane] = 0;
@@ -1363,7 +1397,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   }
   __syncwarp();
   if (nS < k) return false;  // cannot happen: T bounds k candidates
-  if (lane == 0) cnt.rerank += unsigned(nS);
+  if (lane == 0) sh.wc[kWcRerank] += unsigned(nS);
   double ed[SN];
   int ej[SN];
 #pragma unroll
@@ -1429,8 +1463,7 @@ __global__ void __launch_bounds__(kSelWarps * 32, SN == 2 ? 3 : 2) k_select_walk
   SelShared<SN> &sh = reinterpret_cast<SelShared<SN> *>(sel_smem)[threadIdx.x >> 5];
   const long long total = walk_sources(b);
   const int lane = threadIdx.x & 31;
-  SelCounters cnt;
-  if (lane < 8) sh.wc[lane] = 0;
+  if (lane < kWcSlots) sh.wc[lane] = 0;
   __syncwarp();
   constexpr int kGrab = 16;  // consecutive sources share most candidates (L1 reuse)
   for (;;) {
@@ -1443,21 +1476,18 @@ __global__ void __launch_bounds__(kSelWarps * 32, SN == 2 ? 3 : 2) k_select_walk
       const long long p = walk_source_at(b, (long long)base + q);
       if (p < 0) continue;
       const unsigned long long tie = sh.wc[kWcReplays];
-      if (!select_source<SN>(b, p, lane, sh, cnt)) {
+      if (!select_source<SN>(b, p, lane, sh)) {
         if (lane == 0 && sh.wc[kWcReplays] == tie) ++sh.wc[kWcFallback];
         if (lane == 0) push_replay(b, p);
       }
       __syncwarp();
     }
   }
-  const unsigned pairs = __reduce_add_sync(kFull, cnt.pairs);
-  const unsigned pruned = __reduce_add_sync(kFull, cnt.pruned);
-  const unsigned rerank = __reduce_add_sync(kFull, cnt.rerank);
   if (lane == 0) {
     unsigned long long *c = reinterpret_cast<unsigned long long *>(b.counters);
-    atomicAdd(&c[kCntPairs], pairs);
-    atomicAdd(&c[kCntPruned], pruned);
-    atomicAdd(&c[kCntRerank], rerank);
+    atomicAdd(&c[kCntPairs], sh.wc[kWcPairs]);
+    atomicAdd(&c[kCntPruned], sh.wc[kWcPruned]);
+    atomicAdd(&c[kCntRerank], sh.wc[kWcRerank]);
     atomicAdd(&c[kCntInserts], sh.wc[kWcInserts]);
     atomicAdd(&c[kCntShells], sh.wc[kWcShells]);
     atomicAdd(&c[kCntReplays], sh.wc[kWcReplays] + sh.wc[kWcFallback]);
@@ -1465,6 +1495,7 @@ __global__ void __launch_bounds__(kSelWarps * 32, SN == 2 ? 3 : 2) k_select_walk
     atomicAdd(&c[kCntPropOver], sh.wc[kWcOver]);
     atomicAdd(&c[kCntPropExact], sh.wc[kWcExact]);
     atomicAdd(&c[kCntFallback], sh.wc[kWcFallback]);
+    atomicAdd(&c[kCntRevisit], sh.wc[kWcRegather]);
   }
 }
 

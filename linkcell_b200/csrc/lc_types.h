@@ -71,6 +71,12 @@ struct FrameDesc {
   float sel_beta[9];
   float sel_bhi[9];
   float sel_epsr[9];
+  // Partial gather at proposal R: rho2 = max(B(R-1), q B(R)) (exact FP64),
+  // the FP32 filter and row-trimming limit at rho2, the FP32 values below /
+  // above which the exact distance is surely <= / > rho2, and rho2 + 2 band
+  // rounded up (histogram range).
+  double sel_rho2[9];
+  float sel_rho_thr[9], sel_rho_qlim[9], sel_rho_lo[9], sel_rho_hi[9], sel_rho_bhi[9];
   double inv_nx, inv_nxy;  // 1 / nx, 1 / (nx ny) for exact quotient estimates
 };
 

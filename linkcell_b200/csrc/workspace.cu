@@ -182,6 +182,24 @@ float float_up(double v) {
   if (double(f) < v) f = std::nextafter(f, std::numeric_limits<float>::infinity());
   return f;
 }
+// Largest float <= v.
+float float_down(double v) {
+  float f = float(v);
+  if (double(f) > v) f = std::nextafter(f, -std::numeric_limits<float>::infinity());
+  return f;
+}
+// Fraction q of B(R_p) the select walk's first gather covers. The k-th
+// distance squared grows like k^(2/3) at a given density, so q follows it
+// from q0 at k = 32 (LINKCELL_SELECT_Q sets q0, 0 < q0 <= 1); q = 1 gathers
+// the whole proposed ball at once.
+double select_rho_q(int k) {
+  static const double q0 = [] {
+    const char *e = std::getenv("LINKCELL_SELECT_Q");
+    const double v = e ? std::atof(e) : 0.65;
+    return (v > 0.0 && v <= 1.0) ? v : 0.65;
+  }();
+  return std::min(1.0, q0 * std::cbrt(double(k) * double(k) / 1024.0));
+}
 }  // namespace
 
 // Per-reach constants of the cube select walk. The FP32 distance of a
@@ -228,6 +246,15 @@ void fill_select_tables(FrameDesc &fd) {
     fd.sel_bhi[R] = float_up(B + 2.0 * band);
     fd.sel_qlim[R] = lam_s > 0.0 ? float_up(double(fd.sel_thr[R]) / lam_s * 1.0001) : 3.0e38f;
     fd.sel_epsr[R] = float_up(band / (2.0 * fd.cell_min * fd.cell_min) + 16.0 * u * (Ru + 2.0));
+    const double bm = double(Ru - 1) * fd.cell_min;
+    const double rho2 = std::max(bm * bm * (1.0 + 1e-4), select_rho_q(fd.k) * B);
+    const double rband = rho2 * 8.0 * u + beta;
+    fd.sel_rho2[R] = rho2;
+    fd.sel_rho_thr[R] = float_up(rho2 * (1.0 + 8.0 * u) + beta);
+    fd.sel_rho_qlim[R] = lam_s > 0.0 ? float_up(double(fd.sel_rho_thr[R]) / lam_s * 1.0001) : 3.0e38f;
+    fd.sel_rho_lo[R] = float_down(rho2 - rband);
+    fd.sel_rho_hi[R] = float_up(rho2 + rband);
+    fd.sel_rho_bhi[R] = float_up(rho2 + 2.0 * rband);
   }
   fd.inv_nx = 1.0 / double(fd.nx);
   fd.inv_nxy = 1.0 / (double(fd.nx) * double(fd.ny));
