@@ -1259,8 +1259,14 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   const float eps_r = fr.sel_epsr[Rp];
   unsigned long long klo = 0, khi = 0;
   unsigned in_rho = 0;  // first gather: candidates with exact distance <= rho2
+  // the level-1 histogram of step 3 for R* = R_p (the common case) on the way
+  const float spec_hi = partial ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rp];
+  const float spec_scale = 32.f / spec_hi;
+  sh.hist[lane] = 0;
+  __syncwarp();
   for (int i = lane; i < total; i += 32) {
     const float d32 = sh.d[i];
+    if (d32 <= spec_hi) atomicAdd(&sh.hist[min(31, int(d32 * spec_scale))], 1);
     const int s = int(sh.m[i] & 255u);
     const float rr = sqrtf(d32) * inv_c;
     const float rc = ceilf(rr);
@@ -1332,14 +1338,18 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   const float Bs_hi = (partial && Rs == Rp) ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rs];
   const float beta_s = fr.sel_beta[Rs];  // candidates of shells <= R* have offsets <= R*
   const float scale = 32.f / Bs_hi;
-  sh.hist[lane] = 0;
   sh.hmax[lane] = 0u;
   __syncwarp();
-  for (int i = lane; i < total; i += 32) {
-    const float d32 = sh.d[i];
-    if (int(sh.m[i] & 255u) <= Rs && d32 <= Bs_hi) atomicAdd(&sh.hist[min(31, int(d32 * scale))], 1);
+  if (Rs != Rp) {  // the histogram built with the stop reach assumed R* = R_p
+    sh.hist[lane] = 0;
+    __syncwarp();
+    for (int i = lane; i < total; i += 32) {
+      const float d32 = sh.d[i];
+      if (int(sh.m[i] & 255u) <= Rs && d32 <= Bs_hi)
+        atomicAdd(&sh.hist[min(31, int(d32 * scale))], 1);
+    }
+    __syncwarp();
   }
-  __syncwarp();
   int bstar, need;
   {
     const int c = sh.hist[lane];
