@@ -48,6 +48,21 @@ class Workspace {
                                 double cell_hint = 0.0, bool wait = true,
                                 double *out_d2 = nullptr);
 
+  /// Extension (no counterpart in the reference, whose batch shares one
+  /// cell): frames with their own cell, point count, k and mask in one call.
+  /// Frame f's points follow frame f - 1's in xyz; its rows start at the sum
+  /// of n * k over the frames before it; mask_offset indexes the device mask
+  /// (-1: no mask). out_len must be that sum (lc_gpu_knearest_batch).
+  struct Frame {
+    std::size_t n = 0, k = 0;
+    Cell cell;
+    double cell_hint = 0.0;
+    long long mask_offset = -1;
+  };
+  void knearest_into_batch(const double *xyz, const Frame *frames, std::size_t nFrames, int *out,
+                           std::size_t out_len, const int *mask = nullptr,
+                           double *out_d2 = nullptr, bool wait = true);
+
   /// The workspace's CUDA stream; all work is enqueued there.
   void *queue();
   void wait();

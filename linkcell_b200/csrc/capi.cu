@@ -87,6 +87,31 @@ Code check_cell(const lc_cell &c) {
   return code == Code::BadCell ? Code::BadCell : Code::Ok;
 }
 
+// Frames with their own cell, n, k and mask offset, planned and searched as
+// one batch (lc_gpu_knearest_batch, Workspace::knearest_into_batch).
+Code run_batch(WorkspaceImpl &w, const double *xyz, const lc_frame *fr, size_t n_frames,
+               const int *mask, int *out_nn, double *out_d2, bool wait, std::string &detail) {
+  if (n_frames == 0) return Code::NoPoints;
+  std::vector<FrameDesc> frames(n_frames);
+  long long out_base = 0;
+  for (size_t f = 0; f < n_frames; ++f) {
+    const lc_frame &x = fr[f];
+    if (x.n == 0) return Code::NoPoints;
+    if (x.k == 0) return Code::ZeroK;
+    if (x.mask_offset >= 0 && !mask) return Code::NullPointer;
+    double rows[9], origin[3];
+    rows_of(x.cell, rows, origin);
+    const Code c = lc::plan_frame(rows, origin, x.cell_hint, int(x.k), frames[f]);
+    if (c != Code::Ok) return c;
+    frames[f].n = (long long)x.n;
+    frames[f].has_mask = x.mask_offset >= 0 ? 1 : 0;
+    frames[f].mask_base = x.mask_offset >= 0 ? x.mask_offset : 0;
+    frames[f].out_base = out_base;
+    out_base += (long long)(x.n * x.k);
+  }
+  return w.run(frames, xyz, mask, out_nn, out_d2, wait, detail);
+}
+
 // n_frames copies of one planned frame (shared cell, shared length-n mask).
 Code shared_frames(const lc_cell &cell, size_t n, size_t n_frames, size_t k, bool has_mask,
                    double hint, std::vector<FrameDesc> &frames) {
@@ -229,6 +254,27 @@ void fill_device_outputs(int *out, double *out_d2, std::size_t need, cudaStream_
   }
 }
 }  // namespace
+
+void Workspace::knearest_into_batch(const double *xyz, const Frame *frames, std::size_t nFrames,
+                                    int *out, std::size_t out_len, const int *mask, double *out_d2,
+                                    bool wait) {
+  if (!impl_) throw Error(lc::gpu_message(Code::NoDevice));
+  if (xyz == nullptr || frames == nullptr || out == nullptr) throw Error("null pointer");
+  std::vector<lc_frame> fr(nFrames);
+  std::size_t need = 0;
+  for (std::size_t f = 0; f < nFrames; ++f) {
+    fr[f].n = frames[f].n;
+    fr[f].k = frames[f].k;
+    fr[f].cell = frames[f].cell.raw();
+    fr[f].cell_hint = frames[f].cell_hint;
+    fr[f].mask_offset = frames[f].mask_offset;
+    need += frames[f].n * frames[f].k;
+  }
+  if (out_len != need) throw Error("out buffer length must be the sum of n * k over the frames");
+  std::string detail;
+  const Code c = run_batch(impl_->ws, xyz, fr.data(), nFrames, mask, out, out_d2, wait, detail);
+  if (c != Code::Ok) throw_code(c, detail);
+}
 
 void Workspace::knearest_into_many(const double *xyz, std::size_t n, std::size_t nFrames,
                                    const Cell &cell, std::size_t k, int *out, std::size_t out_len,
@@ -647,26 +693,8 @@ int lc_gpu_knearest_batch(lc_gpu_workspace *ws, const double *xyz, const lc_fram
                           size_t n_frames, const int *mask, int *out_nn, double *out_d2,
                           int wait) {
   if (!ws || !xyz || !fr || !out_nn) return gpu_fail(Code::NullPointer);
-  if (n_frames == 0) return gpu_fail(Code::NoPoints);
-  std::vector<FrameDesc> frames(n_frames);
-  long long out_base = 0;
-  for (size_t f = 0; f < n_frames; ++f) {
-    const lc_frame &x = fr[f];
-    if (x.n == 0) return gpu_fail(Code::NoPoints);
-    if (x.k == 0) return gpu_fail(Code::ZeroK);
-    if (x.mask_offset >= 0 && !mask) return gpu_fail(Code::NullPointer);
-    double rows[9], origin[3];
-    rows_of(x.cell, rows, origin);
-    const Code c = lc::plan_frame(rows, origin, x.cell_hint, int(x.k), frames[f]);
-    if (c != Code::Ok) return gpu_fail(c);
-    frames[f].n = (long long)x.n;
-    frames[f].has_mask = x.mask_offset >= 0 ? 1 : 0;
-    frames[f].mask_base = x.mask_offset >= 0 ? x.mask_offset : 0;
-    frames[f].out_base = out_base;
-    out_base += (long long)(x.n * x.k);
-  }
   std::string detail;
-  const Code rc = ws->ws.run(frames, xyz, mask, out_nn, out_d2, wait != 0, detail);
+  const Code rc = run_batch(ws->ws, xyz, fr, n_frames, mask, out_nn, out_d2, wait != 0, detail);
   if (rc != Code::Ok) return gpu_fail(rc, detail);
   gpu_ok();
   return 0;
