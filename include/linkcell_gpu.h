@@ -56,7 +56,13 @@ int lc_gpu_knearest_many(lc_gpu_workspace *ws, const double *xyz, size_t n, size
                          double cell_hint, int *out_nn, double *out_d2, int wait);
 
 /* Cell given as device doubles: 3 (ortho lengths), 9 (rows a, b, c) or 12
- * (rows plus origin) (src/gpu/capi.cpp:110-148). */
+ * (rows plus origin) (src/gpu/capi.cpp:110-148). Up to 16 frames the cell
+ * is planned on the device, without the reference's blocking read of the
+ * mesh (src/gpu/knearest.cpp:860-864): the call never synchronizes when
+ * wait == 0, and a workspace with graphs on replays it with whatever cell
+ * the pointer holds at launch. A cell rejected there ("bad cell", "too many
+ * cells") is reported when the batch is waited for (wait != 0, or
+ * lc_gpu_wait through lc_gpu_last_error). More frames read the cell first. */
 int lc_gpu_knearest_many_dcell(lc_gpu_workspace *ws, const double *xyz, size_t n,
                                size_t n_frames, const double *cell, int cell_n, size_t k,
                                const int *mask, double cell_hint, int *out_nn, double *out_d2,
@@ -64,7 +70,8 @@ int lc_gpu_knearest_many_dcell(lc_gpu_workspace *ws, const double *xyz, size_t n
 
 /* The workspace's cudaStream_t (src/gpu/capi.cpp:150-157). */
 void *lc_gpu_queue(lc_gpu_workspace *ws);
-/* Stream barrier (src/gpu/capi.cpp:159-167). */
+/* Stream barrier (src/gpu/capi.cpp:159-167). Errors a kernel of the
+ * batch reported are left in lc_gpu_last_error. */
 void lc_gpu_wait(lc_gpu_workspace *ws);
 
 /* Helpers used by language bindings (src/gpu/capi.cpp:169-282). kind is a

@@ -41,7 +41,8 @@ class Workspace {
                           const double *frameBox = nullptr, double *out_d2 = nullptr);
 
   /// Device-packed cell: 3 ortho lengths, 9 lattice rows, or 12 rows plus
-  /// origin.
+  /// origin. Up to 16 frames the cell is planned on the device (no blocking
+  /// read of the mesh; errors surface at wait).
   void knearest_into_many_dcell(const double *xyz, std::size_t n, std::size_t nFrames,
                                 const double *cell, int cell_n, std::size_t k, int *out,
                                 std::size_t out_len, const int *mask = nullptr,

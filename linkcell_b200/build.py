@@ -6,7 +6,8 @@ All CUDA sources and the C ABI go into one shared library next to this file.
 Host code is compiled with -ffp-contract=off, because the host cell set-up
 must round exactly as the reference Rust code does. Device code keeps FMA
 contraction on; the exact FP64 paths use the __d*_rn intrinsics, which are
-never contracted.
+never contracted. plan.cu, whose cell planner also runs on the device, is
+built with -fmad=false.
 """
 
 from __future__ import annotations
@@ -20,7 +21,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblinkcell_b200.so")
 SOURCES = ["kernels_prep.cu", "kernels_walk.cu", "workspace.cu", "capi.cu", "mlp.cu", "noalloc.cu",
-           "neighbors.cu"]
+           "neighbors.cu", "plan.cu"]
+# plan.cu: the cell planner runs on the host and on the device and must round
+# the same way on both, so its device code is built without FMA contraction.
+EXTRA = {"plan.cu": ["-fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -57,7 +61,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     procs = []
     for s in srcs:
         obj = os.path.join(objdir, s.replace(".cu", ".o"))
-        cmd = [nvcc, *common, "-c", os.path.join(CSRC, s), "-o", obj]
+        cmd = [nvcc, *common, *EXTRA.get(s, []), "-c", os.path.join(CSRC, s), "-o", obj]
         procs.append((s, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
         objs.append(obj)
     failed = []

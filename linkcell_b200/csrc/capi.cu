@@ -210,11 +210,7 @@ Workspace &Workspace::operator=(Workspace &&o) noexcept {
 
 void *Workspace::queue() { return impl_ ? static_cast<void *>(impl_->ws.stream()) : nullptr; }
 
-void Workspace::wait() {
-  if (!impl_) return;
-  std::string detail;
-  if (impl_->ws.wait(detail) != Code::Ok) throw Error(std::string("stream wait: ") + detail);
-}
+
 
 void Workspace::set_mode(int mode) {
   if (mode < 0 || mode > 3) throw Error("unknown walk mode");
@@ -254,6 +250,13 @@ void fill_device_outputs(int *out, double *out_d2, std::size_t need, cudaStream_
   }
 }
 }  // namespace
+
+void Workspace::wait() {
+  if (!impl_) return;
+  std::string detail;
+  const Code c = impl_->ws.wait(detail);
+  if (c != Code::Ok) throw_code(c, detail);
+}
 
 void Workspace::knearest_into_batch(const double *xyz, const Frame *frames, std::size_t nFrames,
                                     int *out, std::size_t out_len, const int *mask, double *out_d2,
@@ -333,6 +336,14 @@ void Workspace::knearest_into_many_dcell(const double *xyz, std::size_t n, std::
   if (xyz == nullptr || out == nullptr || cell == nullptr) throw Error("null pointer");
   if (cell_n != 3 && cell_n != 9 && cell_n != 12)
     throw Error("device cell must have 3, 9, or 12 doubles");
+  if (nFrames <= std::size_t(WorkspaceImpl::kDeviceCellFrames)) {
+    // planned on the device: no read of the cell, graph-capturable
+    std::string detail;
+    const Code c = impl_->ws.run_device_cell(cell, cell_n, (long long)n, int(nFrames), int(k),
+                                             cell_hint, xyz, mask, out, out_d2, wait, detail);
+    if (c != Code::Ok) throw_code(c, detail);
+    return;
+  }
   double h[12] = {0};
   const cudaStream_t s = impl_->ws.stream();
   if (cudaMemcpyAsync(h, cell, size_t(cell_n) * sizeof(double), cudaMemcpyDeviceToHost, s) !=
@@ -454,6 +465,18 @@ int lc_gpu_knearest_many_dcell(lc_gpu_workspace *ws, const double *xyz, size_t n
   if (n == 0 || n_frames == 0) return gpu_fail(Code::NoPoints);
   if (k == 0) return gpu_fail(Code::ZeroK);
   if (cell_n != 3 && cell_n != 9 && cell_n != 12) return gpu_fail(Code::BadCellN);
+  const size_t smax = std::numeric_limits<size_t>::max();
+  if (n > smax / n_frames || n * n_frames > smax / k) return gpu_fail(Code::Overflow);
+  if (n_frames <= size_t(WorkspaceImpl::kDeviceCellFrames)) {
+    // planned on the device: no read of the cell, graph-capturable
+    std::string detail;
+    const Code c = ws->ws.run_device_cell(cell, cell_n, (long long)n, int(n_frames), int(k),
+                                          cell_hint, xyz, mask, out_nn, out_d2, wait != 0, detail);
+    if (c != Code::Ok) return gpu_fail(c, detail);
+    gpu_ok();
+    return 0;
+  }
+  // more frames than the device-planned cell arrays cover: read the cell
   double h[12] = {0};
   const cudaStream_t s = ws->ws.stream();
   cudaError_t e = cudaMemcpyAsync(h, cell, size_t(cell_n) * sizeof(double),
@@ -476,7 +499,8 @@ void *lc_gpu_queue(lc_gpu_workspace *ws) { return ws ? static_cast<void *>(ws->w
 void lc_gpu_wait(lc_gpu_workspace *ws) {
   if (!ws) return;
   std::string detail;
-  if (ws->ws.wait(detail) != Code::Ok) gpu_fail(Code::Cuda, detail);
+  const Code c = ws->ws.wait(detail);
+  if (c != Code::Ok) gpu_fail(c, detail);
 }
 
 int lc_gpu_alloc(void **ptr, size_t bytes) {

@@ -8,6 +8,8 @@
 // cell is one contiguous range of the sorted arrays.
 #include <cuda/atomic>
 
+#include <algorithm>
+
 #include "lc_kernels.h"
 
 namespace lc {
@@ -49,7 +51,7 @@ __global__ void __launch_bounds__(256)
       if (!act[u]) continue;
       fi[u] = nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
       const FrameDesc &fr = frames[fi[u]];
-      if (fr.has_mask && mask[fr.mask_base + (g - fr.pt_base)] == 0) {
+      if (fr.dead || (fr.has_mask && mask[fr.mask_base + (g - fr.pt_base)] == 0)) {
         cell_of[g] = kInactive;
         act[u] = false;
         continue;
@@ -103,111 +105,137 @@ __device__ __forceinline__ void store_release(unsigned long long *p, unsigned lo
   r.store(v, cuda::memory_order_release);
 }
 
+// ncells is the size of the cell arrays. With live set, only the first
+// *live cells are in use (a device-planned batch, whose mesh the host never
+// reads): the scan covers those and also writes the total to off[ncells],
+// where every consumer reads it. Blocks take tiles until none are left, so
+// a grid smaller than the tile count is fine.
 __global__ void __launch_bounds__(kScanBlock)
     k_scan_cells(const uint32_t *__restrict__ count, uint32_t *__restrict__ off, long long ncells,
-                 unsigned long long *__restrict__ tile_state, uint32_t *__restrict__ tile_counter,
-                 int *__restrict__ status) {
+                 const long long *__restrict__ live, unsigned long long *__restrict__ tile_state,
+                 uint32_t *__restrict__ tile_counter, int *__restrict__ status) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kScanBlock / 32];
   __shared__ unsigned long long s_excl;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
-  __syncthreads();
-  const long long tile = s_tile;
-  const long long base = tile * kScanTile + (long long)tid * kScanItems;
-  uint32_t v[kScanItems];
-  if (base + kScanItems <= ncells) {
-    const uint4 *src = reinterpret_cast<const uint4 *>(count + base);
-    const uint4 a = src[0], b = src[1];
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-  } else {
+  const long long nlive = live ? *live : ncells;
+  const long long ntiles = (nlive + kScanTile - 1) / kScanTile;
+  for (;;) {
+    __syncthreads();  // the previous tile's shared values are consumed
+    if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const long long tile = s_tile;
+    if (tile >= ntiles) return;
+    const long long base = tile * kScanTile + (long long)tid * kScanItems;
+    uint32_t v[kScanItems];
+    if (base + kScanItems <= nlive) {
+      const uint4 *src = reinterpret_cast<const uint4 *>(count + base);
+      const uint4 a = src[0], b = src[1];
+      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+      v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    } else {
 #pragma unroll
-    for (int m = 0; m < kScanItems; ++m) v[m] = (base + m < ncells) ? count[base + m] : 0u;
-  }
-  uint32_t tsum = 0;
+      for (int m = 0; m < kScanItems; ++m) v[m] = (base + m < nlive) ? count[base + m] : 0u;
+    }
+    uint32_t tsum = 0;
 #pragma unroll
-  for (int m = 0; m < kScanItems; ++m) tsum += v[m];
-  // inclusive warp scan of thread sums
-  uint32_t x = tsum;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
-    if (lane >= d) x += y;
-  }
-  if (lane == 31) s_warp[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t w = lane < kScanBlock / 32 ? s_warp[lane] : 0u;
+    for (int m = 0; m < kScanItems; ++m) tsum += v[m];
+    // inclusive warp scan of thread sums
+    uint32_t x = tsum;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
-      if (lane >= d) w += y;
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+      if (lane >= d) x += y;
     }
-    if (lane < kScanBlock / 32) s_warp[lane] = w;  // inclusive warp totals
-  }
-  __syncthreads();
-  const uint32_t agg = s_warp[kScanBlock / 32 - 1];
-  const uint32_t texcl = (warp ? s_warp[warp - 1] : 0u) + x - tsum;
-
-  if (warp == 0) {
-    // publish this tile's aggregate, then look back 32 predecessors at a time
-    if (lane == 0) store_release(&tile_state[tile], (tile == 0 ? kFlagP : kFlagA) | agg);
-    unsigned long long excl = 0;
-    if (tile > 0) {
-      long long end = tile;  // predecessors [end-32, end)
-      bool done = false, timeout = false;
-      while (!done && !timeout) {
-        const long long t = end - 1 - lane;
-        unsigned long long w = kFlagP;  // before tile 0: an empty prefix
-        if (t >= 0) {
-          int spins = 0;
-          w = load_acquire(&tile_state[t]);
-          while ((w >> 62) == 0 && spins < kSpinLimit) {
-            ++spins;
-            w = load_acquire(&tile_state[t]);
-          }
-        }
-        const unsigned invalid = __ballot_sync(0xffffffffu, (w >> 62) == 0);
-        if (invalid) {
-          timeout = true;
-          break;
-        }
-        const unsigned pm = __ballot_sync(0xffffffffu, (w >> 62) == 2);
-        const int stop = pm ? (__ffs(pm) - 1) : 31;
-        unsigned long long val = (lane <= stop) ? (w & kValMask) : 0ull;
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t w = lane < kScanBlock / 32 ? s_warp[lane] : 0u;
 #pragma unroll
-        for (int d = 16; d > 0; d >>= 1) val += __shfl_xor_sync(0xffffffffu, val, d);
-        excl += val;
-        if (pm) done = true;
-        end -= 32;
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
+        if (lane >= d) w += y;
       }
-      if (timeout && lane == 0) atomicOr(status, kStatusScanTimeout);
-      if (lane == 0) store_release(&tile_state[tile], kFlagP | ((excl + agg) & kValMask));
+      if (lane < kScanBlock / 32) s_warp[lane] = w;  // inclusive warp totals
     }
-    if (lane == 0) s_excl = excl;
-  }
-  __syncthreads();
-  uint32_t run = uint32_t(s_excl) + texcl;
-  if (base + kScanItems <= ncells) {
-    uint32_t o[kScanItems];
+    __syncthreads();
+    const uint32_t agg = s_warp[kScanBlock / 32 - 1];
+    const uint32_t texcl = (warp ? s_warp[warp - 1] : 0u) + x - tsum;
+
+    if (warp == 0) {
+      // publish this tile's aggregate, then look back 32 predecessors at a time
+      if (lane == 0) store_release(&tile_state[tile], (tile == 0 ? kFlagP : kFlagA) | agg);
+      unsigned long long excl = 0;
+      if (tile > 0) {
+        long long end = tile;  // predecessors [end-32, end)
+        bool done = false, timeout = false;
+        while (!done && !timeout) {
+          const long long t = end - 1 - lane;
+          unsigned long long w = kFlagP;  // before tile 0: an empty prefix
+          if (t >= 0) {
+            int spins = 0;
+            w = load_acquire(&tile_state[t]);
+            while ((w >> 62) == 0 && spins < kSpinLimit) {
+              ++spins;
+              w = load_acquire(&tile_state[t]);
+            }
+          }
+          const unsigned invalid = __ballot_sync(0xffffffffu, (w >> 62) == 0);
+          if (invalid) {
+            timeout = true;
+            break;
+          }
+          const unsigned pm = __ballot_sync(0xffffffffu, (w >> 62) == 2);
+          const int stop = pm ? (__ffs(pm) - 1) : 31;
+          unsigned long long val = (lane <= stop) ? (w & kValMask) : 0ull;
 #pragma unroll
-    for (int m = 0; m < kScanItems; ++m) {
-      o[m] = run;
-      run += v[m];
+          for (int d = 16; d > 0; d >>= 1) val += __shfl_xor_sync(0xffffffffu, val, d);
+          excl += val;
+          if (pm) done = true;
+          end -= 32;
+        }
+        if (timeout && lane == 0) atomicOr(status, kStatusScanTimeout);
+        if (lane == 0) store_release(&tile_state[tile], kFlagP | ((excl + agg) & kValMask));
+      }
+      if (lane == 0) s_excl = excl;
     }
-    uint4 *dst = reinterpret_cast<uint4 *>(off + base);
-    dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
-    dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
-  } else {
+    __syncthreads();
+    uint32_t run = uint32_t(s_excl) + texcl;
+    if (base + kScanItems <= nlive) {
+      uint32_t o[kScanItems];
 #pragma unroll
-    for (int m = 0; m < kScanItems; ++m) {
-      if (base + m < ncells) off[base + m] = run;
-      run += v[m];
+      for (int m = 0; m < kScanItems; ++m) {
+        o[m] = run;
+        run += v[m];
+      }
+      uint4 *dst = reinterpret_cast<uint4 *>(off + base);
+      dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+      dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+    } else {
+#pragma unroll
+      for (int m = 0; m < kScanItems; ++m) {
+        if (base + m < nlive) off[base + m] = run;
+        run += v[m];
+      }
+    }
+    // the thread that owns the last cell also writes the total
+    if (base <= nlive - 1 && nlive - 1 < base + kScanItems) {
+      off[nlive] = run;
+      if (nlive != ncells) off[ncells] = run;
     }
   }
-  // the thread that owns the last cell also writes off[ncells]
-  if (base <= ncells - 1 && ncells - 1 < base + kScanItems) off[ncells] = run;
+}
+
+// Zeroes the cell counts and scan tile states of a device-planned batch
+// (its first *live cells).
+__global__ void k_zero_live(uint32_t *__restrict__ count, unsigned long long *__restrict__ tile_state,
+                            const long long *__restrict__ live) {
+  const long long n = *live, tiles = (n + kScanTile - 1) / kScanTile;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    count[i] = 0u;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += stride)
+    tile_state[t] = 0ull;
 }
 
 // Arrival slots: tmp[off[c] + arank[g]] = g. The output rows of masked
@@ -354,9 +382,21 @@ cudaError_t launch_fold_bin(const BatchBuffers &b, cudaStream_t s) {
 }
 
 cudaError_t launch_scan(const BatchBuffers &b, cudaStream_t s) {
-  const long long tiles = scan_tiles(b.ncells);
-  k_scan_cells<<<unsigned(tiles), kScanBlock, 0, s>>>(b.count, b.off, b.ncells, b.tile_state,
-                                                       b.tile_counter, b.status);
+  long long grid = scan_tiles(b.ncells);
+  if (b.live_cells) {
+    // the live tile count is only known on the device: blocks loop
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    grid = std::min<long long>(grid, (long long)sms * 4);
+  }
+  k_scan_cells<<<unsigned(grid), kScanBlock, 0, s>>>(b.count, b.off, b.ncells, b.live_cells,
+                                                      b.tile_state, b.tile_counter, b.status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zero_live(const BatchBuffers &b, cudaStream_t s) {
+  k_zero_live<<<grid_for(b.ncells, 256), 256, 0, s>>>(b.count, b.tile_state, b.live_cells);
   return cudaGetLastError();
 }
 

@@ -18,7 +18,9 @@ struct BatchBuffers {
   const FrameDesc *frames = nullptr;  // F
   int nframes = 0;
   long long npts = 0;            // P
-  long long ncells = 0;          // C
+  long long ncells = 0;          // C (cell arrays' size)
+  // device-planned batch: the cells in use (first *live_cells), else null
+  const long long *live_cells = nullptr;
   uint32_t *cell_of = nullptr;   // P: batch cell id or kInactive
   uint32_t *arank = nullptr;     // P: arrival rank inside the cell (atomics)
   uint32_t *tmp = nullptr;       // P: point id at its arrival slot
@@ -92,6 +94,8 @@ long long scan_tiles(long long ncells);
 cudaError_t launch_fold_bin(const BatchBuffers &b, cudaStream_t s);
 // exclusive scan of the histogram (single-pass decoupled look-back).
 cudaError_t launch_scan(const BatchBuffers &b, cudaStream_t s);
+// Zeroes counts and scan tile states of the live cells (device-planned batches).
+cudaError_t launch_zero_live(const BatchBuffers &b, cudaStream_t s);
 // stable cell-sorted placement: arrival slots, then in-cell rank by point id.
 cudaError_t launch_place(const BatchBuffers &b, cudaStream_t s);
 

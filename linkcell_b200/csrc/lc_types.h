@@ -18,6 +18,9 @@
 
 namespace lc {
 
+// Most cells of one frame's mesh (MAX_CELLS, src/knearest.rs:20,386-397).
+constexpr long long kMaxCellsPerFrame = 16777216LL;
+
 // Marks a masked point in the cell-of array.
 constexpr uint32_t kInactive = 0xFFFFFFFFu;
 
@@ -27,6 +30,8 @@ enum StatusBits : int {
   kStatusBadIndex = 2,       // a kernel saw an offset outside its buffers
   kStatusReplayOverflow = 4, // replay queue longer than its buffer
   kStatusMmaTimeout = 8,     // a tensor-core product did not complete in bounded time
+  kStatusPlanBadCell = 16,   // the device-cell planner rejected the cell (singular)
+  kStatusPlanTooFine = 32,   // the device-cell planner's mesh exceeds the bin caps
 };
 
 // Per-frame flags (frame_flags[f]).
@@ -54,6 +59,7 @@ struct FrameDesc {
   int k;             // neighbours per source
   int has_mask;
   int mode;          // per-frame walk mode (batched launches)
+  int dead;          // the planner rejected the frame's cell: every point inactive
   long long n;          // points in the frame
   long long pt_base;    // first point of the frame in the batch
   long long cell_base;  // first cell of the frame in the batch

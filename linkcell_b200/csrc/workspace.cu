@@ -1,8 +1,5 @@
-// Host planning and launch sequence of one batch.
-//
-// Host code in this file is compiled with -ffp-contract=off: plan_frame
-// reproduces the reference's FP64 cell set-up bit for bit
-// (src/cell.rs:97-124,322-388 and src/knearest.rs:42-48,377-397,430).
+// Launch sequence of one batch and the device workspace around it (the
+// cell planning is in plan.cu).
 #include "workspace.h"
 
 #include "lc_mlp.h"
@@ -44,220 +41,6 @@ const char *gpu_message(Code c) {
     case Code::NoDevice: return "CUDA driver or nvrtc not loaded";
     default: return cpu_message(c);
   }
-}
-
-namespace {
-
-// src/cell.rs:343-353
-void cross3(const double u[3], const double v[3], double o[3]) {
-  o[0] = u[1] * v[2] - u[2] * v[1];
-  o[1] = u[2] * v[0] - u[0] * v[2];
-  o[2] = u[0] * v[1] - u[1] * v[0];
-}
-double norm3(const double v[3]) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
-
-// Smallest eigenvalue of a symmetric 3x3 matrix (closed form), used only
-// for the conservative cell-pruning bound of the walk.
-double min_eig_sym3(const double m[3][3]) {
-  const double p1 = m[0][1] * m[0][1] + m[0][2] * m[0][2] + m[1][2] * m[1][2];
-  const double q = (m[0][0] + m[1][1] + m[2][2]) / 3.0;
-  if (p1 == 0.0) return std::min(m[0][0], std::min(m[1][1], m[2][2]));
-  const double p2 = (m[0][0] - q) * (m[0][0] - q) + (m[1][1] - q) * (m[1][1] - q) +
-                    (m[2][2] - q) * (m[2][2] - q) + 2.0 * p1;
-  const double p = std::sqrt(p2 / 6.0);
-  double bm[3][3];
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) bm[i][j] = (m[i][j] - (i == j ? q : 0.0)) / p;
-  const double detb = bm[0][0] * (bm[1][1] * bm[2][2] - bm[1][2] * bm[2][1]) -
-                      bm[0][1] * (bm[1][0] * bm[2][2] - bm[1][2] * bm[2][0]) +
-                      bm[0][2] * (bm[1][0] * bm[2][1] - bm[1][1] * bm[2][0]);
-  double r = detb / 2.0;
-  r = std::max(-1.0, std::min(1.0, r));
-  const double phi = std::acos(r) / 3.0;
-  const double e1 = q + 2.0 * p * std::cos(phi);
-  const double e3 = q + 2.0 * p * std::cos(phi + 2.0943951023931953);
-  const double e2 = 3.0 * q - e1 - e3;
-  return std::min(e1, std::min(e2, e3));
-}
-
-}  // namespace
-
-Code plan_frame(const double *rows, const double *origin, double cell_hint, int k, FrameDesc &fd) {
-  std::memset(&fd, 0, sizeof(fd));
-  const double a[3] = {rows[0], rows[1], rows[2]};
-  const double b[3] = {rows[3], rows[4], rows[5]};
-  const double c[3] = {rows[6], rows[7], rows[8]};
-  // H by columns (src/cell.rs:103)
-  for (int r = 0; r < 3; ++r) {
-    fd.h[0 * 3 + r] = a[r];
-    fd.h[1 * 3 + r] = b[r];
-    fd.h[2 * 3 + r] = c[r];
-  }
-  // invert_columns (src/cell.rs:355-388)
-  const double det = a[0] * (b[1] * c[2] - b[2] * c[1]) - a[1] * (b[0] * c[2] - b[2] * c[0]) +
-                     a[2] * (b[0] * c[1] - b[1] * c[0]);
-  if (!std::isfinite(det) || std::fabs(det) < 1e-18) return Code::BadCell;
-  const double invdet = 1.0 / det;
-  fd.hinv[0] = (b[1] * c[2] - b[2] * c[1]) * invdet;
-  fd.hinv[1] = (a[2] * c[1] - a[1] * c[2]) * invdet;
-  fd.hinv[2] = (a[1] * b[2] - a[2] * b[1]) * invdet;
-  fd.hinv[3] = (b[2] * c[0] - b[0] * c[2]) * invdet;
-  fd.hinv[4] = (a[0] * c[2] - a[2] * c[0]) * invdet;
-  fd.hinv[5] = (a[2] * b[0] - a[0] * b[2]) * invdet;
-  fd.hinv[6] = (b[0] * c[1] - b[1] * c[0]) * invdet;
-  fd.hinv[7] = (a[1] * c[0] - a[0] * c[1]) * invdet;
-  fd.hinv[8] = (a[0] * b[1] - a[1] * b[0]) * invdet;
-  // perpendicular widths (src/cell.rs:108-116)
-  double bc[3], ca[3], ab[3];
-  cross3(b, c, bc);
-  cross3(c, a, ca);
-  cross3(a, b, ab);
-  const double wa = std::fabs(det) / norm3(bc);
-  const double wb = std::fabs(det) / norm3(ca);
-  const double wc = std::fabs(det) / norm3(ab);
-  if (!(wa > 0.0 && wb > 0.0 && wc > 0.0)) return Code::BadCell;
-  fd.widths[0] = wa;
-  fd.widths[1] = wb;
-  fd.widths[2] = wc;
-  fd.origin[0] = origin[0];
-  fd.origin[1] = origin[1];
-  fd.origin[2] = origin[2];
-  // is_axis_aligned (src/cell.rs:322-331)
-  {
-    const double scale = std::fmax(norm3(a) + norm3(b) + norm3(c), 1.0);
-    const double tol = 1e-12 * scale;
-    fd.ortho = std::fabs(a[1]) <= tol && std::fabs(a[2]) <= tol && std::fabs(b[0]) <= tol &&
-               std::fabs(b[2]) <= tol && std::fabs(c[0]) <= tol && std::fabs(c[1]) <= tol;
-  }
-  // edge and bins (src/knearest.rs:42-48,377-397). The C ABI passes
-  // Some(hint) only for hint > 0 (src/capi.rs:235-239).
-  double edge = cell_hint > 0.0 ? cell_hint : 3.0;
-  if (!std::isfinite(edge) || edge <= 0.0) edge = 3.0;
-  edge = std::fmin(std::fmin(std::fmin(edge, wa), wb), wc);
-  int nb[3];
-  const double w[3] = {wa, wb, wc};
-  for (int d = 0; d < 3; ++d) {
-    const double nn = std::fmax(std::floor(w[d] / edge), 1.0);
-    if (!std::isfinite(nn) || nn > 1000000.0) return Code::TooFine;
-    nb[d] = int(nn);
-  }
-  const long long ncell = (long long)nb[0] * nb[1] * nb[2];
-  if (!(ncell > 0 && ncell <= 16777216LL)) return Code::TooFine;
-  fd.nx = nb[0];
-  fd.ny = nb[1];
-  fd.nz = nb[2];
-  fd.cell_min = std::fmin(std::fmin(wa / double(nb[0]), wb / double(nb[1])), wc / double(nb[2]));
-  fd.max_reach = std::max(nb[0], std::max(nb[1], nb[2])) / 2 + 1;
-  fd.k = k;
-  // FP32 cell edge vectors and the bin-unit metric (pruning only)
-  double ev[3][3];
-  for (int ax = 0; ax < 3; ++ax)
-    for (int r = 0; r < 3; ++r) {
-      ev[ax][r] = fd.h[ax * 3 + r] / double(nb[ax]);
-      fd.ev[ax * 3 + r] = float(ev[ax][r]);
-    }
-  double g[3][3];
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) g[i][j] = ev[i][0] * ev[j][0] + ev[i][1] * ev[j][1] + ev[i][2] * ev[j][2];
-  fd.lam_min = std::max(0.0, min_eig_sym3(g)) * (1.0 - 1e-6);
-  // (H / n)^-1 = diag(n) Hinv: row a of Hinv times n_a
-  for (int ax = 0; ax < 3; ++ax)
-    for (int r = 0; r < 3; ++r) fd.nhinv[ax * 3 + r] = float(double(nb[ax]) * fd.hinv[r * 3 + ax]);
-  double ell = 0.0;
-  for (int r = 0; r < 3; ++r)
-    ell = std::max(ell, std::fabs(ev[0][r]) + std::fabs(ev[1][r]) + std::fabs(ev[2][r]));
-  fd.ell = float(ell * (1.0 + 1e-6));
-  double mag = std::fabs(origin[0]) + std::fabs(origin[1]) + std::fabs(origin[2]);
-  for (int t = 0; t < 9; ++t) mag += std::fabs(fd.h[t]);
-  // generous: 2^-36 of the largest coordinate / shift magnitude per unit wrap
-  fd.eps64 = std::ldexp(mag, -36);
-  fill_select_tables(fd);
-  return Code::Ok;
-}
-
-namespace {
-// Smallest float >= v.
-float float_up(double v) {
-  float f = float(v);
-  if (double(f) < v) f = std::nextafter(f, std::numeric_limits<float>::infinity());
-  return f;
-}
-// Largest float <= v.
-float float_down(double v) {
-  float f = float(v);
-  if (double(f) > v) f = std::nextafter(f, -std::numeric_limits<float>::infinity());
-  return f;
-}
-// Fraction q of B(R_p) the select walk's first gather covers. The k-th
-// distance squared grows like k^(2/3) at a given density, so q follows it
-// from q0 at k = 32 (LINKCELL_SELECT_Q sets q0, 0 < q0 <= 1); q = 1 gathers
-// the whole proposed ball at once.
-double select_rho_q(int k) {
-  static const double q0 = [] {
-    const char *e = std::getenv("LINKCELL_SELECT_Q");
-    const double v = e ? std::atof(e) : 0.65;
-    return (v > 0.0 && v <= 1.0) ? v : 0.65;
-  }();
-  return std::min(1.0, q0 * std::cbrt(double(k) * double(k) / 1024.0));
-}
-}  // namespace
-
-// Per-reach constants of the cube select walk. The FP32 distance of a
-// candidate whose cell offset is at most R per axis differs from the
-// reference's FP64 value by at most band(d) = 8u d + beta(R), with
-// e = u (6R + 8) ell + eps64 (R + 2) the per-component error of the FP32
-// offset and beta(R) = 4 e^2 / u + 4 e^2 (the cross terms 2 |D| e are
-// bounded by u D^2 + e^2 / u); 1e-6 of margin on top.
-void fill_select_tables(FrameDesc &fd) {
-  const double u = 5.9604644775390625e-08;  // 2^-24
-  // Row trimming: in bin units the squared distance of an offset D is
-  // D^T M D with M = E^T E. For fixed (D_b, D_c) the D_a giving at most thr
-  // lie within h of c = -(M_ab D_b + M_ac D_c) / M_aa, h^2 = (thr - S) / M_aa,
-  // S the Schur form of (D_b, D_c), bounded below by lam_s |(D_b, D_c)|^2.
-  double E[3][3];
-  for (int a = 0; a < 3; ++a)
-    for (int r = 0; r < 3; ++r) E[a][r] = fd.h[a * 3 + r] / double(a == 0 ? fd.nx : (a == 1 ? fd.ny : fd.nz));
-  double M[3][3];
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) M[i][j] = E[i][0] * E[j][0] + E[i][1] * E[j][1] + E[i][2] * E[j][2];
-  const double s11 = M[1][1] - M[0][1] * M[0][1] / M[0][0];
-  const double s12 = M[1][2] - M[0][1] * M[0][2] / M[0][0];
-  const double s22 = M[2][2] - M[0][2] * M[0][2] / M[0][0];
-  const double tr = 0.5 * (s11 + s22), df = 0.5 * (s11 - s22);
-  double lam_s = std::max(0.0, tr - std::sqrt(df * df + s12 * s12)) * 0.99;
-  fd.sel_r01 = float(M[0][1] / M[0][0]);
-  fd.sel_r02 = float(M[0][2] / M[0][0]);
-  fd.sel_ls00 = float(lam_s / M[0][0]);
-  if (!(lam_s > 1e-9 * M[0][0])) {
-    // near-degenerate metric: the isotropic bound lam_min |D|^2 <= thr instead
-    lam_s = double(float(fd.lam_min) * 0.99f);
-    fd.sel_r01 = fd.sel_r02 = 0.f;
-    fd.sel_ls00 = 1.f;
-  }
-  for (int R = 0; R <= 8; ++R) {
-    const int Ru = R < 1 ? 1 : R;
-    const double e = u * (6.0 * Ru + 8.0) * double(fd.ell) + fd.eps64 * (Ru + 2.0);
-    const double beta = (4.0 * e * e / u + 4.0 * e * e) * (1.0 + 1e-6);
-    const double b = double(Ru) * fd.cell_min;
-    const double B = b * b;
-    const double band = B * 8.0 * u + beta;
-    fd.sel_beta[R] = float_up(beta);
-    fd.sel_thr[R] = float_up(B * (1.0 + 8.0 * u) + beta);
-    fd.sel_bhi[R] = float_up(B + 2.0 * band);
-    fd.sel_qlim[R] = lam_s > 0.0 ? float_up(double(fd.sel_thr[R]) / lam_s * 1.0001) : 3.0e38f;
-    fd.sel_epsr[R] = float_up(band / (2.0 * fd.cell_min * fd.cell_min) + 16.0 * u * (Ru + 2.0));
-    const double bm = double(Ru - 1) * fd.cell_min;
-    const double rho2 = std::max(bm * bm * (1.0 + 1e-4), select_rho_q(fd.k) * B);
-    const double rband = rho2 * 8.0 * u + beta;
-    fd.sel_rho2[R] = rho2;
-    fd.sel_rho_thr[R] = float_up(rho2 * (1.0 + 8.0 * u) + beta);
-    fd.sel_rho_qlim[R] = lam_s > 0.0 ? float_up(double(fd.sel_rho_thr[R]) / lam_s * 1.0001) : 3.0e38f;
-    fd.sel_rho_lo[R] = float_down(rho2 - rband);
-    fd.sel_rho_hi[R] = float_up(rho2 + rband);
-    fd.sel_rho_bhi[R] = float_up(rho2 + 2.0 * rband);
-  }
-  fd.inv_nx = 1.0 / double(fd.nx);
-  fd.inv_nxy = 1.0 / (double(fd.nx) * double(fd.ny));
 }
 
 // Device address of page-locked host memory, or null (pageable, device or
@@ -333,7 +116,10 @@ Code WorkspaceImpl::wait(std::string &detail) {
     detail = cudaGetErrorString(e);
     return Code::Cuda;
   }
-  return Code::Ok;
+  if (!done_pending_) return Code::Ok;
+  // the last batch ran without a wait: its status word is reported here
+  done_pending_ = false;
+  return read_status(detail);
 }
 
 template <class T>
@@ -371,7 +157,7 @@ void WorkspaceImpl::release_all() {
   rel(sidx_); rel(replay_list_); rel(replay_i_); rel(scell_); rel(sx_); rel(sy_); rel(sz_);
   rel(replay_d_); rel(rec_); rel(frames_); rel(counters_); rel(h_xyz_); rel(h_d2_);
   rel(h_mask_); rel(h_nn_); rel(active_); rel(proposal_); rel(cell_prop_); rel(stop_log_);
-  rel(order_); rel(csr_counts_); rel(csr_off_);
+  rel(order_); rel(csr_counts_); rel(csr_off_); rel(live_);
   rel(model_); rel(shell_table_);
   shell_table_ready_ = false;
 }
@@ -430,6 +216,7 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   LC_TRY(grow(replay_list_, P));
   LC_TRY(grow(frames_, size_t(nf)));
   LC_TRY(grow(counters_, size_t(kNumCounters)));
+  if (dcell_.on) LC_TRY(grow(live_, 1));
   if (opts.log_shells) LC_TRY(grow(stop_log_, P));
   if (opts.mode == kModeLearned && !has_model_ && opts.fixed_proposal <= 0 && !model_tried_) {
     model_tried_ = true;
@@ -486,6 +273,7 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   b.nframes = nf;
   b.npts = npts;
   b.ncells = ncells;
+  b.live_cells = dcell_.on ? live_.p : nullptr;
   b.cell_of = cell_of_.p;
   b.arank = arank_.p;
   b.tmp = tmp_.p;
@@ -569,15 +357,11 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
     // autotuning left this batch's results and stats in place
   } else if (opts.graph) {
     const GraphKey key{npts, ncells, nf, kmax, xyz, mask, out_nn, out_d2, wl.mode, wl.tpp,
-                       wl.block, has_model_ ? 1 : 0, opts.fixed_proposal, opts.log_shells};
+                       wl.block, has_model_ ? 1 : 0, opts.fixed_proposal, opts.log_shells,
+                       dcell_.on ? dcell_.cell : nullptr, dcell_.on ? dcell_.cell_n : 0,
+                       dcell_.on ? dcell_.hint : 0.0};
     if (!graph_exec_ || !(key == graph_key_)) {
       if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
-  if (copy_stream_) {
-    cudaStreamSynchronize(copy_stream_);
-    cudaStreamDestroy(copy_stream_);
-  }
-  for (auto &e : range_ev_)
-    if (e) cudaEventDestroy(e);
       graph_exec_ = nullptr;
       cudaGraph_t g = nullptr;
       LC_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -610,8 +394,15 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   if (!wait) return Code::Ok;
   LC_TRY(cudaStreamSynchronize(s));
   done_pending_ = false;
+  return read_status(detail);
+}
+
+Code WorkspaceImpl::read_status(std::string &detail) {
+  if (!status_.p) return Code::Ok;
   int st = 0;
   LC_TRY(cudaMemcpy(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st & kStatusPlanBadCell) return Code::BadCell;
+  if (st & kStatusPlanTooFine) return Code::TooFine;
   if (st != 0) {
     detail = "device status " + std::to_string(st);
     return Code::DeviceStatus;
@@ -619,12 +410,34 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   return Code::Ok;
 }
 
+Code WorkspaceImpl::run_device_cell(const double *cell, int cell_n, long long n, int nframes,
+                                    int k, double hint, const double *xyz, const int *mask,
+                                    int *out_nn, double *out_d2, bool wait, std::string &detail) {
+  if (nframes < 1 || nframes > kDeviceCellFrames) return Code::TooLarge;
+  // host-side placeholders: sizes only; the device planner writes the table
+  std::vector<FrameDesc> frames(static_cast<size_t>(nframes));
+  for (auto &fd : frames) {
+    std::memset(&fd, 0, sizeof(fd));
+    fd.n = n;
+    fd.k = k;
+    fd.nx = int(kMaxCellsPerFrame);
+    fd.ny = fd.nz = 1;
+    fd.has_mask = mask ? 1 : 0;
+  }
+  dcell_ = DeviceCell{true, cell, cell_n, n, nframes, k, hint};
+  const Code c = run(frames, xyz, mask, out_nn, out_d2, wait, detail);
+  dcell_.on = false;
+  return c;
+}
+
 Code WorkspaceImpl::enqueue(BatchBuffers &b, const WalkLaunch &wl, int nf, size_t C,
                             long long tiles, cudaStream_t s, bool timed, std::string &detail) {
-  LC_TRY(cudaMemcpyAsync(frames_.p, h_frames_, sizeof(FrameDesc) * size_t(nf),
-                         cudaMemcpyHostToDevice, s));
-  LC_TRY(cudaMemsetAsync(count_.p, 0, C * sizeof(uint32_t), s));
-  LC_TRY(cudaMemsetAsync(tile_state_.p, 0, size_t(tiles) * sizeof(unsigned long long), s));
+  if (!dcell_.on) {
+    LC_TRY(cudaMemcpyAsync(frames_.p, h_frames_, sizeof(FrameDesc) * size_t(nf),
+                           cudaMemcpyHostToDevice, s));
+    LC_TRY(cudaMemsetAsync(count_.p, 0, C * sizeof(uint32_t), s));
+    LC_TRY(cudaMemsetAsync(tile_state_.p, 0, size_t(tiles) * sizeof(unsigned long long), s));
+  }
   LC_TRY(cudaMemsetAsync(tile_counter_.p, 0, sizeof(uint32_t), s));
   LC_TRY(cudaMemsetAsync(work_.p, 0, sizeof(uint32_t), s));
   LC_TRY(cudaMemsetAsync(replay_count_.p, 0, sizeof(uint32_t), s));
@@ -632,6 +445,12 @@ Code WorkspaceImpl::enqueue(BatchBuffers &b, const WalkLaunch &wl, int nf, size_
   LC_TRY(cudaMemsetAsync(frame_flags_.p, 0, sizeof(int) * size_t(nf), s));
   LC_TRY(cudaMemsetAsync(counters_.p, 0, sizeof(long long) * kNumCounters, s));
   if (timed) LC_TRY(cudaEventRecord(ev_[0], s));
+  if (dcell_.on) {
+    // the frame table and the live cell count come from the device cell
+    LC_TRY(launch_plan_device_cell(dcell_.cell, dcell_.cell_n, dcell_.n, dcell_.nframes, dcell_.k,
+                                   dcell_.hint, b.mask, frames_.p, live_.p, status_.p, s));
+    LC_TRY(launch_zero_live(b, s));
+  }
   LC_TRY(launch_fold_bin(b, s));
   LC_TRY(launch_scan(b, s));
   LC_TRY(launch_place(b, s));
@@ -816,13 +635,8 @@ Code WorkspaceImpl::run_host(std::vector<FrameDesc> &frames, const double *xyz, 
       LC_TRY(cudaMemcpyAsync(out_d2, h_d2_.p, out_n * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
   LC_TRY(cudaStreamSynchronize(s));
-  int st = 0;
-  LC_TRY(cudaMemcpy(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost));
-  if (st != 0) {
-    detail = "device status " + std::to_string(st);
-    return Code::DeviceStatus;
-  }
-  return Code::Ok;
+  done_pending_ = false;
+  return read_status(detail);
 }
 
 Code WorkspaceImpl::neighbors_within(const int *nn, const double *d2, size_t rows, size_t k,

@@ -41,8 +41,15 @@ const char *gpu_message(Code c);
 // src/knearest.rs:377-397,430) into a FrameDesc. rows = a, b, c (9 doubles)
 // and origin (3 doubles). hint <= 0 or NaN selects the default edge 3.0.
 Code plan_frame(const double *rows, const double *origin, double cell_hint, int k, FrameDesc &fd);
-// Fills the per-reach constants of the cube select walk (FrameDesc::sel_*).
-void fill_select_tables(FrameDesc &fd);
+// Fraction of B(R_p) the select walk's first gather covers, for k.
+double select_rho_q(int k);
+// Plans the shared cell of a device-cell batch on the device (no host
+// read of the cell) and writes the frame table of nframes frames of n
+// points; *live_cells gets the batch's cell count. Rejections leave
+// kStatusPlanBadCell / kStatusPlanTooFine in status.
+cudaError_t launch_plan_device_cell(const double *cell, int cell_n, long long n, int nframes, int k,
+                                    double hint, const int *mask, FrameDesc *frames,
+                                    long long *live_cells, int *status, cudaStream_t s);
 // Device address of page-locked host memory, or null.
 void *mapped_host(const void *p);
 
@@ -84,6 +91,17 @@ class WorkspaceImpl {
   // device pointers.
   Code run(std::vector<FrameDesc> &frames, const double *xyz, const int *mask, int *out_nn,
            double *out_d2, bool wait, std::string &detail);
+
+  // Device-cell batch without a host read of the cell: nframes frames of n
+  // points sharing the cell at the device pointer cell (cell_n = 3, 9 or 12
+  // doubles), planned on the device at every launch (and every graph
+  // replay). The cell arrays are sized for the largest mesh a cell may have
+  // (kMaxCellsPerFrame per frame), so nframes is at most kDeviceCellFrames.
+  // A rejected cell reports BadCell / TooFine when the batch is waited for.
+  static constexpr int kDeviceCellFrames = 16;
+  Code run_device_cell(const double *cell, int cell_n, long long n, int nframes, int k,
+                       double hint, const double *xyz, const int *mask, int *out_nn,
+                       double *out_d2, bool wait, std::string &detail);
 
   WalkOptions opts;
   bool collect_stats = true;
@@ -128,12 +146,27 @@ class WorkspaceImpl {
     int nf = 0, kmax = 0;
     const void *xyz = nullptr, *mask = nullptr, *nn = nullptr, *d2 = nullptr;
     int mode = 0, tpp = 0, block = 0, model = 0, fixed = 0, log = 0;
+    const void *dcell = nullptr;  // device-planned batch: its cell and launch constants
+    int cell_n = 0;
+    double hint = 0.0;
     bool operator==(const GraphKey &o) const {
       return npts == o.npts && ncells == o.ncells && nf == o.nf && kmax == o.kmax && xyz == o.xyz &&
              mask == o.mask && nn == o.nn && d2 == o.d2 && mode == o.mode && tpp == o.tpp &&
-             block == o.block && model == o.model && fixed == o.fixed && log == o.log;
+             block == o.block && model == o.model && fixed == o.fixed && log == o.log &&
+             dcell == o.dcell && cell_n == o.cell_n && hint == o.hint;
     }
   };
+  // the device-cell batch being enqueued (run_device_cell)
+  struct DeviceCell {
+    bool on = false;
+    const double *cell = nullptr;
+    int cell_n = 0;
+    long long n = 0;
+    int nframes = 0, k = 0;
+    double hint = 0.0;
+  };
+  DeviceCell dcell_;
+  Buf<long long> live_;
   GraphKey graph_key_;
   cudaGraphExec_t graph_exec_ = nullptr;
   bool graph_total_ = false;
@@ -169,6 +202,7 @@ class WorkspaceImpl {
  private:
   bool done_pending_ = false;
   void release_all();
+  Code read_status(std::string &detail);  // the status word of the last batch
 
   int device_ = -1;
   cudaStream_t own_ = nullptr;
