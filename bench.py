@@ -56,6 +56,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-gpulite", action="store_true",
+                   help="skip the reference's gpulite GPU path timed beside the headline")
+    p.add_argument("--gpulite-child", action="store_true", help=argparse.SUPPRESS)
     p.add_argument("--workload", default="c2", choices=["c2", "c3"],
                    help="c2: the 4M bimodal frame (headline); c3: 256 frames of uneven n, "
                         "cell, k and mask in one batched call")
@@ -183,6 +186,123 @@ def cpu_baseline(w, seconds_target=15.0):
             "sample": (f"fold+bin+lists over all {n} points ({r['prep_s']:.2f} s) plus the walk of "
                        f"{r['walked']} sources (every {stride}-th, {r['walk_s']:.2f} s), "
                        f"extrapolated to all sources")}
+
+
+GPULITE_LIB = os.path.join(ROOT, "oracle", "_ref", "libref_gpulite.so")
+GPULITE_K = 16            # the gpulite path supports k <= 16 (src/gpu/knearest.cpp:23)
+GPULITE_CELLS = 262144    # ... and at most this many cells (src/gpu/knearest.cpp:24)
+
+
+def gpulite_hint(cell, k_cap=GPULITE_CELLS):
+    """The smallest cell edge (3.0 and up, in steps of 0.05) whose mesh of
+    the given cell stays within the gpulite path's cell cap."""
+    h = np.asarray(cell, dtype=np.float64)
+    a, b, c = h[0], h[1], h[2]
+    det = abs(float(np.dot(a, np.cross(b, c))))
+    widths = [det / np.linalg.norm(np.cross(b, c)), det / np.linalg.norm(np.cross(c, a)),
+              det / np.linalg.norm(np.cross(a, b))]
+    edge = 3.0
+    while np.prod([max(1, int(np.floor(wd / edge))) for wd in widths]) > k_cap:
+        edge = round(edge + 0.05, 2)
+    return edge
+
+
+def gpulite_child(args):
+    """Child process of the gpulite leg: the reference's own gpulite GPU path
+    (src/gpu/knearest.cpp + capi.cpp, built from the reference sources into
+    oracle/_ref by oracle/build_ref.sh) timed through its C ABI on the same
+    points as the headline, at k = 16 and the smallest cell edge its cell cap
+    allows. Only that library is loaded here (it exports the same lc_gpu_*
+    names as ours). Prints one JSON line."""
+    import torch
+    torch.cuda.set_device(0)
+    lib = ctypes.CDLL(GPULITE_LIB)
+    vp, sz, d, i = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_double, ctypes.c_int
+    lib.lc_gpu_workspace_new.restype = vp
+    lib.lc_gpu_workspace_free.argtypes = [vp]
+    lib.lc_gpu_last_error.restype = ctypes.c_char_p
+    lib.lc_gpu_knearest_many.argtypes = [vp, vp, sz, sz, vp, sz, vp, d, vp, vp, i]
+    w = workload(args.n, args.k, seed=2)
+    n = w["xyz"].shape[0]
+    hint = gpulite_hint(w["cell"])
+    rows = np.asarray(w["cell"], dtype=np.float64).reshape(-1)
+    cell = (ctypes.c_double * 12)(*[float(v) for v in rows], 0.0, 0.0, 0.0)
+    x = torch.as_tensor(w["xyz"], device="cuda")
+    nn = torch.empty((n, GPULITE_K), dtype=torch.int32, device="cuda")
+    d2 = torch.empty((n, GPULITE_K), dtype=torch.float64, device="cuda")
+    ws = lib.lc_gpu_workspace_new()
+    if not ws:
+        print(json.dumps({"unavailable": (lib.lc_gpu_last_error() or b"").decode()}))
+        return
+
+    def step():
+        rc = lib.lc_gpu_knearest_many(ws, x.data_ptr(), n, 1, ctypes.byref(cell), GPULITE_K, None,
+                                      hint, nn.data_ptr(), d2.data_ptr(), 1)
+        if rc != 0:
+            raise RuntimeError((lib.lc_gpu_last_error() or b"").decode())
+    torch.cuda.synchronize()
+    for _ in range(max(2, args.warmup)):  # the first call compiles the kernels (nvrtc)
+        step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    lib.lc_gpu_workspace_free(ws)
+    ms = 1000.0 * statistics.median(times)
+    print(json.dumps({"value": n / (ms / 1000.0), "ms_per_step": ms, "k": GPULITE_K,
+                      "cell_hint": hint, "n": n}))
+
+
+def gpulite_leg(args, L, ws, x, n):
+    """The reference's gpulite GPU path, timed in a child process, and ours
+    on the same configuration (k = 16, the same cell edge), both as
+    synchronous calls with inputs resident on the device, median wall time."""
+    import torch
+    if not os.path.exists(GPULITE_LIB):
+        return {"unavailable": "oracle/_ref/libref_gpulite.so not built (no reference sources)"}
+    steps = 5
+    cmd = [sys.executable, os.path.abspath(__file__), "--gpulite-child", "--n", str(args.n),
+           "--k", str(args.k), "--steps", str(steps), "--warmup", "2"]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "gpulite child did not finish in 900 s"}
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        tail = (r.stderr.strip().splitlines() or ["no output"])[-1]
+        return {"unavailable": f"gpulite child failed: {tail[:200]}"}
+    ref = json.loads(lines[-1])
+    if "unavailable" in ref:
+        return ref
+    from linkcell_b200 import _capi
+    from linkcell_b200 import _cell_struct
+    w = workload(args.n, args.k, seed=2)
+    cell = _cell_struct(np.asarray(w["cell"], dtype=np.float64))
+    nn = torch.empty((n, GPULITE_K), dtype=torch.int32, device="cuda")
+    d2 = torch.empty((n, GPULITE_K), dtype=torch.float64, device="cuda")
+
+    def step():
+        rc = L.lc_gpu_knearest_many(ws, x.data_ptr(), n, 1, ctypes.byref(cell), GPULITE_K, None,
+                                    ref["cell_hint"], nn.data_ptr(), d2.data_ptr(), 1)
+        assert rc == 0, _capi.gpu_error()
+    for _ in range(3):
+        step()
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    ours_ms = 1000.0 * statistics.median(times)
+    del nn, d2
+    return {"value": ref["value"], "unit": "sources/s", "ms_per_step": ref["ms_per_step"],
+            "config": (f"the headline's {n} points at k = {GPULITE_K} and cell_hint "
+                       f"{ref['cell_hint']} (the gpulite path takes k <= 16 and at most "
+                       f"{GPULITE_CELLS} cells, so it cannot run the k = 32 headline)"),
+            "timer": "host wall clock around a synchronous call, median of 5",
+            "kind": "reference gpulite (src/gpu/knearest.cpp, nvrtc-compiled at run time)",
+            "ours_same_config": {"value": n / (ours_ms / 1000.0), "ms_per_step": ours_ms,
+                                 "mode": "learned"}}
 
 
 def run_reference(args):
@@ -363,6 +483,10 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(w, args.cpu_seconds)
+    gpulite = None
+    if rank == 0 and world == 1 and not args.no_gpulite:
+        assert L.lc_gpu_set_mode(ws, best_mode) == 0
+        gpulite = gpulite_leg(args, L, ws, x, n)
 
     names = ["pairs", "inserts", "replays", "shells", "pruned", "reranks", "prop_under",
              "prop_over", "prop_exact", "revisited", "fallback"]
@@ -379,7 +503,7 @@ def run_ours(args):
                       "tpp_source": "forced" if args.tpp else "autotuned",
                       "parallelism": f"replicas x{world}",
                       "l2": "flushed between timed steps (256 MB write)"},
-           "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+           "roofline": roofline, "cpu_baseline": cpu, "gpulite_baseline": gpulite, "e2e": e2e,
            "gpu_launches": launches_per_step * args.steps, "clocks": sampler.summary(),
            "plain_fp64": {"value": plain_value, "unit": "sources/s",
                           "walk_ms": statistics.mean(plain_walk), "tpp": plain_cnt[-1]},
@@ -527,7 +651,9 @@ def run_c3(args):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.gpulite_child:
+        gpulite_child(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "c3":
         run_c3(args)

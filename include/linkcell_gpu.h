@@ -86,7 +86,8 @@ int lc_gpu_memcpy(void *dst, const void *src, size_t bytes, int kind);
  * reference's exact results; every mode returns identical indices.
  */
 
-/* Walk selection. */
+/* Walk selection. Every mode gives the same rows; the default is
+ * LC_GPU_MODE_LEARNED (LINKCELL_MODE overrides it for new workspaces). */
 #define LC_GPU_MODE_PLAIN_F64 0 /* shell-by-shell FP64 walk */
 #define LC_GPU_MODE_FAST_F32 1  /* FP32 candidates, FP64 rerank of the boundary band */
 #define LC_GPU_MODE_LEARNED 2   /* FP32 walk that opens a learned shell proposal at once */
