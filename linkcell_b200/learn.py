@@ -195,7 +195,7 @@ def main():
     ap.add_argument("--n", type=int, default=100_000)
     ap.add_argument("--rows-per-run", type=int, default=2000)
     ap.add_argument("--epochs", type=int, default=12)
-    ap.add_argument("--tau", type=float, default=0.9)
+    ap.add_argument("--tau", type=float, default=0.95)
     ap.add_argument("--out", default=MODEL_PATH)
     a = ap.parse_args()
     X, y = collect(a.runs, a.n, a.rows_per_run)
