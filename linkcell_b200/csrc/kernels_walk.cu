@@ -1932,18 +1932,101 @@ cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t
 }
 
 namespace {
-__global__ void k_source_order(BatchBuffers b, int *__restrict__ order) {
+constexpr int kPartBlock = 256, kPartItems = 8;  // a block partitions 2048 sorted positions
+
+// Row range of sorted position p: its output row (point units) against the cuts.
+__device__ __forceinline__ int range_of(const BatchBuffers &b, const RowCuts &rc, long long p) {
+  const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
+  const long long row = b.frames[f].pt_base + b.sidx[p];
+  int r = 0;
+#pragma unroll
+  for (int c = 1; c < kMaxRowRanges; ++c) r += (c < rc.nr && row >= rc.cut[c]) ? 1 : 0;
+  return r;
+}
+
+// Per block and range: how many of the block's sorted positions fall in the
+// range (range-major, so that one scan gives every block's stable offsets).
+__global__ void __launch_bounds__(kPartBlock)
+    k_part_count(BatchBuffers b, RowCuts rc, uint32_t *__restrict__ cnt, int nblk) {
+  __shared__ uint32_t s_cnt[kMaxRowRanges];
+  if (threadIdx.x < kMaxRowRanges) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
   const long long total = b.off[b.ncells];
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < total;
-       p += (long long)gridDim.x * blockDim.x) {
-    const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
-    order[b.frames[f].pt_base + b.sidx[p]] = int(p);
+  const long long base = (long long)blockIdx.x * kPartBlock * kPartItems;
+#pragma unroll
+  for (int i = 0; i < kPartItems; ++i) {
+    const long long p = base + i * kPartBlock + threadIdx.x;
+    if (p < total) atomicAdd(&s_cnt[range_of(b, rc, p)], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < rc.nr) cnt[(long long)threadIdx.x * nblk + blockIdx.x] = s_cnt[threadIdx.x];
+}
+
+// Stable scatter: positions in ascending order within each range.
+__global__ void __launch_bounds__(kPartBlock)
+    k_part_scatter(BatchBuffers b, RowCuts rc, const uint32_t *__restrict__ off, int nblk,
+                   int *__restrict__ order) {
+  constexpr int kWarps = kPartBlock / 32;
+  __shared__ uint32_t s_run[kMaxRowRanges];
+  __shared__ uint32_t s_w[kWarps][kMaxRowRanges];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x < kMaxRowRanges) s_run[threadIdx.x] = 0;
+  const long long total = b.off[b.ncells];
+  const long long base = (long long)blockIdx.x * kPartBlock * kPartItems;
+  unsigned lt;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+  for (int i = 0; i < kPartItems; ++i) {
+    const long long p = base + i * kPartBlock + threadIdx.x;
+    const int r = p < total ? range_of(b, rc, p) : -1;
+    int rank = 0;
+    for (int c = 0; c < rc.nr; ++c) {
+      const unsigned m = __ballot_sync(0xffffffffu, r == c);
+      if (r == c) rank = __popc(m & lt);
+      if (lane == 0) s_w[warp][c] = __popc(m);
+    }
+    __syncthreads();
+    if (r >= 0) {
+      uint32_t pos = off[(long long)r * nblk + blockIdx.x] + s_run[r] + uint32_t(rank);
+      for (int w = 0; w < warp; ++w) pos += s_w[w][r];
+      order[pos] = int(p);
+    }
+    __syncthreads();
+    if (threadIdx.x < rc.nr) {
+      uint32_t add = 0;
+      for (int w = 0; w < kWarps; ++w) add += s_w[w][threadIdx.x];
+      s_run[threadIdx.x] += add;
+    }
+    __syncthreads();
   }
 }
 }  // namespace
 
-cudaError_t launch_source_order(const BatchBuffers &b, int *order, cudaStream_t s) {
-  k_source_order<<<sm_count() * 8, 256, 0, s>>>(b, order);
+long long range_partition_blocks(long long sources) {
+  const long long per = (long long)kPartBlock * kPartItems;
+  return std::max<long long>(1, (sources + per - 1) / per);
+}
+
+cudaError_t launch_range_partition(const BatchBuffers &b, const RowCuts &cuts, uint32_t *cnt,
+                                   uint32_t *off, unsigned long long *tile_state,
+                                   uint32_t *tile_counter, int *order, cudaStream_t s) {
+  // b.npts bounds the active sources: the grid covers them all
+  const int nblk = int(range_partition_blocks(b.npts));
+  k_part_count<<<nblk, kPartBlock, 0, s>>>(b, cuts, cnt, nblk);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  BatchBuffers sb;  // the cell-count scan over the range-major block counts
+  sb.count = cnt;
+  sb.off = off;
+  sb.ncells = (long long)cuts.nr * nblk;
+  sb.tile_state = tile_state;
+  sb.tile_counter = tile_counter;
+  sb.status = b.status;
+  if ((e = cudaMemsetAsync(tile_state, 0, size_t(scan_tiles(sb.ncells)) * sizeof(unsigned long long),
+                           s)) != cudaSuccess ||
+      (e = cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), s)) != cudaSuccess)
+    return e;
+  if ((e = launch_scan(sb, s)) != cudaSuccess) return e;
+  k_part_scatter<<<nblk, kPartBlock, 0, s>>>(b, cuts, off, nblk, order);
   return cudaGetLastError();
 }
 

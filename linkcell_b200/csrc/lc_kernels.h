@@ -53,17 +53,18 @@ struct BatchBuffers {
   const uint32_t *shell_table = nullptr;  // near-first shell offsets, shells 1..shell_rmax
   int shell_rmax = 0;
   // optional source order: when set, the walk visits sorted positions
-  // src_order[src_begin .. src_end) (-1 entries skipped) instead of all of them
+  // src_order[*src_lo .. *src_hi) instead of all of them (the bounds are
+  // device values, written by the kernels that built the order)
   const int *src_order = nullptr;
-  long long src_begin = 0, src_end = 0;
+  const uint32_t *src_lo = nullptr, *src_hi = nullptr;
 };
 
 // Sources a walk launch visits, and the sorted position of the q-th.
 __device__ __forceinline__ long long walk_sources(const BatchBuffers &b) {
-  return b.src_order ? b.src_end - b.src_begin : (long long)b.off[b.ncells];
+  return b.src_order ? (long long)*b.src_hi - (long long)*b.src_lo : (long long)b.off[b.ncells];
 }
 __device__ __forceinline__ long long walk_source_at(const BatchBuffers &b, long long q) {
-  return b.src_order ? (long long)b.src_order[b.src_begin + q] : q;
+  return b.src_order ? (long long)b.src_order[*b.src_lo + q] : q;
 }
 
 // Walk statistics accumulated on the device (counters[...]).
@@ -121,7 +122,22 @@ cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t
 cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s);
 // order[pt_base + index] = sorted position of each active source (order is
 // pre-filled with -1 for masked points).
-cudaError_t launch_source_order(const BatchBuffers &b, int *order, cudaStream_t s);
+// Output-row ranges of a host-pointer search: row cuts cut[0] = 0 <
+// cut[1] < ... < cut[nr] (point units).
+constexpr int kMaxRowRanges = 8;
+struct RowCuts {
+  long long cut[kMaxRowRanges + 1];
+  int nr;
+};
+// Sorted positions partitioned by the row range of their source, cell order
+// kept inside each range: order[off[r * nblk] .. off[(r + 1) * nblk]) are
+// range r's. cnt and off (nr * nblk + 1 entries) are scratch of
+// range_partition_blocks(); tile_state (scan tiles of nr * nblk) and
+// tile_counter serve the scan.
+long long range_partition_blocks(long long sources);
+cudaError_t launch_range_partition(const BatchBuffers &b, const RowCuts &cuts, uint32_t *cnt,
+                                   uint32_t *off, unsigned long long *tile_state,
+                                   uint32_t *tile_counter, int *order, cudaStream_t s);
 // CSR of the entries within a cutoff of n x k rows (sorted ascending, -1 /
 // NaN padded): counts and row_off are rows + 1 scratch words, tile_state /
 // tile_counter the scan's scratch; row_ptr gets rows + 1 offsets, col /

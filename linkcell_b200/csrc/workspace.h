@@ -179,7 +179,7 @@ class WorkspaceImpl {
   // while the next range is searched, 2 = rows written to mapped host memory,
   // 0 = one copy at the end (LINKCELL_HOST_ROWS)
   int host_rows_ = 1;
-  static constexpr int kRowRanges = 8;
+  static constexpr long long kMinRangeRows = 16384;  // shortest row range
   struct Pipe {
     bool on = false, done = false;
     int *host_nn = nullptr;
@@ -189,7 +189,9 @@ class WorkspaceImpl {
   Pipe pipe_;
   Buf<int> order_;
   cudaStream_t copy_stream_ = nullptr;
-  cudaEvent_t range_ev_[kRowRanges + 1] = {};
+  cudaEvent_t range_ev_[kMaxRowRanges + 1] = {};
+  Buf<uint32_t> part_cnt_, part_off_;
+  Buf<unsigned long long> part_tiles_;
   Code walk_in_row_ranges(BatchBuffers &b, const WalkLaunch &wl, cudaStream_t s, bool timed,
                           std::string &detail);
   Buf<uint32_t> csr_counts_, csr_off_;
