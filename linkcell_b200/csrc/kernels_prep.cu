@@ -238,12 +238,12 @@ __global__ void k_zero_live(uint32_t *__restrict__ count, unsigned long long *__
     tile_state[t] = 0ull;
 }
 
-// Arrival slots: tmp[off[c] + arank[g]] = g. The output rows of masked
+// Arrival slots: tmp[off[c] + arank[g]] = (g, c). The output rows of masked
 // points are filled here with -1 / NaN (src/knearest.rs:293-296).
 __global__ void __launch_bounds__(256)
     k_place_slots(const FrameDesc *__restrict__ frames, int nframes,
                   const uint32_t *__restrict__ cell_of, const uint32_t *__restrict__ arank,
-                  const uint32_t *__restrict__ off, uint32_t *__restrict__ tmp, long long npts,
+                  const uint32_t *__restrict__ off, uint2 *__restrict__ tmp, long long npts,
                   long long ncells, int *__restrict__ out_nn, double *__restrict__ out_d2,
                   int *__restrict__ status) {
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -268,23 +268,24 @@ __global__ void __launch_bounds__(256)
       atomicOr(status, kStatusBadIndex);
       continue;
     }
-    tmp[pos] = uint32_t(g);
+    tmp[pos] = make_uint2(uint32_t(g), c);
   }
 }
 
 // Stable placement, one thread per sorted slot: the point g arriving at
 // slot pos of cell c lands at off[c] + (number of points of c with a
 // smaller id), so the order inside a cell is by point id (the reference
-// bins points in id order). The reads of g's coordinates are gathers; the
-// writes of the sorted SoA records stay within the cell's few slots, so a
-// warp's stores remain coalesced. Two slots per thread and the coordinate
-// gathers issued first keep more loads in flight (the kernel is bound by the
-// latency of its dependent gathers).
+// bins points in id order). The slot holds the cell next to the point id,
+// so the only gather by id is g's coordinates; the writes of the sorted SoA
+// records stay within the cell's few slots, so a warp's stores remain
+// coalesced. Two slots per thread and the coordinate gathers issued first
+// keep more loads in flight (the kernel is bound by the latency of its
+// dependent gathers).
 __global__ void __launch_bounds__(256, 3)
     k_place_records(const double *__restrict__ xyz, const FrameDesc *__restrict__ frames,
                     int nframes, long long npts, long long ncells,
-                    const uint32_t *__restrict__ cell_of, const uint32_t *__restrict__ off,
-                    const uint32_t *__restrict__ tmp, double *__restrict__ sx,
+                    const uint32_t *__restrict__ off, const uint2 *__restrict__ tmp,
+                    double *__restrict__ sx,
                     double *__restrict__ sy, double *__restrict__ sz, int *__restrict__ sidx,
                     uint32_t *__restrict__ scell, float4 *__restrict__ rec,
                     int *__restrict__ status) {
@@ -299,7 +300,9 @@ __global__ void __launch_bounds__(256, 3)
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
       live[u] = pos[u] < total;
-      g[u] = live[u] ? tmp[pos[u]] : 0u;
+      const uint2 gc = live[u] ? tmp[pos[u]] : make_uint2(0u, kInactive);
+      g[u] = gc.x;
+      c[u] = gc.y;
     }
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
@@ -308,7 +311,7 @@ __global__ void __launch_bounds__(256, 3)
       r[u][0] = ok ? xyz[b3 + 0] : 0.0;
       r[u][1] = ok ? xyz[b3 + 1] : 0.0;
       r[u][2] = ok ? xyz[b3 + 2] : 0.0;
-      c[u] = ok ? cell_of[g[u]] : kInactive;
+      if (!ok) c[u] = kInactive;
     }
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
@@ -319,7 +322,7 @@ __global__ void __launch_bounds__(256, 3)
       }
       const uint32_t a = off[c[u]], e = off[c[u] + 1];
       uint32_t rk = 0;
-      for (uint32_t q = a; q < e; ++q) rk += tmp[q] < g[u] ? 1u : 0u;
+      for (uint32_t q = a; q < e; ++q) rk += tmp[q].x < g[u] ? 1u : 0u;
       const long long dst = (long long)a + rk;
       if (dst >= (long long)e) {
         atomicOr(status, kStatusBadIndex);
@@ -407,8 +410,8 @@ cudaError_t launch_place(const BatchBuffers &b, cudaStream_t s) {
                                   b.ncells, b.out_nn, b.out_d2, b.status);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_place_records<<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.npts, b.ncells, b.cell_of, b.off,
-                                    b.tmp, b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec, b.status);
+  k_place_records<<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.npts, b.ncells, b.off, b.tmp,
+                                    b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec, b.status);
   return cudaGetLastError();
 }
 

@@ -23,7 +23,7 @@ struct BatchBuffers {
   const long long *live_cells = nullptr;
   uint32_t *cell_of = nullptr;   // P: batch cell id or kInactive
   uint32_t *arank = nullptr;     // P: arrival rank inside the cell (atomics)
-  uint32_t *tmp = nullptr;       // P: point id at its arrival slot
+  uint2 *tmp = nullptr;          // P: (point id, cell) at the point's arrival slot
   uint32_t *count = nullptr;     // C
   uint32_t *off = nullptr;       // C+1: exclusive scan of count
   unsigned long long *tile_state = nullptr;  // scan tiles
