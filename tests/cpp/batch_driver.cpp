@@ -7,10 +7,14 @@
 //   per frame: int64 n, int64 k, int64 mask_offset, double cell[12] (a, b, c
 //   rows, origin), double cell_hint
 //   double xyz[3 * sum n], int32 mask[mask_len]
-// Output: int32 rows[sum n k], double dist2[sum n k].
+// Output: int32 rows[sum n k], double dist2[sum n k], then for frame 0 alone
+// three more (rows, dist2) pairs of n0 k0 entries each: through
+// Workspace::knearest_into, Workspace::knearest_into_many_dcell (the cell
+// as 12 device doubles) and the host API linkcell::knearest.
 // It also checks that a wrong out_len throws linkcell::Error before any work.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -102,6 +106,44 @@ int main(int argc, char **argv) {
         if (!o || std::fwrite(out.data(), sizeof(int), rows, o) != rows ||
             std::fwrite(d2.data(), sizeof(double), rows, o) != rows)
           rc = 2;
+        // frame 0 through the single-frame entry points
+        const auto &f0 = frames[0];
+        const std::size_t r0 = f0.n * f0.k;
+        const int *dm0 = f0.mask_offset >= 0 ? d_mask + f0.mask_offset : nullptr;
+        const int *hm0 = f0.mask_offset >= 0 ? mask.data() + f0.mask_offset : nullptr;
+        const lc_cell raw = f0.cell.raw();
+        const double cell12[12] = {raw.ax, raw.ay, raw.az, raw.bx, raw.by, raw.bz,
+                                   raw.cx, raw.cy, raw.cz, raw.ox, raw.oy, raw.oz};
+        double *d_cell = nullptr;
+        std::vector<int> o0(r0);
+        std::vector<double> e0(r0);
+        auto emit = [&]() {
+          if (!o || std::fwrite(o0.data(), sizeof(int), r0, o) != r0 ||
+              std::fwrite(e0.data(), sizeof(double), r0, o) != r0)
+            rc = 2;
+        };
+        auto fetch = [&]() {
+          return check(cudaMemcpy(o0.data(), d_out, r0 * sizeof(int), cudaMemcpyDeviceToHost),
+                       "copy out") &&
+                 check(cudaMemcpy(e0.data(), d_d2, r0 * sizeof(double), cudaMemcpyDeviceToHost),
+                       "copy d2");
+        };
+        ws.knearest_into(d_xyz, f0.n, f0.cell, f0.k, d_out, r0, dm0, f0.cell_hint, d_d2);
+        if (fetch()) emit(); else rc = 3;
+        if (check(cudaMalloc(&d_cell, sizeof(cell12)), "malloc cell") &&
+            check(cudaMemcpy(d_cell, cell12, sizeof(cell12), cudaMemcpyHostToDevice), "copy cell")) {
+          ws.knearest_into_many_dcell(d_xyz, f0.n, 1, d_cell, 12, f0.k, d_out, r0, dm0,
+                                      f0.cell_hint, true, d_d2);
+          if (fetch()) emit(); else rc = 3;
+        } else {
+          rc = 3;
+        }
+        cudaFree(d_cell);
+        const linkcell::Neighbours nb = linkcell::knearest(xyz.data(), f0.n, f0.cell, f0.k, hm0,
+                                                           f0.cell_hint);
+        std::copy(nb.begin(), nb.end(), o0.begin());
+        std::copy(nb.distances(), nb.distances() + r0, e0.begin());
+        emit();
         if (o) std::fclose(o);
       }
     }

@@ -1,11 +1,13 @@
-"""The C++ class entry for per-frame batches,
-linkcell::gpu::Workspace::knearest_into_batch, through a small C++ program
-(tests/cpp/batch_driver.cpp) built against include/linkcell_gpu.hpp and the
-in-tree library.
+"""The C++ entry points through a small C++ program
+(tests/cpp/batch_driver.cpp) built against include/linkcell_gpu.hpp,
+include/linkcell.hpp and the in-tree library.
 
-The CPU test checks that the header compiles and the program links; the GPU
+The CPU test checks that the headers compile and the program links. The GPU
 test runs a heterogeneous batch (own cell, n, k, hint and mask per frame)
-through it and compares every frame with the oracle."""
+through linkcell::gpu::Workspace::knearest_into_batch. It then runs the first
+frame through Workspace::knearest_into, Workspace::knearest_into_many_dcell
+and the host linkcell::knearest, and compares every result with the
+oracle."""
 
 from __future__ import annotations
 
@@ -77,10 +79,11 @@ def test_cpp_batch_matches_oracle(gpu, oracle_mod, tmp_path):
     r = subprocess.run([exe, str(src), str(dst)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     total = sum(len(f["xyz"]) * f["k"] for f in frames)
+    r0 = len(frames[0]["xyz"]) * frames[0]["k"]
     raw = np.fromfile(dst, dtype=np.uint8)
-    assert raw.size == total * 12
+    assert raw.size == total * 12 + 3 * r0 * 12
     nn = raw[:total * 4].view(np.int32)
-    d2 = raw[total * 4:].view(np.float64)
+    d2 = raw[total * 4:total * 12].view(np.float64)
     off = 0
     for i, f in enumerate(frames):
         n, k = len(f["xyz"]), f["k"]
@@ -89,3 +92,15 @@ def test_cpp_batch_matches_oracle(gpu, oracle_mod, tmp_path):
         got = (nn[off:off + n * k].reshape(n, k), d2[off:off + n * k].reshape(n, k))
         assert_same(got, want, f"frame {i}")
         off += n * k
+    # frame 0 through Workspace::knearest_into, knearest_into_many_dcell and
+    # the host linkcell::knearest
+    f = frames[0]
+    n, k = len(f["xyz"]), f["k"]
+    want = oracle_mod.knearest(f["xyz"], f["cell"], k, mask=f.get("mask"),
+                               cell_hint=f.get("cell_hint", 0.0))
+    pos = total * 12
+    for name in ("knearest_into", "knearest_into_many_dcell", "linkcell::knearest"):
+        got = (raw[pos:pos + 4 * r0].view(np.int32).reshape(n, k),
+               raw[pos + 4 * r0:pos + 12 * r0].view(np.float64).reshape(n, k))
+        assert_same(got, want, name)
+        pos += 12 * r0
