@@ -44,9 +44,9 @@ cudaError_t mlp_grad(const float *params, const float *X, const int *y, int B, M
                      float *grad, float *loss, cudaStream_t s);
 cudaError_t mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr,
                      cudaStream_t s);
-// Proposed shell per occupied cell (tensor-core inference over 16-cell row
-// tiles, the first layer as a 5x5x5 convolution of the occupancy grid),
-// then per sorted source.
+// Proposed shell per cell (tcgen05 inference over 128-cell tiles of four
+// 32-cell row segments, the first layer as a 5x5x5 convolution of the
+// occupancy grid), then per sorted source.
 cudaError_t mlp_propose(const float *params, const BatchBuffers &b, int8_t *cell_prop,
                         int8_t *source_prop, float tau, cudaStream_t s);
 // Training rows from a logged search: features of the cell of every
