@@ -595,8 +595,8 @@ Code WorkspaceImpl::run_host(std::vector<FrameDesc> &frames, const double *xyz, 
   // Output rows land in a random order, so a finished search cannot be
   // copied back in pieces while it runs. With page-locked output buffers
   // the search is cut into row ranges instead: the walk visits the sources
-  // of one range of output rows at a time (in the order of their rows) and
-  // a copy engine brings each finished range back while the next one is
+  // of one range of output rows at a time (in cell order inside the range)
+  // and a copy engine brings each finished range back while the next one is
   // searched (host_rows 1, the default). host_rows 2 has the kernels write
   // the rows straight into the mapped host buffers; pageable buffers (or
   // host_rows 0) take one copy back at the end.
