@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(256, 3)
       const double c0 = fr.h[0] * f0 + fr.h[3] * f1 + fr.h[6] * f2 + fr.origin[0];
       const double c1 = fr.h[1] * f0 + fr.h[4] * f1 + fr.h[7] * f2 + fr.origin[1];
       const double c2 = fr.h[2] * f0 + fr.h[5] * f1 + fr.h[8] * f2 + fr.origin[2];
-      rec[dst] = make_float4(float(q0 - c0), float(q1 - c1), float(q2 - c2), __int_as_float(i));
+      rec[dst] = make_float4(float(q0 - c0), float(q1 - c1), float(q2 - c2), __int_as_float(cx));
     }
   }
 }

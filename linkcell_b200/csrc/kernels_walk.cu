@@ -382,11 +382,10 @@ __device__ void walk_source(const BatchBuffers &b, long long p, double *hd, int 
             ++cnt.v[kCntPairs];
             if (d32 > thr) continue;  // exact distance > theta: rejected
             ++cnt.v[kCntRerank];
-            j = __float_as_int(q.w);
           } else {
             ++cnt.v[kCntPairs];
-            j = -1;
           }
+          j = -1;
           if (!have_shift) {
             lattice_shift(fr, wa, wb, wc, shx, shy, shz);
             have_shift = true;
@@ -817,10 +816,8 @@ __device__ void team_source(const BatchBuffers &b, long long p, int lane, LocalC
               const float ez = (q.z - plz) + oDz;
               const float d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
               pass = !(d32 > thr);
-              j = __float_as_int(q.w);
-            } else {
-              j = b.sidx[t];
             }
+            if (pass) j = b.sidx[t];
           }
           const unsigned pm = __ballot_sync(kFull, pass);
           if (pm == 0) continue;
@@ -1000,7 +997,7 @@ struct __align__(16) SelRow {  // one non-empty row of the cube
   int excl;                    // first candidate position of the row
   int startA, lenA;            // sorted range of the cells inside the box
   int startB;                  // sorted range of the cells wrapped in x, minus lenA
-  int xoffA, xoffB;            // dx = scell + xoff (A: no x wrap, B: wrapped)
+  int xoffA, xoffB;            // dx = candidate cell x + xoff (A: no x wrap, B: wrapped)
   int metaA, metaB;            // wrap counts of a candidate (A / B) in SelShared::m layout
   float Dx, Dy, Dz;            // dy e_b + dz e_c (FP32)
   int syz;                     // max(1, |dy|, |dz|)
@@ -1150,8 +1147,8 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
         }
         rw.lenA = lenA;
         rw.startB = sB - lenA;
-        rw.xoffA = -rowbase - ix;
-        rw.xoffB = -rowbase - ix + wrapB * nx;
+        rw.xoffA = -ix;
+        rw.xoffB = -ix + wrapB * nx;
         const int wbc = ((wb + 1) << 10) | ((wc + 1) << 12);
         rw.metaA = (1 << 8) | wbc;
         rw.metaB = ((wrapB + 1) << 8) | wbc;
@@ -1218,12 +1215,8 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
         }
       }
       float4 q[2];
-      int sc[2];
 #pragma unroll
-      for (int w = 0; w < 2; ++w) {
-        q[w] = live[w] ? b.rec[t[w]] : make_float4(0.f, 0.f, 0.f, 0.f);
-        sc[w] = live[w] ? int(b.scell[t[w]]) : 0;
-      }
+      for (int w = 0; w < 2; ++w) q[w] = live[w] ? b.rec[t[w]] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
       for (int w = 0; w < 2; ++w) {
         bool keep = false;
@@ -1231,7 +1224,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
         uint32_t mm = 0;
         if (live[w]) {
           const SelRow &R = sh.rows[owner[w]];
-          const int dx = sc[w] + xo[w];
+          const int dx = __float_as_int(q[w].w) + xo[w];  // the candidate cell's x index
           const float fdx = float(dx);
           const float ex = (q[w].x - plx) + fmaf(fdx, ev0, R.Dx);
           const float ey = (q[w].y - ply) + fmaf(fdx, ev1, R.Dy);

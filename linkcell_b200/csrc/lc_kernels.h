@@ -34,7 +34,7 @@ struct BatchBuffers {
   double *sx = nullptr, *sy = nullptr, *sz = nullptr;  // folded FP64 SoA
   int *sidx = nullptr;           // index of the point inside its frame
   uint32_t *scell = nullptr;     // cell id inside the frame
-  float4 *rec = nullptr;         // FP32 offset from the cell corner, idx bits in w
+  float4 *rec = nullptr;         // FP32 offset from the cell corner; w: the cell's x index (int bits)
   // outputs (caller's)
   int *out_nn = nullptr;
   double *out_d2 = nullptr;
