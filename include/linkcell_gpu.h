@@ -160,8 +160,13 @@ int lc_gpu_set_stream(lc_gpu_workspace *ws, void *stream);
 /* Walk counters of the last search issued with wait != 0: pairs evaluated,
  * heap insertions, exact replays, shells, pruned cells, FP64 reranks,
  * proposal under / over / exact, revisited shells. device_ms is the device
- * time of the whole search. Returns the number of counters written. */
+ * time of the whole search. Returns the number of counters written. The
+ * learned mode's warp walk counts only with lc_gpu_set_stats on. */
 int lc_gpu_stats(lc_gpu_workspace *ws, long long *counters, int n_counters, double *device_ms);
+
+/* Extension: counting in the learned mode's warp-per-source walk (off by
+ * default: the counters cost about 3 % of that walk). */
+int lc_gpu_set_stats(lc_gpu_workspace *ws, int on);
 
 /* Device time of the last search's phases, from CUDA events on the
  * workspace stream: fold + bin + scan + placement, the walk kernel, and the

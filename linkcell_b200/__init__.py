@@ -160,6 +160,11 @@ class Workspace:
         h = int(getattr(stream, "cuda_stream", stream))
         self._L.lc_gpu_set_stream(self._ws, ctypes.c_void_p(h if h else 1))
 
+    def set_stats(self, on: bool = True) -> None:
+        """Count walk statistics in the learned mode's warp walk (off by
+        default; they cost about 3 % of that walk)."""
+        self._L.lc_gpu_set_stats(self._ws, 1 if on else 0)
+
     def stats(self) -> dict:
         buf = (ctypes.c_longlong * 16)()
         ms = ctypes.c_double()

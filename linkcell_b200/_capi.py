@@ -35,6 +35,7 @@ EXPORTS = (
     "lc_gpu_wait", "lc_gpu_alloc", "lc_gpu_free", "lc_gpu_fill_i32", "lc_gpu_memcpy",
     "lc_gpu_set_mode", "lc_gpu_get_mode", "lc_gpu_set_proposal", "lc_gpu_set_tpp",
     "lc_gpu_get_tpp", "lc_gpu_set_graph", "lc_gpu_graph_captures", "lc_gpu_set_stream", "lc_gpu_stats",
+    "lc_gpu_set_stats",
     "lc_gpu_phase_times", "lc_gpu_phase_times4", "lc_gpu_neighbors_within", "lc_gpu_set_model", "lc_gpu_log_shells", "lc_gpu_training_rows",
     "lc_gpu_proposals",
     "lc_gpu_mlp_params", "lc_gpu_mlp_scratch_floats", "lc_gpu_mlp_forward", "lc_gpu_mlp_grad",
@@ -90,6 +91,7 @@ def load():
     L.lc_gpu_get_tpp.argtypes = [vp]
     L.lc_gpu_set_graph.argtypes = [vp, i]
     L.lc_gpu_graph_captures.argtypes = [vp]
+    L.lc_gpu_set_stats.argtypes = [vp, i]
     L.lc_gpu_set_stream.argtypes = [vp, vp]
     L.lc_gpu_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), i, dp]
     L.lc_gpu_phase_times.argtypes = [vp, dp, dp, dp]

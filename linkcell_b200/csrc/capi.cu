@@ -573,6 +573,12 @@ int lc_gpu_set_graph(lc_gpu_workspace *ws, int on) {
 
 int lc_gpu_graph_captures(lc_gpu_workspace *ws) { return ws ? ws->ws.graph_captures : -1; }
 
+int lc_gpu_set_stats(lc_gpu_workspace *ws, int on) {
+  if (!ws) return gpu_fail(Code::NullPointer);
+  ws->ws.opts.stats = on != 0;
+  return 0;
+}
+
 int lc_gpu_set_model(lc_gpu_workspace *ws, const float *params, size_t n_params, float tau) {
   if (!ws || !params) return gpu_fail(Code::NullPointer);
   if (!(tau > 0.f && tau <= 1.f)) return gpu_fail_msg("tau must lie in (0, 1]");

@@ -1045,8 +1045,9 @@ __device__ __forceinline__ uint32_t quot(uint32_t x, uint32_t n, double inv) {
   return q;
 }
 
-// One source; false: the source must go to the literal replay.
-template <int SN>
+// One source; false: the source must go to the literal replay. STATS: count
+// the walk statistics (lc_gpu_set_stats; they cost about 3 % of the walk).
+template <int SN, bool STATS>
 __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelShared<SN> &sh) {
   const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
   const FrameDesc &fr = b.frames[f];
@@ -1162,7 +1163,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
       }
     }
     const int len = lenA + lenB;
-    {
+    if (STATS) {
       const unsigned pr = __reduce_add_sync(kFull, unsigned(pruned));
       if (lane == 0) sh.wc[kWcPruned] += pr;
     }
@@ -1176,7 +1177,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
     }
     const int tot = __shfl_sync(kFull, incl, 31);
     const int excl = incl - len;
-    if (lane == 0) sh.wc[kWcPairs] += unsigned(tot);  // the source itself included
+    if (STATS && lane == 0) sh.wc[kWcPairs] += unsigned(tot);  // the source itself included
     __syncwarp();
     if (len > 0) {
       rw.excl = excl;
@@ -1269,7 +1270,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
       bR = 1;
     } else if (rc - rr < eps_r || rr - (rc - 1.f) < eps_r) {
       dex = exact(i);
-      atomicAdd(&sh.wc[kWcRerank], 1ull);
+      if (STATS) atomicAdd(&sh.wc[kWcRerank], 1ull);
       int R = max(1, int(rc) - 1);
       while (R <= Rp && !(dex <= stop_bound(R, cell_min))) ++R;
       bR = R;
@@ -1282,7 +1283,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
       } else if (!(d32 > fr.sel_rho_hi[Rp])) {
         if (dex < 0.0) {
           dex = exact(i);
-          atomicAdd(&sh.wc[kWcRerank], 1ull);
+          if (STATS) atomicAdd(&sh.wc[kWcRerank], 1ull);
         }
         in_rho += dex <= fr.sel_rho2[Rp] ? 1u : 0u;
       }
@@ -1314,17 +1315,17 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   if (Rs == 0 && partial && __reduce_add_sync(kFull, in_rho) >= unsigned(k)) Rs = Rp;
   if (Rs != 0) break;
   if (!partial) {
-    if (lane == 0) ++sh.wc[kWcUnder];
+    if (STATS && lane == 0) ++sh.wc[kWcUnder];
     return false;
   }
-  if (lane == 0) ++sh.wc[kWcRegather];
+  if (STATS && lane == 0) ++sh.wc[kWcRegather];
   __syncwarp();
   }  // gathers
   if (Rs < Rp)
-    { if (lane == 0) ++sh.wc[kWcOver]; }
+    { if (STATS && lane == 0) ++sh.wc[kWcOver]; }
   else
-    { if (lane == 0) ++sh.wc[kWcExact]; }
-  if (lane == 0) sh.wc[kWcShells] += unsigned(Rs);
+    { if (STATS && lane == 0) ++sh.wc[kWcExact]; }
+  if (STATS && lane == 0) sh.wc[kWcShells] += unsigned(Rs);
 
   // 3. select: two-level histogram over candidates of shells <= R* within
   // B(R*) (within rho2 when the first gather settled R* = R_p)
@@ -1400,7 +1401,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   }
   __syncwarp();
   if (nS < k) return false;  // cannot happen: T bounds k candidates
-  if (lane == 0) sh.wc[kWcRerank] += unsigned(nS);
+  if (STATS && lane == 0) sh.wc[kWcRerank] += unsigned(nS);
   double ed[SN];
   int ej[SN];
 #pragma unroll
@@ -1445,7 +1446,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   __syncwarp();
   // a tie across the k-th slot: the k-th and (k+1)-th values are equal
   if (nS > k && sh.hmax[0] == sh.hmax[2] && sh.hmax[1] == sh.hmax[3]) {
-    if (lane == 0) ++sh.wc[kWcReplays];
+    if (STATS && lane == 0) ++sh.wc[kWcReplays];
     return false;
   }
 #pragma unroll
@@ -1456,11 +1457,11 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
     }
   }
   if (b.stop_log && lane == 0) b.stop_log[p] = int8_t(Rs);
-  if (lane == 0) sh.wc[kWcInserts] += unsigned(k);
+  if (STATS && lane == 0) sh.wc[kWcInserts] += unsigned(k);
   return true;
 }
 
-template <int SN>
+template <int SN, bool STATS>
 __global__ void __launch_bounds__(kSelWarps * 32, SN == 2 ? 3 : 2) k_select_walk(BatchBuffers b) {
   extern __shared__ __align__(16) unsigned char sel_smem[];
   SelShared<SN> &sh = reinterpret_cast<SelShared<SN> *>(sel_smem)[threadIdx.x >> 5];
@@ -1478,15 +1479,15 @@ __global__ void __launch_bounds__(kSelWarps * 32, SN == 2 ? 3 : 2) k_select_walk
       if ((long long)base + q >= total) break;
       const long long p = walk_source_at(b, (long long)base + q);
       if (p < 0) continue;
-      const unsigned long long tie = sh.wc[kWcReplays];
-      if (!select_source<SN>(b, p, lane, sh)) {
-        if (lane == 0 && sh.wc[kWcReplays] == tie) ++sh.wc[kWcFallback];
+      const unsigned long long tie = STATS ? sh.wc[kWcReplays] : 0ull;
+      if (!select_source<SN, STATS>(b, p, lane, sh)) {
+        if (STATS && lane == 0 && sh.wc[kWcReplays] == tie) ++sh.wc[kWcFallback];
         if (lane == 0) push_replay(b, p);
       }
       __syncwarp();
     }
   }
-  if (lane == 0) {
+  if (STATS && lane == 0) {
     unsigned long long *c = reinterpret_cast<unsigned long long *>(b.counters);
     atomicAdd(&c[kCntPairs], sh.wc[kWcPairs]);
     atomicAdd(&c[kCntPruned], sh.wc[kWcPruned]);
@@ -1504,18 +1505,24 @@ __global__ void __launch_bounds__(kSelWarps * 32, SN == 2 ? 3 : 2) k_select_walk
 
 int sm_count();
 
-template <int SN>
-cudaError_t launch_select(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
+template <int SN, bool STATS>
+cudaError_t launch_select_as(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
   const size_t smem = sizeof(SelShared<SN>) * kSelWarps;
-  cudaError_t e = cudaFuncSetAttribute(k_select_walk<SN>,
+  cudaError_t e = cudaFuncSetAttribute(k_select_walk<SN, STATS>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk<SN>, kSelWarps * 32, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk<SN, STATS>, kSelWarps * 32,
+                                                smem);
   if (per_sm < 1) per_sm = 1;
   const int grid = w.grid > 0 ? w.grid : sm_count() * per_sm;
-  k_select_walk<SN><<<grid, kSelWarps * 32, smem, s>>>(b);
+  k_select_walk<SN, STATS><<<grid, kSelWarps * 32, smem, s>>>(b);
   return cudaGetLastError();
+}
+
+template <int SN>
+cudaError_t launch_select(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
+  return w.stats ? launch_select_as<SN, true>(b, w, s) : launch_select_as<SN, false>(b, w, s);
 }
 
 // Warp-parallel literal replay of the reference heap for one source (finite

@@ -115,6 +115,7 @@ struct WalkLaunch {
   int grid = 0;
   int kmax = 32;
   int prune = 1;
+  bool stats = false;  // the learned select walk counts its statistics
   const int8_t *proposal = nullptr;  // per sorted source proposed shell (learned mode)
 };
 

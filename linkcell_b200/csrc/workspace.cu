@@ -311,6 +311,7 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   wl.mode = kmax > 256 ? int(kModeReplayAll) : opts.mode;
   wl.kmax = kmax;
   wl.prune = opts.prune;
+  wl.stats = opts.stats;
   const int kclass = kmax <= 32 ? 0 : (kmax <= 64 ? 1 : (kmax <= 128 ? 2 : 3));
   const int tkey = (wl.mode * 4 + kclass) * 2 + (nf > 1 ? 1 : 0);
   auto set_tpp = [&](int tpp) {
@@ -359,7 +360,8 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   } else if (opts.graph) {
     const GraphKey key{npts, ncells, nf, kmax, xyz, mask, out_nn, out_d2, wl.mode, wl.tpp,
                        wl.block, has_model_ ? 1 : 0, opts.fixed_proposal, opts.log_shells,
-                       dcell_.on ? dcell_.cell : nullptr, dcell_.on ? dcell_.cell_n : 0,
+                       opts.stats ? 1 : 0, dcell_.on ? dcell_.cell : nullptr,
+                       dcell_.on ? dcell_.cell_n : 0,
                        dcell_.on ? dcell_.hint : 0.0};
     if (!graph_exec_ || !(key == graph_key_)) {
       if (graph_exec_) cudaGraphExecDestroy(graph_exec_);

@@ -65,6 +65,7 @@ struct WalkOptions {
   bool tpp_forced = false; // tpp set explicitly (API or LINKCELL_TPP): no autotuning
   bool autotune = true;    // time the walk designs on the first batch of each kind
   bool graph = false;      // capture the launch sequence in a CUDA graph and replay it
+  bool stats = false;      // the learned select walk counts its statistics (lc_gpu_stats)
 };
 
 struct Stats {
@@ -146,7 +147,7 @@ class WorkspaceImpl {
     long long npts = -1, ncells = -1;
     int nf = 0, kmax = 0;
     const void *xyz = nullptr, *mask = nullptr, *nn = nullptr, *d2 = nullptr;
-    int mode = 0, tpp = 0, block = 0, model = 0, fixed = 0, log = 0;
+    int mode = 0, tpp = 0, block = 0, model = 0, fixed = 0, log = 0, stats = 0;
     const void *dcell = nullptr;  // device-planned batch: its cell and launch constants
     int cell_n = 0;
     double hint = 0.0;
@@ -154,6 +155,7 @@ class WorkspaceImpl {
       return npts == o.npts && ncells == o.ncells && nf == o.nf && kmax == o.kmax && xyz == o.xyz &&
              mask == o.mask && nn == o.nn && d2 == o.d2 && mode == o.mode && tpp == o.tpp &&
              block == o.block && model == o.model && fixed == o.fixed && log == o.log &&
+             stats == o.stats &&
              dcell == o.dcell && cell_n == o.cell_n && hint == o.hint;
     }
   };

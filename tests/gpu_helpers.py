@@ -64,6 +64,9 @@ class DeviceRunner:
     def set_proposal(self, shell):
         assert self.L.lc_gpu_set_proposal(self.ws, shell) == 0
 
+    def set_stats(self, on):
+        assert self.L.lc_gpu_set_stats(self.ws, 1 if on else 0) == 0
+
     def run(self, xyz, cell, k, mask=None, hint=0.0, n_frames=1, wait=1):
         torch = self.torch
         x = torch.as_tensor(np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3),

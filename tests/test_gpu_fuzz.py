@@ -78,6 +78,7 @@ def test_random_sweep(fuzz_runner, oracle_mod, block):
         r.set_mode(c["mode"])
         r.set_tpp(c["tpp"])
         r.set_proposal(c["shell"])
+        r.set_stats(seed % 2 == 1)  # both builds of the warp walk: counting and not
         got = r.run(c["xyz"], c["cell"], c["k"], mask=c["mask"], hint=c["hint"],
                     n_frames=c["frames"])
         label = (f"seed {seed}: n={c['n']} k={c['k']} frames={c['frames']} hint={c['hint']:.2f} "

@@ -81,6 +81,7 @@ def test_learned_walk_with_network_is_exact_and_saves_work(gpu, oracle_mod):
     w = W.bimodal_triclinic(n=150000, seed=77, k=32)
     want = oracle_mod.knearest(w["xyz"], w["cell"], 32, cell_hint=3.0)
     r = DeviceRunner()
+    r.set_stats(True)  # counters of the learned warp walk are collected on request
     try:
         r.set_mode(1)
         assert_same(r.run(w["xyz"], w["cell"], 32, hint=3.0), want, "fast")

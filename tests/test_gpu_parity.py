@@ -207,6 +207,7 @@ def test_learned_walk_any_proposal_is_exact(runner, oracle_mod, shell):
     want = _oracle(oracle_mod, w["xyz"], w["cell"], 32, hint=3.0)
     runner.set_mode(2)
     runner.set_proposal(shell)
+    runner.set_stats(True)  # the warp walk counts only on request
     try:
         assert_same(runner.run(w["xyz"], w["cell"], 32, hint=3.0), want, f"proposal {shell}")
         cnt, _ = runner.stats()
@@ -215,6 +216,7 @@ def test_learned_walk_any_proposal_is_exact(runner, oracle_mod, shell):
         if shell == 1:
             assert under > 0
     finally:
+        runner.set_stats(False)
         runner.set_proposal(0)
         runner.set_mode(0)
 
