@@ -90,6 +90,11 @@ def whole_job_rate(units_per_rank: int, steps: int, max_ms: float, world: int) -
     return world * units_per_rank * steps / (max_ms / 1000.0)
 
 
+def workload_name(n, k):
+    """Name of the bimodal workload of n points and k neighbours."""
+    return "bimodal_triclinic_4M_k32" if (n, k) == (4_000_000, 32) else f"bimodal_triclinic_n{n}_k{k}"
+
+
 def workload(n, k, seed):
     from linkcell_b200 import workloads as W
     return W.bimodal_triclinic(n=n, seed=seed, k=k)
@@ -328,7 +333,7 @@ def run_reference(args):
     out = {"metric": METRIC, "value": v, "unit": "sources/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "bimodal_triclinic_4M_k32", "n": n, "k": args.k,
+           "config": {"workload": workload_name(n, args.k), "n": n, "k": args.k,
                       "cell_hint": 3.0, "l2": "n/a (CPU)"},
            "impl": "reference",
            "cpu_baseline": {"value": v, "unit": "sources/s", "cores": threads, "kind": "port",
@@ -503,7 +508,7 @@ def run_ours(args):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic",
-           "config": {"workload": "bimodal_triclinic_4M_k32", "n": n, "k": k, "cell_hint": 3.0,
+           "config": {"workload": workload_name(n, k), "n": n, "k": k, "cell_hint": 3.0,
                       "mode": MODE_NAMES[best_mode], "tpp": cnt[-1],
                       "tpp_source": "forced" if args.tpp else "autotuned",
                       "parallelism": f"replicas x{world}",
