@@ -991,7 +991,11 @@ __global__ void __launch_bounds__(256, 2) k_team_walk(BatchBuffers b) {
 // (64 entries for k <= 32, 128 for k <= 64) sends
 // the source to the literal replay.
 constexpr int kSelCap = 512;   // FP32-filtered candidates per warp
-constexpr int kSelWarps = 8;   // warps per block
+// Warps per block: 8 for k <= 32 (3 blocks per SM, register bound); 4 for
+// k <= 64, whose larger S buffers fit 5 smaller blocks per SM where only 2 of 8
+// warps would.
+template <int SN>
+constexpr int sel_warps() { return SN == 2 ? 8 : 4; }
 
 struct __align__(16) SelRow {  // one non-empty row of the cube
   int excl;                    // first candidate position of the row
@@ -1462,7 +1466,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
 }
 
 template <int SN, bool STATS>
-__global__ void __launch_bounds__(kSelWarps * 32, SN == 2 ? 3 : 2) k_select_walk(BatchBuffers b) {
+__global__ void __launch_bounds__(sel_warps<SN>() * 32, SN == 2 ? 3 : 5) k_select_walk(BatchBuffers b) {
   extern __shared__ __align__(16) unsigned char sel_smem[];
   SelShared<SN> &sh = reinterpret_cast<SelShared<SN> *>(sel_smem)[threadIdx.x >> 5];
   const long long total = walk_sources(b);
@@ -1507,16 +1511,16 @@ int sm_count();
 
 template <int SN, bool STATS>
 cudaError_t launch_select_as(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
-  const size_t smem = sizeof(SelShared<SN>) * kSelWarps;
+  const size_t smem = sizeof(SelShared<SN>) * sel_warps<SN>();
   cudaError_t e = cudaFuncSetAttribute(k_select_walk<SN, STATS>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk<SN, STATS>, kSelWarps * 32,
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk<SN, STATS>, sel_warps<SN>() * 32,
                                                 smem);
   if (per_sm < 1) per_sm = 1;
   const int grid = w.grid > 0 ? w.grid : sm_count() * per_sm;
-  k_select_walk<SN, STATS><<<grid, kSelWarps * 32, smem, s>>>(b);
+  k_select_walk<SN, STATS><<<grid, sel_warps<SN>() * 32, smem, s>>>(b);
   return cudaGetLastError();
 }
 
