@@ -206,6 +206,14 @@ int lc_gpu_knearest_batch(lc_gpu_workspace *ws, const double *xyz, const lc_fram
                           size_t n_frames, const int *mask, int *out_nn, double *out_d2,
                           int wait);
 
+/* Extension: the same heterogeneous batch with HOST pointers (xyz, mask and
+ * outputs), served like lc_knearest_d2 by the calling thread's workspace:
+ * with page-locked output buffers the rows come back in ranges while the
+ * rest is searched. mask spans max(mask_offset + n) ints. Errors go to
+ * lc_last_error. Returns 0 or 1. */
+int lc_knearest_batch(const double *xyz, const lc_frame *frames, size_t n_frames, const int *mask,
+                      int *out_nn, double *out_d2);
+
 /* One search that allocates no device memory (no counterpart in the
  * reference). For callers that cannot call cudaMalloc: hosts whose own pool
  * allocator owns all device memory, real-time loops that must not allocate,

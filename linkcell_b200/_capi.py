@@ -40,7 +40,7 @@ EXPORTS = (
     "lc_gpu_proposals",
     "lc_gpu_mlp_params", "lc_gpu_mlp_scratch_floats", "lc_gpu_mlp_forward", "lc_gpu_mlp_grad",
     "lc_gpu_mlp_adam",
-    "lc_gpu_knearest_batch", "lc_gpu_knearest_noalloc",
+    "lc_gpu_knearest_batch", "lc_gpu_knearest_noalloc", "lc_knearest_batch",
 )
 
 _lib = None
@@ -113,6 +113,7 @@ def load():
     L.lc_gpu_mlp_grad.argtypes = [vp, vp, vp, i, vp, vp, vp, vp]
     L.lc_gpu_mlp_adam.argtypes = [vp, vp, vp, vp, i, ctypes.c_float, vp]
     L.lc_gpu_knearest_batch.argtypes = [vp, vp, ctypes.POINTER(LcFrame), sz, vp, vp, vp, i]
+    L.lc_knearest_batch.argtypes = [vp, ctypes.POINTER(LcFrame), sz, vp, vp, vp]
     L.lc_gpu_knearest_noalloc.argtypes = [vp, sz, cp, sz, vp, d, vp, vp, vp, i]
     _lib = L
     return L

@@ -6,6 +6,7 @@
 // src/gpu/knearest.cpp:705-878 for lc_gpu_*.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -87,18 +88,19 @@ Code check_cell(const lc_cell &c) {
   return code == Code::BadCell ? Code::BadCell : Code::Ok;
 }
 
-// Frames with their own cell, n, k and mask offset, planned and searched as
-// one batch (lc_gpu_knearest_batch, Workspace::knearest_into_batch).
-Code run_batch(WorkspaceImpl &w, const double *xyz, const lc_frame *fr, size_t n_frames,
-               const int *mask, int *out_nn, double *out_d2, bool wait, std::string &detail) {
+// The frame table of a batch of frames with their own cell, n, k and mask
+// offset; also the batch's points, output elements and mask extent.
+Code plan_batch(const lc_frame *fr, size_t n_frames, bool has_mask,
+                std::vector<FrameDesc> &frames, size_t &points, size_t &out_n, size_t &mask_n) {
   if (n_frames == 0) return Code::NoPoints;
-  std::vector<FrameDesc> frames(n_frames);
+  frames.assign(n_frames, FrameDesc());
   long long out_base = 0;
+  points = mask_n = 0;
   for (size_t f = 0; f < n_frames; ++f) {
     const lc_frame &x = fr[f];
     if (x.n == 0) return Code::NoPoints;
     if (x.k == 0) return Code::ZeroK;
-    if (x.mask_offset >= 0 && !mask) return Code::NullPointer;
+    if (x.mask_offset >= 0 && !has_mask) return Code::NullPointer;
     double rows[9], origin[3];
     rows_of(x.cell, rows, origin);
     const Code c = lc::plan_frame(rows, origin, x.cell_hint, int(x.k), frames[f]);
@@ -108,7 +110,21 @@ Code run_batch(WorkspaceImpl &w, const double *xyz, const lc_frame *fr, size_t n
     frames[f].mask_base = x.mask_offset >= 0 ? x.mask_offset : 0;
     frames[f].out_base = out_base;
     out_base += (long long)(x.n * x.k);
+    points += x.n;
+    if (x.mask_offset >= 0) mask_n = std::max(mask_n, size_t(x.mask_offset) + x.n);
   }
+  out_n = size_t(out_base);
+  return Code::Ok;
+}
+
+// Frames with their own cell, n, k and mask offset, planned and searched as
+// one batch (lc_gpu_knearest_batch, Workspace::knearest_into_batch).
+Code run_batch(WorkspaceImpl &w, const double *xyz, const lc_frame *fr, size_t n_frames,
+               const int *mask, int *out_nn, double *out_d2, bool wait, std::string &detail) {
+  std::vector<FrameDesc> frames;
+  size_t points = 0, out_n = 0, mask_n = 0;
+  const Code c = plan_batch(fr, n_frames, mask != nullptr, frames, points, out_n, mask_n);
+  if (c != Code::Ok) return c;
   return w.run(frames, xyz, mask, out_nn, out_d2, wait, detail);
 }
 
@@ -386,6 +402,23 @@ int lc_knearest_d2(const double *xyz, size_t n, const lc_cell *simbox, size_t k,
 int lc_knearest_many(const double *xyz, size_t n, size_t n_frames, const lc_cell *simbox, size_t k,
                      const int *mask, double cell_hint, int *out_nn, double *out_d2) {
   return host_search(xyz, n, n_frames, simbox, k, mask, cell_hint, out_nn, out_d2);
+}
+
+int lc_knearest_batch(const double *xyz, const lc_frame *frames, size_t n_frames, const int *mask,
+                      int *out_nn, double *out_d2) {
+  if (!xyz || !frames || !out_nn) return cpu_fail(Code::NullPointer);
+  std::vector<FrameDesc> fd;
+  size_t points = 0, out_n = 0, mask_n = 0;
+  const Code c = plan_batch(frames, n_frames, mask != nullptr, fd, points, out_n, mask_n);
+  if (c != Code::Ok) return cpu_fail(c);
+  if (points >= 0xFFFFFFF0ull || out_n > size_t(INT32_MAX) * 4) return cpu_fail(Code::TooLarge);
+  if (!device_present()) return cpu_fail(Code::NoDevice);
+  std::string detail;
+  const Code rc = host_workspace().run_host(fd, xyz, points * 3, mask, mask_n, out_nn, out_d2,
+                                            out_n, detail);
+  if (rc != Code::Ok) return cpu_fail(rc, detail);
+  cpu_ok();
+  return 0;
 }
 
 const char *lc_last_error(void) { return t_cpu_has_err ? t_cpu_err.c_str() : nullptr; }

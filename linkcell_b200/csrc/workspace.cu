@@ -624,7 +624,6 @@ Code WorkspaceImpl::run_host(std::vector<FrameDesc> &frames, const double *xyz, 
     pipe_.on = true;
     pipe_.host_nn = out_nn;
     pipe_.host_d2 = out_d2;
-    pipe_.k = frames.empty() ? 0 : frames[0].k;
   }
   const Code c = run(frames, h_xyz_.p, mask ? h_mask_.p : nullptr, map_nn ? map_nn : h_nn_.p,
                      out_d2 ? (map_nn ? map_d2 : h_d2_.p) : nullptr, false, detail);
@@ -675,7 +674,21 @@ Code WorkspaceImpl::neighbors_within(const int *nn, const double *d2, size_t row
 Code WorkspaceImpl::walk_in_row_ranges(BatchBuffers &b, const WalkLaunch &wl, cudaStream_t s,
                                        bool timed, std::string &detail) {
   const long long rows = b.npts;
-  const size_t k = size_t(pipe_.k);
+  // First output element of point row r (frames are contiguous in points and
+  // in outputs, each with its own k), from the host copy of the frame table.
+  const int nf = b.nframes;
+  auto elem_at = [&](long long r) -> size_t {
+    int lo = 0, hi = nf - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (h_frames_[mid].pt_base <= r)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const FrameDesc &f = h_frames_[lo];
+    return size_t(f.out_base + std::min<long long>(r - f.pt_base, f.n) * f.k);
+  };
   // Geometric ranges: the copy engine (slower than the walk) starts after a
   // small first range, and each later range is as long as all before it, so
   // its walk ends before the copies ahead of it do. 4M rows: 1/32, 1/32,
@@ -716,7 +729,7 @@ Code WorkspaceImpl::walk_in_row_ranges(BatchBuffers &b, const WalkLaunch &wl, cu
     LC_TRY(launch_replay(br, s));
     LC_TRY(cudaEventRecord(range_ev_[r], s));
     LC_TRY(cudaStreamWaitEvent(copy_stream_, range_ev_[r], 0));
-    const size_t e0 = size_t(r0) * k, ne = size_t(r1 - r0) * k;
+    const size_t e0 = elem_at(r0), ne = elem_at(r1) - e0;
     LC_TRY(cudaMemcpyAsync(pipe_.host_nn + e0, b.out_nn + e0, ne * sizeof(int),
                            cudaMemcpyDeviceToHost, copy_stream_));
     if (pipe_.host_d2)

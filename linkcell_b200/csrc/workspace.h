@@ -186,7 +186,6 @@ class WorkspaceImpl {
     bool on = false, done = false;
     int *host_nn = nullptr;
     double *host_d2 = nullptr;
-    int k = 0;
   };
   Pipe pipe_;
   Buf<int> order_;

@@ -104,3 +104,50 @@ def test_host_abi_many_frames_with_mask_pinned(gpu, lib, oracle_mod, rows):
                                      ctypes.cast(d2_t.data_ptr(), dp)) for _ in range(3)]
     assert _with_env({"LINKCELL_MODE": "2", "LINKCELL_HOST_ROWS": rows}, call) == [0, 0, 0]
     assert_same((nn_t.numpy(), d2_t.numpy()), want, f"many frames rows={rows}")
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_host_batch_heterogeneous_frames(gpu, lib, oracle_mod, pinned):
+    """lc_knearest_batch: frames with their own cell, n, k and mask, host
+    pointers. With page-locked outputs the rows come back in row ranges that
+    cross frame boundaries, where k changes."""
+    import torch
+    from gpu_helpers import lc_cell_of
+    from linkcell_b200 import LcFrame
+    from linkcell_b200 import workloads as W
+    frames = W.frames_batch(n_frames=12, seed=17, n_min=500, n_max=20000)
+    arr = (LcFrame * len(frames))()
+    total, moff = 0, 0
+    for i, f in enumerate(frames):
+        arr[i].n, arr[i].k = len(f["xyz"]), f["k"]
+        arr[i].cell = lc_cell_of(f["cell"])
+        arr[i].cell_hint = float(f["cell_hint"])
+        arr[i].mask_offset = moff
+        moff += len(f["xyz"])
+        total += len(f["xyz"]) * f["k"]
+    assert moff > 2 * 16384  # several row ranges
+    xyz = np.ascontiguousarray(np.concatenate([f["xyz"] for f in frames]), dtype=np.float64)
+    mask = np.ascontiguousarray(np.concatenate([f["mask"] for f in frames]), dtype=np.int32)
+    if pinned:
+        nn_t = torch.full((total,), -9, dtype=torch.int32).pin_memory()
+        d2_t = torch.zeros((total,), dtype=torch.float64).pin_memory()
+        nn_p, d2_p = nn_t.data_ptr(), d2_t.data_ptr()
+    else:
+        nn_a = np.full(total, -9, dtype=np.int32)
+        d2_a = np.zeros(total)
+        nn_p, d2_p = nn_a.ctypes.data, d2_a.ctypes.data
+
+    def call():
+        return lib.lc_knearest_batch(xyz.ctypes.data, arr, len(frames), mask.ctypes.data, nn_p,
+                                     d2_p)
+    rc = _in_thread(lambda: [call(), call()])  # the first call tunes the walk
+    assert rc == [0, 0], lib.lc_last_error()
+    nn, d2 = (nn_t.numpy(), d2_t.numpy()) if pinned else (nn_a, d2_a)
+    off = 0
+    for i, f in enumerate(frames):
+        n, k = len(f["xyz"]), f["k"]
+        want = oracle_mod.knearest(f["xyz"], f["cell"], k, mask=f["mask"],
+                                   cell_hint=f["cell_hint"])
+        got = (nn[off:off + n * k].reshape(n, k), d2[off:off + n * k].reshape(n, k))
+        assert_same(got, want, f"host batch pinned={pinned} frame {i}")
+        off += n * k
