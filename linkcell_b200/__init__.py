@@ -301,18 +301,16 @@ def _knearest_cuda(L, xyz, cell, k, mask, hint, dev, workspace, sync):
 
 def knearest_batch(xyz, frames, mask=None, *, workspace: Workspace | None = None,
                    sync: bool = True):
-    """Heterogeneous batch on the device (extension, lc_gpu_knearest_batch).
+    """Heterogeneous batch (extension): frames with their own cell, n, k and mask.
 
-    xyz: CUDA float64 (sum n_f, 3). frames: list of dicts with keys n, k,
-    cell ((3,), (3,3) or (4,3) host doubles), optional cell_hint and
-    mask_offset. Returns flat (indices, dist2) CUDA tensors of sum n_f * k_f
-    entries; frame f starts at sum over g < f of n_g * k_g.
+    xyz: float64 (sum n_f, 3), a CUDA tensor (lc_gpu_knearest_batch, CUDA
+    outputs on torch's current stream) or host memory (lc_knearest_batch,
+    numpy outputs). frames: list of dicts with keys n, k, cell ((3,), (3,3)
+    or (4,3) host doubles), optional cell_hint and mask_offset. Returns flat
+    (indices, dist2) of sum n_f * k_f entries; frame f starts at sum over
+    g < f of n_g * k_g.
     """
-    import torch
     L = _capi.load()
-    x = xyz.contiguous()
-    if not x.is_cuda or x.dtype != torch.float64:
-        raise ValueError("xyz must be a CUDA float64 tensor")
     arr = (LcFrame * len(frames))()
     total = 0
     for f, fr in enumerate(frames):
@@ -322,6 +320,23 @@ def knearest_batch(xyz, frames, mask=None, *, workspace: Workspace | None = None
         arr[f].cell_hint = float(fr.get("cell_hint", 0.0) or 0.0)
         arr[f].mask_offset = int(fr.get("mask_offset", -1))
         total += arr[f].n * arr[f].k
+    cuda_in, _ = _device_of(xyz)
+    if not cuda_in:
+        x = np.ascontiguousarray(_host_array(xyz), dtype=np.float64)
+        m = None if mask is None else np.ascontiguousarray((_host_array(mask) != 0).astype(np.int32))
+        nn = np.empty(total, dtype=np.int32)
+        d2 = np.empty(total, dtype=np.float64)
+        rc = L.lc_knearest_batch(x.ctypes.data, arr, len(frames),
+                                 None if m is None else m.ctypes.data, nn.ctypes.data,
+                                 d2.ctypes.data)
+        if rc != 0:
+            _raise_from_lib(_capi.cpu_error())
+        return nn, d2
+    import torch
+    x = xyz if isinstance(xyz, torch.Tensor) else torch.from_dlpack(xyz)
+    x = x.contiguous()
+    if x.dtype != torch.float64:
+        raise ValueError("xyz must be float64")
     dev = x.device.index
     ws = workspace if workspace is not None else _workspace_for(dev)
     with torch.cuda.device(dev):

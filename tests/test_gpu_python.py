@@ -98,3 +98,32 @@ def test_errors_on_gpu(gpu):
     with pytest.raises(RuntimeError, match="linked-cell mesh is too fine"):
         L.knearest(np.random.default_rng(0).random((4, 3)), np.array([10.0, 10.0, 10.0]), 1,
                    cell_hint=1e-9)
+
+
+def test_knearest_batch_host_and_cuda(gpu, oracle_mod):
+    """linkcell_b200.knearest_batch: host arrays give numpy rows (lc_knearest_batch),
+    CUDA tensors give CUDA rows (lc_gpu_knearest_batch), both the oracle's."""
+    import torch
+    import linkcell_b200 as L
+    from linkcell_b200 import workloads as W
+    frames = W.frames_batch(n_frames=5, seed=23, n_min=200, n_max=4000)
+    xyz = np.concatenate([f["xyz"] for f in frames]).astype(np.float64)
+    mask = np.concatenate([f["mask"] for f in frames]).astype(np.int32)
+    spec, off = [], 0
+    for f in frames:
+        spec.append(dict(n=len(f["xyz"]), k=f["k"], cell=f["cell"], cell_hint=f["cell_hint"],
+                         mask_offset=off))
+        off += len(f["xyz"])
+    nn_h, d2_h = L.knearest_batch(xyz, spec, mask)
+    nn_c, d2_c = L.knearest_batch(torch.as_tensor(xyz, device="cuda"), spec,
+                                  torch.as_tensor(mask, device="cuda"))
+    assert isinstance(nn_h, np.ndarray) and nn_c.is_cuda
+    assert np.array_equal(nn_h, nn_c.cpu().numpy())
+    assert np.array_equal(d2_h.view(np.int64), d2_c.cpu().numpy().view(np.int64))
+    pos = 0
+    for i, f in enumerate(frames):
+        n, k = len(f["xyz"]), f["k"]
+        want = oracle_mod.knearest(f["xyz"], f["cell"], k, mask=f["mask"],
+                                   cell_hint=f["cell_hint"])
+        assert np.array_equal(nn_h[pos:pos + n * k].reshape(n, k), want[0]), f"frame {i}"
+        pos += n * k
