@@ -125,7 +125,7 @@ cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s);
 // pre-filled with -1 for masked points).
 // Output-row ranges of a host-pointer search: row cuts cut[0] = 0 <
 // cut[1] < ... < cut[nr] (point units).
-constexpr int kMaxRowRanges = 8;
+constexpr int kMaxRowRanges = 12;
 struct RowCuts {
   long long cut[kMaxRowRanges + 1];
   int nr;

@@ -689,17 +689,20 @@ Code WorkspaceImpl::walk_in_row_ranges(BatchBuffers &b, const WalkLaunch &wl, cu
     const FrameDesc &f = h_frames_[lo];
     return size_t(f.out_base + std::min<long long>(r - f.pt_base, f.n) * f.k);
   };
-  // Geometric ranges: the copy engine (slower than the walk) starts after a
-  // small first range, and each later range is as long as all before it, so
-  // its walk ends before the copies ahead of it do. 4M rows: 1/32, 1/32,
-  // 1/16, 1/8, 1/4, 1/2 (measured against eight equal ranges and first
-  // ranges of 1/64 and 1/16: the fastest).
+  // The copy engine starts after a short first range (1/32 of the rows).
+  // Later ranges double, so each is walked before the copies ahead of it
+  // finish, up to 1/8 of the rows, so that little is left to copy after the
+  // last walk when the walk is about as long as the copy. 4M rows: 1/32,
+  // 1/32, 1/16, then 1/8 each (measured against eight equal ranges and
+  // geometric ranges up to 1/2).
   RowCuts rc;
   rc.nr = 0;
   rc.cut[0] = 0;
   const long long first = std::max<long long>(rows / 32, kMinRangeRows);
+  const long long cap = std::max<long long>(rows / 8, first);
   while (rc.cut[rc.nr] < rows) {
-    const long long len = rc.nr == 0 ? first : std::max(first, rc.cut[rc.nr]);
+    const long long len =
+        rc.nr == 0 ? first : std::min(cap, std::max(first, rc.cut[rc.nr]));
     rc.cut[rc.nr + 1] = rc.nr + 1 == kMaxRowRanges ? rows : std::min(rows, rc.cut[rc.nr] + len);
     ++rc.nr;
   }
