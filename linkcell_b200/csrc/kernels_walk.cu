@@ -1823,7 +1823,7 @@ __device__ void warp_replay(const BatchBuffers &b, const FrameDesc &fr, long lon
 }
 
 template <int KPL>
-__global__ void __launch_bounds__(256, 2) k_replay_warp(BatchBuffers b) {
+__global__ void __launch_bounds__(64, 11) k_replay_warp(BatchBuffers b) {
   long long cnt = *b.replay_count;
   if (cnt > b.replay_cap) cnt = b.replay_cap;
   const int lane = threadIdx.x & 31;
@@ -2038,16 +2038,17 @@ cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s) {
   if (b.replay_threads <= 0) return cudaSuccess;
   if (b.kmax <= 256) {
     // one warp per queued source; NaN frames take one thread of the warp
-    const int warps = std::max(1, std::min(b.replay_threads, sm_count() * 16));
-    const int grid = (warps + 7) / 8;
+    // 2-warp blocks, 11 per SM (the replay is bound by latency: more warps)
+    const int warps = std::max(1, std::min(b.replay_threads, sm_count() * 22));
+    const int grid = (warps + 1) / 2;
     if (b.kmax <= 32)
-      k_replay_warp<1><<<grid, 256, 0, s>>>(b);
+      k_replay_warp<1><<<grid, 64, 0, s>>>(b);
     else if (b.kmax <= 64)
-      k_replay_warp<2><<<grid, 256, 0, s>>>(b);
+      k_replay_warp<2><<<grid, 64, 0, s>>>(b);
     else if (b.kmax <= 128)
-      k_replay_warp<4><<<grid, 256, 0, s>>>(b);
+      k_replay_warp<4><<<grid, 64, 0, s>>>(b);
     else
-      k_replay_warp<8><<<grid, 256, 0, s>>>(b);
+      k_replay_warp<8><<<grid, 64, 0, s>>>(b);
     return cudaGetLastError();
   }
   const int block = 128;

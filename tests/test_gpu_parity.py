@@ -136,6 +136,32 @@ def test_many_frames_share_cell_and_mask(runner, oracle_mod, mode):
     assert_same(host_abi(xyz, [12.0, 12.0, 12.0], 6, mask, n_frames=F), want, "frames host")
 
 
+@pytest.mark.parametrize("mode", MODES)
+def test_lattice_ties_large_k(runner, oracle_mod, mode):
+    """k of 100 and 200 on a cubic lattice with duplicates: the k-th values tie,
+    so sources go through the literal warp replay with 4 and 8 heap slots per
+    lane (k up to 128 and 256)."""
+    runner.set_mode(mode)
+    runner.set_stats(True)
+    nside = 12
+    a = 30.0 / nside
+    g = np.stack(np.meshgrid(np.arange(nside), np.arange(nside), np.arange(nside),
+                             indexing="ij"), -1).reshape(-1, 3)[:, ::-1] * a
+    rng = np.random.default_rng(5)
+    dup = g[rng.choice(len(g), 40, replace=False)]
+    xyz = np.ascontiguousarray(np.concatenate([g, dup]), dtype=np.float64)
+    try:
+        for k in (100, 200):
+            want = _oracle(oracle_mod, xyz, [30.0, 30.0, 30.0], k, hint=3.0)
+            assert_same(runner.run(xyz, [30.0, 30.0, 30.0], k, hint=3.0), want,
+                        f"lattice k={k} mode {mode}")
+        cnt, _ = runner.stats()
+        assert mode == 3 or cnt[2] > 0  # ties sent to the replay
+    finally:
+        runner.set_stats(False)
+        runner.set_mode(0)
+
+
 def test_large_k_and_replay_all(runner, oracle_mod):
     """k above the shared-memory heap (exact sequential walk for every source)."""
     rng = np.random.default_rng(2)
