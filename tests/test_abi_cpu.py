@@ -127,3 +127,34 @@ def test_struct_layout():
     from linkcell_b200 import LcCell, LcFrame
     assert ctypes.sizeof(LcCell) == 12 * 8
     assert ctypes.sizeof(LcFrame) == 8 + 8 + 96 + 8 + 8
+
+
+def test_host_batch_argument_checks(lib):
+    """lc_knearest_batch validates every frame before it needs a device."""
+    from linkcell_b200 import LcCell, LcFrame
+    L = lib
+    xyz = np.zeros((4, 3))
+    out = np.zeros(64, dtype=np.int32)
+
+    def call(frames, mask=None):
+        arr = (LcFrame * len(frames))(*frames)
+        return L.lc_knearest_batch(xyz.ctypes.data, arr, len(frames),
+                                   None if mask is None else mask.ctypes.data, out.ctypes.data,
+                                   None)
+
+    box = LcCell(10.0, 0, 0, 0, 10.0, 0, 0, 0, 10.0, 0, 0, 0)
+    flat = LcCell(10.0, 0, 0, 20.0, 0, 0, 0, 0, 10.0, 0, 0, 0)  # a and b parallel
+    good = LcFrame(2, 2, box, 0.0, -1)
+    assert call([good, LcFrame(0, 2, box, 0.0, -1)]) == 1
+    assert L.lc_last_error() == b"no points"
+    assert call([good, LcFrame(2, 0, box, 0.0, -1)]) == 1
+    assert L.lc_last_error() == b"k must be at least 1"
+    assert call([good, LcFrame(2, 2, box, 0.0, 0)]) == 1  # masked frame, no mask
+    assert L.lc_last_error() == b"null pointer"
+    assert call([good, LcFrame(2, 2, flat, 0.0, -1)]) == 1
+    assert L.lc_last_error() == b"singular or non-positive cell"
+    assert call([]) == 1
+    assert L.lc_last_error() == b"no points"
+    if not has_gpu():
+        assert call([good, good]) == 1
+        assert L.lc_last_error() == b"no CUDA device available"
