@@ -193,6 +193,30 @@ def cpu_baseline(w, seconds_target=15.0):
                        f"extrapolated to all sources")}
 
 
+def parity_sample(w, nn, d2, count=20000):
+    """The oracle as the checker, beside the CPU baseline: the rows of a seeded
+    sample of sources from the timed search against the reference walk's
+    (oracle.knearest_subset): rows whose indices differ, and the largest
+    relative dist2 difference."""
+    import torch
+    from oracle import oracle as O
+    O.build()
+    n = w["xyz"].shape[0]
+    src = np.sort(np.random.default_rng(7).choice(n, size=min(count, n), replace=False))
+    want_nn, want_d2 = O.knearest_subset(w["xyz"], w["cell"], w["k"], src, mask=w.get("mask"),
+                                         cell_hint=w["cell_hint"], threads=os.cpu_count() or 1)
+    idx = torch.as_tensor(src, device=nn.device)
+    got_nn, got_d2 = nn[idx].cpu().numpy(), d2[idx].cpu().numpy()
+    bad_rows = int((got_nn != want_nn).any(axis=1).sum())
+    finite = np.isfinite(want_d2)
+    both_nan = ~finite & np.isnan(got_d2)
+    rel = np.abs(got_d2[finite] - want_d2[finite]) / np.maximum(np.abs(want_d2[finite]), 1e-300)
+    return {"sources": int(src.size), "index_mismatch_rows": bad_rows,
+            "dist2_max_rel_err": float(rel.max()) if rel.size else 0.0,
+            "dist2_nan_agree": bool(both_nan.sum() == (~finite).sum()),
+            "checker": "oracle reference walk (knearest_subset), seeded sample of the timed rows"}
+
+
 GPULITE_LIB = os.path.join(ROOT, "oracle", "_ref", "libref_gpulite.so")
 GPULITE_K = 16            # the gpulite path supports k <= 16 (src/gpu/knearest.cpp:23)
 GPULITE_CELLS = 262144    # ... and at most this many cells (src/gpu/knearest.cpp:24)
@@ -490,9 +514,10 @@ def run_ours(args):
                "h2d_bytes_per_step": n * 24, "d2h_bytes_per_step": n * k * 12,
                "ms_per_step": 1000.0 * tot / args.steps, "timer": "host wall clock around the call"}
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(w, args.cpu_seconds)
+        parity = parity_sample(w, nn, d2)
     gpulite = None
     if rank == 0 and world == 1 and not args.no_gpulite:
         assert L.lc_gpu_set_mode(ws, best_mode) == 0
@@ -514,6 +539,7 @@ def run_ours(args):
                       "parallelism": f"replicas x{world}",
                       "l2": "flushed between timed steps (256 MB write)"},
            "roofline": roofline, "cpu_baseline": cpu, "gpulite_baseline": gpulite, "e2e": e2e,
+           "parity_sample": parity,
            "gpu_launches": launches_per_step * args.steps, "clocks": sampler.summary(),
            "plain_fp64": {"value": plain_value, "unit": "sources/s",
                           "walk_ms": statistics.mean(plain_walk), "tpp": plain_cnt[-1]},
