@@ -964,12 +964,15 @@ __global__ void __launch_bounds__(256, 2) k_team_walk(BatchBuffers b) {
 //  1. Gather. The cube is (2 R_p + 1)^2 rows of cells along x; cells sort by
 //     (z, y, x), so the cells of a row that survive the distance bound form
 //     at most two contiguous ranges of the sorted points (two when the row
-//     wraps the box in x). Each lane trims one row to the x range whose FP32
-//     lower bound lam |gap|^2 can pass the filter at B(R_p) = (R_p cell_min)^2,
-//     the warp walks the concatenated ranges 32 candidates at a time (the
-//     row of candidate g is found from one OR-reduction of row starts), and
-//     candidates with d32 <= thr(B(R_p)) go to a per-warp buffer (FP32
-//     distance, sorted position, shell, wrap counts).
+//     wraps the box in x). Each lane trims one row to the x range that can
+//     hold a point within the filter (the Schur form of the bin-unit metric
+//     bounds the other two axes' share), the warp walks the concatenated
+//     ranges in two 32-candidate windows per trip (the row of candidate g is
+//     found from one OR-reduction of row starts), and candidates below the
+//     FP32 filter go to a per-warp buffer (FP32 distance, sorted position,
+//     shell, wrap counts). The first gather covers only
+//     rho2 = max(B(R_p - 1), q B(R_p)); when fewer than k candidates lie
+//     within rho2, the whole ball B(R_p) = (R_p cell_min)^2 is gathered.
 //  2. Stop reach. The reference stops at the first R with at least k
 //     candidates of shells <= R within B(R). Each candidate counts from
 //     reach max(shell, b(d)), b(d) = the first R >= 1 with d <= B(R), read
