@@ -11,8 +11,17 @@ timed steps by writing a 256 MB buffer; each step also writes 1.5 GB of
 output rows.
 
 --impl reference times the reference CPU walk (the C++ restatement of
-src/knearest.rs in oracle/, on every host thread) on a bounded sample of
-sources of the same workload.
+src/knearest.rs in oracle/, on every host thread): each step is the fold,
+bin and linked lists over all points plus the walk of a quarter of the
+sources (every 4th, rotating), timed as it runs.
+
+Beside the headline, the default run reports: the rooflines of the walk
+(reference candidate pairs per second against the FP32-issue bound) and of
+the prep (fold, bin, scan, placement against HBM); the network against the
+best constant shell proposal on the same select walk; the batched-frames
+configuration (256 frames in one graph-replayed call, and end to end through
+lc_knearest_batch); the reference CPU walk on all host threads and on one;
+the reference's gpulite GPU path; and a parity sample against the oracle.
 
 Under torchrun each rank runs its own frame on its own GPU (no collective on
 the data path; weak scaling); timings are the max over ranks.
@@ -24,6 +33,7 @@ import argparse
 import ctypes
 import json
 import os
+import platform
 import statistics
 import subprocess
 import sys
@@ -54,6 +64,9 @@ def parse():
     p.add_argument("--plain-tpp", type=int, default=0,
                    help="the same for the plain FP64 walk timed beside it")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-sweep", action="store_true",
+                   help="skip the network-vs-constant-proposal sweep")
+    p.add_argument("--no-c3", action="store_true", help="skip the batched-frames block")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-gpulite", action="store_true",
@@ -172,25 +185,56 @@ class ClockSampler:
                 "samples": len(self.rows), "power_w_max": max(num(r[2]) or 0 for r in self.rows)}
 
 
-def cpu_baseline(w, seconds_target=15.0):
-    """The reference walk restated in oracle/ on all host threads, on a bounded
-    sample of sources; extrapolated to sources/s of the whole frame."""
-    from oracle import oracle as O
-    O.build()
+def host_info():
+    """The host the CPU figures come from: name, CPU model, logical cores."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"host": platform.node(), "cpu_model": model, "logical_cores": os.cpu_count()}
+
+
+def _sampled_rate(O, w, threads, seconds_target):
+    """The reference walk on `threads` threads: fold + bin + lists over all
+    points, then the walk of an evenly strided sample of sources sized to
+    about seconds_target; sources/s of the whole frame with the walk time
+    scaled from the sample."""
     n = w["xyz"].shape[0]
-    threads = os.cpu_count() or 1
     probe = O.time_sample(w["xyz"], w["cell"], w["k"], cell_hint=w["cell_hint"], first=0,
-                          stride=max(1, n // 20000), count=20000, threads=threads)
+                          stride=max(1, n // 4000), count=4000, threads=threads)
     per_src = probe["walk_s"] / max(1, probe["walked"])
-    count = int(max(20000, min(n, seconds_target / max(per_src, 1e-9))))
+    count = int(max(4000, min(n, seconds_target / max(per_src, 1e-9))))
     stride = max(1, n // count)
     r = O.time_sample(w["xyz"], w["cell"], w["k"], cell_hint=w["cell_hint"], first=0,
                       stride=stride, count=count, threads=threads)
     est_total = r["prep_s"] + r["walk_s"] * (n / max(1, r["walked"]))
-    return {"value": n / est_total, "unit": "sources/s", "cores": threads, "kind": "port",
+    return n / est_total, r, stride
+
+
+def cpu_baseline(w, seconds_target=15.0):
+    """The reference walk restated in oracle/ on all host threads, and on one
+    thread, each on a bounded sample of sources (scaled to sources/s of the
+    whole frame; the sample is stated)."""
+    from oracle import oracle as O
+    O.build()
+    n = w["xyz"].shape[0]
+    threads = os.cpu_count() or 1
+    v, r, stride = _sampled_rate(O, w, threads, seconds_target)
+    v1, r1, stride1 = _sampled_rate(O, w, 1, seconds_target / 3.0)
+    return {"value": v, "unit": "sources/s", "cores": threads, "kind": "port",
             "sample": (f"fold+bin+lists over all {n} points ({r['prep_s']:.2f} s) plus the walk of "
-                       f"{r['walked']} sources (every {stride}-th, {r['walk_s']:.2f} s), "
-                       f"extrapolated to all sources")}
+                       f"{r['walked']} sources (every {stride}-th, {r['walk_s']:.2f} s), the walk "
+                       f"time scaled to all sources"),
+            "single_core": {"value": v1, "unit": "sources/s", "cores": 1,
+                            "sample": (f"the same on one thread: prep {r1['prep_s']:.2f} s, walk of "
+                                       f"{r1['walked']} sources (every {stride1}-th, "
+                                       f"{r1['walk_s']:.2f} s)")},
+            **host_info()}
 
 
 def parity_sample(w, nn, d2, count=20000):
@@ -203,8 +247,9 @@ def parity_sample(w, nn, d2, count=20000):
     O.build()
     n = w["xyz"].shape[0]
     src = np.sort(np.random.default_rng(7).choice(n, size=min(count, n), replace=False))
-    want_nn, want_d2 = O.knearest_subset(w["xyz"], w["cell"], w["k"], src, mask=w.get("mask"),
-                                         cell_hint=w["cell_hint"], threads=os.cpu_count() or 1)
+    want_nn, want_d2, visits = O.knearest_subset(w["xyz"], w["cell"], w["k"], src,
+                                                 mask=w.get("mask"), cell_hint=w["cell_hint"],
+                                                 threads=os.cpu_count() or 1, with_visits=True)
     idx = torch.as_tensor(src, device=nn.device)
     got_nn, got_d2 = nn[idx].cpu().numpy(), d2[idx].cpu().numpy()
     bad_rows = int((got_nn != want_nn).any(axis=1).sum())
@@ -214,6 +259,7 @@ def parity_sample(w, nn, d2, count=20000):
     return {"sources": int(src.size), "index_mismatch_rows": bad_rows,
             "dist2_max_rel_err": float(rel.max()) if rel.size else 0.0,
             "dist2_nan_agree": bool(both_nan.sum() == (~finite).sum()),
+            "ref_pairs_per_source": float(visits.mean()),
             "checker": "oracle reference walk (knearest_subset), seeded sample of the timed rows"}
 
 
@@ -334,7 +380,15 @@ def gpulite_leg(args, L, ws, x, n):
                                  "mode": "learned"}}
 
 
+REF_PARTS = 4  # a reference step walks every REF_PARTS-th source
+
+
 def run_reference(args):
+    """The reference CPU walk (the oracle's restatement of src/knearest.rs,
+    kind "port": the image has no Rust toolchain) on all host threads. Each
+    step is timed as it runs: fold + bin + linked lists over all points, then
+    the walk of every 4th source (offset rotating by step), so a step walks a
+    quarter of the frame's sources; value = sources walked / step time."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
@@ -343,17 +397,16 @@ def run_reference(args):
     O.build()
     n = w["xyz"].shape[0]
     threads = os.cpu_count() or 1
-    # bounded sample per step so the whole run stays within minutes
-    count = int(os.environ.get("LINKCELL_REF_SAMPLE", "60000"))
-    stride = max(1, n // count)
-    vals = []
+    count = (n + REF_PARTS - 1) // REF_PARTS
+    secs, walked = [], []
     for step in range(args.warmup + args.steps):
-        r = O.time_sample(w["xyz"], w["cell"], w["k"], cell_hint=w["cell_hint"], first=step % stride,
-                          stride=stride, count=count, threads=threads)
+        r = O.time_sample(w["xyz"], w["cell"], w["k"], cell_hint=w["cell_hint"],
+                          first=step % REF_PARTS, stride=REF_PARTS, count=count, threads=threads)
         if step >= args.warmup:
-            vals.append(n / (r["prep_s"] + r["walk_s"] * (n / max(1, r["walked"]))))
-    v = statistics.median(vals)
-    ms = 1000.0 * n / v
+            secs.append(r["prep_s"] + r["walk_s"])
+            walked.append(r["walked"])
+    v = sum(walked) / sum(secs)
+    ms = 1000.0 * sum(secs) / len(secs)
     out = {"metric": METRIC, "value": v, "unit": "sources/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -361,11 +414,51 @@ def run_reference(args):
                       "cell_hint": 3.0, "l2": "n/a (CPU)"},
            "impl": "reference",
            "cpu_baseline": {"value": v, "unit": "sources/s", "cores": threads, "kind": "port",
-                            "sample": f"fold+bin over all {n} points plus the walk of every "
-                                      f"{stride}-th source ({count} sources) per step, "
-                                      "extrapolated to the whole frame"},
+                            "sample": (f"each step: fold+bin+lists over all {n} points, then the "
+                                       f"walk of every {REF_PARTS}th source ({walked[0]} "
+                                       f"sources), timed as it runs"),
+                            **host_info()},
            "e2e": {"value": v, "unit": "sources/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
+
+
+COUNTER_NAMES = ["pairs", "inserts", "replays", "shells", "pruned", "reranks", "prop_under",
+                 "prop_over", "prop_exact", "revisited", "fallback"]
+
+
+def prep_roofline(frame_rows, n, prep_ms, peak):
+    """Fold, bin, scan and placement against HBM: the design-independent
+    minimum per search (read the coordinates, write the cell-sorted FP64
+    coordinates and the point index, count and offset per cell) over the
+    measured prep time, and the DRAM traffic of those kernels from the
+    committed ncu summary, where there is one."""
+    from linkcell_b200 import workloads as W
+    cells = int(np.prod(W.bins_of(np.asarray(frame_rows, dtype=np.float64))))
+    algo = n * (24 + 24 + 4) + 8 * (cells + 1)
+    achieved = algo / (prep_ms / 1000.0) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "prep_bimodal_4M_traffic.txt")
+    if os.path.exists(tpath) and n == 4_000_000:
+        for line in open(tpath):
+            if line.startswith("traffic_bytes_per_search:"):
+                traffic = float(line.split(":")[1])
+    return {"bound": "hbm", "unit": "GB/s", "achieved": achieved, "peak": peak,
+            "frac": achieved / peak, "algorithmic_bytes": algo,
+            "bytes_per_point": algo / n, "ms": prep_ms, "traffic": traffic,
+            "traffic_over_algorithmic": None if traffic is None else traffic / algo,
+            "kernels": "k_fold_bin, k_scan_cells, k_place_slots, k_place_records"}
+
+
+def walk_roofline(ref_pairs, walk_ms, f_sm_mhz, sms):
+    """The walk in candidate-pair evaluations as the reference visits them
+    (its heap pushes: every occupant of every cell of shells 1..R*, minus the
+    source) per second, against the FP32-issue bound of about 8 FP32
+    instructions per pair: SMs x 128 lanes x f_SM / 8."""
+    achieved = ref_pairs / (walk_ms / 1000.0)
+    peak = sms * 128 * f_sm_mhz * 1e6 / 8.0
+    return {"bound": "fp32_issue", "unit": "pair-evals/s", "achieved": achieved, "peak": peak,
+            "frac": achieved / peak, "ref_pairs": ref_pairs, "walk_ms": walk_ms,
+            "f_sm_mhz": f_sm_mhz, "sms": sms}
 
 
 def run_ours(args):
@@ -378,6 +471,7 @@ def run_ours(args):
     else:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
     from linkcell_b200 import _capi
     from linkcell_b200 import build as B
     from linkcell_b200 import _cell_struct
@@ -408,9 +502,13 @@ def run_ours(args):
             _, tau, meta = learn.load()
             model_info = {"path": os.path.relpath(learn.MODEL_PATH, ROOT), "tau": tau, "trained": meta}
 
-    def time_mode(mode, steps, warmup, tpp):
+    def time_mode(mode, steps, warmup, tpp, shell=0):
+        """steps timed searches of one configuration (shell > 0: that shell
+        proposed for every source instead of the network's proposals), then
+        one untimed search that counts the walk statistics."""
         assert L.lc_gpu_set_mode(ws, mode) == 0
         assert L.lc_gpu_set_tpp(ws, tpp) == 0  # 0: the autotuner's choice
+        assert L.lc_gpu_set_proposal(ws, shell) == 0
         for _ in range(warmup):
             step()
             L.lc_gpu_wait(ws)
@@ -420,7 +518,6 @@ def run_ours(args):
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(steps)]
         walk_ms, prep_ms, replay_ms, prop_ms = [], [], [], []
-        counters = None
         for s in range(steps):
             with torch.cuda.stream(tstream):
                 flush.fill_(s & 0xFF)  # L2 flush between timed steps, outside the events
@@ -445,43 +542,67 @@ def run_ours(args):
         assert L.lc_gpu_set_stats(ws, 0) == 0
         buf = (ctypes.c_longlong * 16)()
         L.lc_gpu_stats(ws, buf, 16, None)
-        counters = list(buf)
-        counters.append(int(L.lc_gpu_get_tpp(ws)))  # walk design used (autotuned unless forced)
+        counters = {nm: int(buf[i]) for i, nm in enumerate(COUNTER_NAMES)}
+        counters["tpp"] = int(L.lc_gpu_get_tpp(ws))  # walk design used (autotuned unless forced)
+        assert L.lc_gpu_set_proposal(ws, 0) == 0
         total = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), "cuda")
-        return total, walk_ms, counters, prep_ms, replay_ms, prop_ms
+        return {"total_ms": total, "ms": total / steps, "walk_ms": statistics.mean(walk_ms),
+                "prep_ms": statistics.mean(prep_ms), "replay_ms": statistics.mean(replay_ms),
+                "propose_ms": statistics.mean(prop_ms), "counters": counters}
 
     best_mode = args.mode if args.mode >= 0 else 2
     # plain FP64 walk (the 2x denominator), then the headline mode
     sampler = ClockSampler(dev)
     sampler.start()  # clocks over both timed regions
     time.sleep(0.3)  # nvidia-smi start-up
-    plain_total, plain_walk, plain_cnt, _, _, _ = time_mode(0, max(3, args.steps // 2),
-                                                            args.warmup, args.plain_tpp)
-    total, walk_ms, cnt, prep_ms, replay_ms, prop_ms = time_mode(best_mode, args.steps,
-                                                                 args.warmup, args.tpp)
+    plain_steps = max(3, args.steps // 2)
+    plain = time_mode(0, plain_steps, args.warmup, args.plain_tpp)
+    head = time_mode(best_mode, args.steps, args.warmup, args.tpp)
     sampler.stop()
-    ms_per_step = total / args.steps
-    value = whole_job_rate(n, args.steps, total, world)
-    plain_value = whole_job_rate(n, max(3, args.steps // 2), plain_total, world)
+    clocks = sampler.summary()
+    ms_per_step = head["ms"]
+    value = whole_job_rate(n, args.steps, head["total_ms"], world)
+    plain_value = whole_job_rate(n, plain_steps, plain["total_ms"], world)
 
     # roofline of the dominant kernel (the walk): algorithmic bytes per launch
     peak, peak_kind = measured_peaks()
     # per source: FP32 record 16 B + FP64 coordinates 24 B + index and cell 8 B read,
     # the output row (i32 + f64 per slot) written
     walk_bytes = n * (48 + 12 * k)
-    walk_avg_ms = statistics.mean(walk_ms)
+    walk_avg_ms = head["walk_ms"]
     achieved = walk_bytes / (walk_avg_ms / 1000.0) / 1e9
     traffic = None
     tname = "select_walk" if best_mode == 2 else "walk"
     tpath = os.path.join(ROOT, "profiles", f"{tname}_bimodal_4M_k32_traffic.txt")
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and (n, k) == (4_000_000, 32):
         for line in open(tpath):
             if line.startswith("traffic_bytes_per_launch:"):
                 traffic = float(line.split(":")[1])
+    f_sm = clocks.get("sm_mhz") or 1965.0
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_select_walk" if best_mode == 2 else "walk",
-                "algorithmic_bytes_per_source": 48 + 12 * k}
+                "peak_source": f"{peak_kind} hbm_gbs",
+                "kernel": "k_select_walk" if best_mode == 2 else "walk",
+                "algorithmic_bytes_per_source": 48 + 12 * k,
+                # the plain FP64 walk visits exactly the reference's pairs (its
+                # counter equals the oracle's heap pushes: 348.65 per source here)
+                "walk": walk_roofline(float(plain["counters"]["pairs"]), walk_avg_ms, f_sm, sms),
+                "prep": prep_roofline(w["cell"], n, head["prep_ms"], peak)}
+
+    # the network against one constant shell for every source, same select walk
+    lvc = None
+    if best_mode == 2 and model_info is not None and not args.no_sweep:
+        sweep = []
+        for shell in range(1, 7):
+            r = time_mode(2, 5, 1, args.tpp, shell=shell)
+            sweep.append({"shell": shell, "ms": r["ms"], "walk_ms": r["walk_ms"],
+                          "replay_ms": r["replay_ms"], **r["counters"]})
+        best = min(sweep, key=lambda e: e["ms"])
+        lvc = {"network": {"ms": head["ms"], "walk_ms": head["walk_ms"],
+                           "propose_ms": head["propose_ms"], "replay_ms": head["replay_ms"],
+                           **head["counters"]},
+               "best_constant": best, "constant_sweep": sweep,
+               "speedup_network_vs_best_constant": best["ms"] / head["ms"]}
 
     # end to end through the host C ABI with pinned buffers
     e2e = None
@@ -513,6 +634,7 @@ def run_ours(args):
         e2e = {"value": whole_job_rate(n, args.steps, 1000.0 * tot, world), "unit": "sources/s",
                "h2d_bytes_per_step": n * 24, "d2h_bytes_per_step": n * k * 12,
                "ms_per_step": 1000.0 * tot / args.steps, "timer": "host wall clock around the call"}
+        del hx, hnn, hd2
 
     cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -522,10 +644,13 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_gpulite:
         assert L.lc_gpu_set_mode(ws, best_mode) == 0
         gpulite = gpulite_leg(args, L, ws, x, n)
+    L.lc_gpu_workspace_free(ws)
+    del x, nn, d2
+    torch.cuda.empty_cache()
+    c3 = None
+    if rank == 0 and world == 1 and not args.no_c3:
+        c3 = c3_block(args, max(5, args.steps // 2), world, flush)
 
-    names = ["pairs", "inserts", "replays", "shells", "pruned", "reranks", "prop_under",
-             "prop_over", "prop_exact", "revisited", "fallback"]
-    walk_stats = {nm: cnt[i] for i, nm in enumerate(names)}  # an untimed step after the timing
     # our kernels per step: fold, scan, slots, records, walk, replay; the learned
     # mode adds the proposal network and the per-source proposal gather
     launches_per_step = 6 + (2 if (best_mode == 2 and model_info is not None) else 0)
@@ -534,48 +659,40 @@ def run_ours(args):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic",
            "config": {"workload": workload_name(n, k), "n": n, "k": k, "cell_hint": 3.0,
-                      "mode": MODE_NAMES[best_mode], "tpp": cnt[-1],
+                      "mode": MODE_NAMES[best_mode], "tpp": head["counters"]["tpp"],
                       "tpp_source": "forced" if args.tpp else "autotuned",
                       "parallelism": f"replicas x{world}",
                       "l2": "flushed between timed steps (256 MB write)"},
            "roofline": roofline, "cpu_baseline": cpu, "gpulite_baseline": gpulite, "e2e": e2e,
            "parity_sample": parity,
-           "gpu_launches": launches_per_step * args.steps, "clocks": sampler.summary(),
-           "plain_fp64": {"value": plain_value, "unit": "sources/s",
-                          "walk_ms": statistics.mean(plain_walk), "tpp": plain_cnt[-1]},
+           "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
+           "plain_fp64": {"value": plain_value, "unit": "sources/s", "walk_ms": plain["walk_ms"],
+                          "tpp": plain["counters"]["tpp"]},
            "speedup_vs_plain": value / plain_value, "walk_ms": walk_avg_ms,
-           "prep_ms": statistics.mean(prep_ms), "replay_ms": statistics.mean(replay_ms),
-           "propose_ms": statistics.mean(prop_ms),
-           "walk_stats_last_step": walk_stats, "model": model_info,
-           "plain_walk_stats_last_step": {nm: plain_cnt[i] for i, nm in enumerate(names)}}
+           "prep_ms": head["prep_ms"], "replay_ms": head["replay_ms"],
+           "propose_ms": head["propose_ms"],
+           "walk_stats_last_step": {nm: head["counters"][nm] for nm in COUNTER_NAMES},
+           "learned_vs_constant": lvc, "c3": c3, "model": model_info,
+           "plain_walk_stats_last_step": {nm: plain["counters"][nm] for nm in COUNTER_NAMES}}
     if rank == 0:
         print(json.dumps(out), flush=True)
-    L.lc_gpu_workspace_free(ws)
     if world > 1:
         torch.distributed.destroy_process_group()
 
 
-def run_c3(args):
-    """C3: 256 frames of their own sheared cells, densities, k in {4, 8, 16, 32}
-    and masks (linkcell_b200.workloads.frames_batch, seed 3) searched by one
-    lc_gpu_knearest_batch call per step, the launch sequence captured once in
-    a CUDA graph and replayed. value = active sources of all frames per
-    second (device time); e2e is the same batch through lc_knearest_batch
-    with host buffers: the copies of the coordinates and mask in and
-    of the rows out."""
+def c3_block(args, steps, world, flush):
+    """The batched-frames configuration: 256 frames of their own sheared
+    cells, densities, k in {4, 8, 16, 32} and masks
+    (linkcell_b200.workloads.frames_batch, seed 3) searched by one
+    lc_gpu_knearest_batch call per step, the launch sequence captured once
+    in a CUDA graph and replayed; value = active sources of all frames per
+    second (device time), beside the plain FP64 walk; e2e is the same batch
+    through lc_knearest_batch with host buffers: the copies of the
+    coordinates and mask in and of the rows out."""
     import torch
-    world, rank, local = dist_env()
-    if world > 1:
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    else:
-        torch.cuda.set_device(0)
-    dev = torch.cuda.current_device()
     from linkcell_b200 import _capi, _cell_struct, learn, workloads as W
-    from linkcell_b200 import build as B
-    B.build()
     L = _capi.load()
+    rank = dist_env()[1]
     frames = W.frames_batch(256, seed=3 + rank)
     arr = (_capi.LcFrame * len(frames))()
     total_out, moff, active = 0, 0, 0
@@ -593,7 +710,6 @@ def run_c3(args):
     m = torch.as_tensor(mask_h, device="cuda")
     nn = torch.empty(total_out, dtype=torch.int32, device="cuda")
     d2 = torch.empty(total_out, dtype=torch.float64, device="cuda")
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     ws = L.lc_gpu_workspace_new()
     assert ws, _capi.gpu_error()
     learn.attach(ws)
@@ -628,15 +744,12 @@ def run_c3(args):
         torch.cuda.synchronize()
         return max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), "cuda")
 
-    sampler = ClockSampler(dev)
-    sampler.start()
-    time.sleep(0.3)
-    plain_ms = time_mode(0, max(3, args.steps // 2))
-    total_ms = time_mode(2, args.steps)
-    sampler.stop()
-    value = whole_job_rate(active, args.steps, total_ms, world)
-    plain_value = whole_job_rate(active, max(3, args.steps // 2), plain_ms, world)
+    plain_ms = time_mode(0, max(3, steps // 2))
+    total_ms = time_mode(2, steps)
+    value = whole_job_rate(active, steps, total_ms, world)
+    plain_value = whole_job_rate(active, max(3, steps // 2), plain_ms, world)
     captures = int(L.lc_gpu_graph_captures(ws))
+    tuned = int(L.lc_gpu_get_tpp(ws))
 
     # end to end through lc_knearest_batch: the same batch from host memory
     # (page-locked), rows back into page-locked buffers, which the library
@@ -653,7 +766,7 @@ def run_c3(args):
         assert rc == 0, _capi.cpu_error()
 
     times = []
-    for i in range(args.warmup + args.steps):
+    for i in range(args.warmup + steps):
         flush.fill_(1)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -662,30 +775,56 @@ def run_c3(args):
             times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(sum(times), "cuda")
     ks = sorted({fr["k"] for fr in frames})
-    out = {"metric": "kNN sources/s, C3: 256 frames of uneven n, cell, k and mask, 1 B200, "
+    out = {"metric": "kNN sources/s, 256 frames of uneven n, cell, k and mask in one call, "
                      "exact indices",
-           "value": value, "unit": "sources/s", "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "c3_256_frames", "frames": len(frames), "points": int(moff),
-                      "active_sources": active, "k": ks, "mode": "learned", "graph": True,
-                      "graph_captures": captures, "parallelism": f"replicas x{world}",
+           "value": value, "unit": "sources/s", "steps": steps, "ms_per_step": total_ms / steps,
+           "config": {"workload": "batched_256_frames_seed3", "frames": len(frames),
+                      "points": int(moff), "active_sources": active, "k": ks, "mode": "learned",
+                      "graph": True, "graph_captures": captures, "tpp": tuned,
                       "l2": "flushed between timed steps (256 MB write)"},
-           "roofline": None, "cpu_baseline": None,
-           "e2e": {"value": whole_job_rate(active, args.steps, 1000.0 * e2e_s, world),
+           "e2e": {"value": whole_job_rate(active, steps, 1000.0 * e2e_s, world),
                    "unit": "sources/s", "h2d_bytes_per_step": int(xyz_h.nbytes + mask_h.nbytes),
                    "d2h_bytes_per_step": int(total_out * 12),
+                   "ms_per_step": 1000.0 * e2e_s / steps,
                    "timer": "host wall clock around lc_knearest_batch with host buffers"},
-           "gpu_launches": None, "clocks": sampler.summary(),
            "plain_fp64": {"value": plain_value, "unit": "sources/s"},
            "speedup_vs_plain": value / plain_value}
-    if rank == 0:
-        print(json.dumps(out), flush=True)
     # the copies above ran on the workspace's stream: release every tensor
     # that recorded it before the stream goes away with the workspace
     torch.cuda.synchronize()
-    del x, m, nn, d2, xh, mh, nnh, d2h, flush
+    del x, m, nn, d2, xh, mh, nnh, d2h
     L.lc_gpu_workspace_free(ws)
+    return out
+
+
+def run_c3(args):
+    """--workload c3: the batched-frames block alone, as its own JSON line."""
+    import torch
+    world, rank, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    from linkcell_b200 import build as B
+    B.build()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    sampler = ClockSampler(dev)
+    sampler.start()
+    time.sleep(0.3)
+    blk = c3_block(args, args.steps, world, flush)
+    sampler.stop()
+    out = {"metric": blk["metric"], "value": blk["value"], "unit": "sources/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": blk["ms_per_step"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "config": {**blk["config"], "parallelism": f"replicas x{world}"},
+           "roofline": None, "cpu_baseline": None, "e2e": blk["e2e"], "gpu_launches": None,
+           "clocks": sampler.summary(), "plain_fp64": blk["plain_fp64"],
+           "speedup_vs_plain": blk["speedup_vs_plain"]}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
 

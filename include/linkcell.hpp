@@ -4,7 +4,13 @@
 #ifndef LINKCELL_HPP
 #define LINKCELL_HPP
 
-#if defined(__cplusplus) && __cplusplus < 201703L && !defined(_MSVC_LANG)
+// MSVC reports __cplusplus as 199711L unless /Zc:__cplusplus is given; its
+// language level is in _MSVC_LANG.
+#if defined(_MSC_VER)
+#if !defined(_MSVC_LANG) || _MSVC_LANG < 201703L
+#error "linkcell.hpp requires C++17 or later"
+#endif
+#elif defined(__cplusplus) && __cplusplus < 201703L
 #error "linkcell.hpp requires C++17 or later"
 #endif
 
@@ -17,6 +23,7 @@ extern "C" {
 #include <limits>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -112,6 +119,20 @@ class Neighbours {
 
 namespace detail {
 
+// The count type of the C ABI, read off lc_knearest's second parameter, so
+// that a header whose counts are narrower than size_t is caught here instead
+// of truncating silently (reference include/linkcell.hpp:144-163).
+template <typename R, typename P0, typename Count, typename... Rest>
+Count count_param(R (*)(P0, Count, Rest...));
+using c_count = decltype(count_param(&lc_knearest));
+static_assert(std::is_integral<c_count>::value, "lc_knearest counts must be an integral type");
+
+inline c_count to_c_count(std::size_t v, const char *what) {
+  if (v > static_cast<std::size_t>(std::numeric_limits<c_count>::max()))
+    throw Error(std::string("linkcell: ") + what + " exceeds the C ABI count range");
+  return static_cast<c_count>(v);
+}
+
 inline void call_c(const double *xyz, std::size_t n, const Cell &cell, std::size_t k, int *out,
                    const int *mask, double cell_hint, double *out_d2 = nullptr,
                    std::size_t n_frames = 1) {
@@ -119,7 +140,8 @@ inline void call_c(const double *xyz, std::size_t n, const Cell &cell, std::size
   if (k == 0) throw Error("k must be at least 1");
   if (xyz == nullptr || out == nullptr) throw Error("null pointer");
   const lc_cell raw = cell.raw();
-  const int status = lc_knearest_many(xyz, n, n_frames, &raw, k, mask, cell_hint, out, out_d2);
+  const int status = lc_knearest_many(xyz, to_c_count(n, "n"), to_c_count(n_frames, "n_frames"),
+                                      &raw, to_c_count(k, "k"), mask, cell_hint, out, out_d2);
   if (status != 0) {
     const char *msg = lc_last_error();
     throw Error(status, msg ? std::string(msg) : std::string("linkcell: knearest failed"));

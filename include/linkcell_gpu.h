@@ -168,6 +168,32 @@ int lc_gpu_stats(lc_gpu_workspace *ws, long long *counters, int n_counters, doub
  * default: the counters cost about 3 % of that walk). */
 int lc_gpu_set_stats(lc_gpu_workspace *ws, int on);
 
+/* Extension (several GPUs, one process each): one rank's share of a search
+ * whose inputs every rank holds. No counterpart in the reference; its split
+ * point is the per-source loop of src/knearest.rs:477-485 (sources are
+ * independent once the points are binned). Arguments as for
+ * lc_gpu_knearest_many (device pointers, shared cell and mask), plus rank in
+ * [0, world). Every rank bins the whole input; the cell-sorted sources are cut
+ * into world contiguous ranges of equal expected work (cell occupancy times
+ * the proposed cube) and this call walks rank's range. out_owned (n * n_frames
+ * device ints) gets nonzero exactly for the rows this call wrote (its
+ * sources, and on rank 0 the -1 / NaN rows of masked points); the other rows
+ * of out_nn / out_d2 are left as they were. Zeroing the rows a rank does not
+ * own and summing over the ranks (one all-reduce) gives the full rows. */
+int lc_gpu_knearest_shard(lc_gpu_workspace *ws, const double *xyz, size_t n, size_t n_frames,
+                          const struct lc_cell *simbox, size_t k, const int *mask,
+                          double cell_hint, int rank, int world, int *out_nn, double *out_d2,
+                          int *out_owned, int wait);
+
+/* Extension, for failure-detection tests: the cell-count scan's look-back
+ * waits at most spins loads (spins <= 0: the default bound), and the scan
+ * tile silent_tile (-1: none) never publishes its state, so that the next
+ * tile's wait runs out. A wait that runs out still yields exact offsets (the
+ * tile sums its prefix from the counts) and the search then fails with
+ * "device search failed" when it is waited for. No counterpart in the
+ * reference, whose prefix scan does not wait across blocks. */
+int lc_gpu_set_scan_limit(lc_gpu_workspace *ws, int spins, long long silent_tile);
+
 /* Device time of the last search's phases, from CUDA events on the
  * workspace stream: fold + bin + scan + placement, the walk kernel, and the
  * exact replay of tied sources. Waits for the search to finish. */
@@ -224,10 +250,14 @@ int lc_knearest_batch(const double *xyz, const lc_frame *frames, size_t n_frames
  * a host lc_cell. Limits: n <= 65536 points, at most 65536 linked cells,
  * k <= 64; larger searches fail with an error. Work is enqueued on stream
  * (a cudaStream_t, NULL for the legacy default stream); wait != 0 also
- * waits and checks the device status. The first call on a device looks up
- * the array's device address. All calls share the array and leave their
- * contents in it: calls that overlap on the GPU race and must not be
- * issued. Results equal lc_gpu_knearest's. */
+ * waits and checks the device status. Every call looks up the array's
+ * device address on the current device; the first call on a device also
+ * loads the library's kernels there, so it should come before any stream
+ * capture. With a mask, a mesh past the limits is an error only when some
+ * point is active; an all-masked search returns -1 / NaN rows, as the
+ * reference does, and the call then waits for its check of the mask. All
+ * calls share the array and leave their contents in it: calls that overlap
+ * on the GPU race and must not be issued. Results equal lc_gpu_knearest's. */
 int lc_gpu_knearest_noalloc(const double *xyz, size_t n, const struct lc_cell *simbox, size_t k,
                             const int *mask, double cell_hint, int *out_nn, double *out_d2,
                             void *stream, int wait);

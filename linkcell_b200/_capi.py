@@ -35,12 +35,13 @@ EXPORTS = (
     "lc_gpu_wait", "lc_gpu_alloc", "lc_gpu_free", "lc_gpu_fill_i32", "lc_gpu_memcpy",
     "lc_gpu_set_mode", "lc_gpu_get_mode", "lc_gpu_set_proposal", "lc_gpu_set_tpp",
     "lc_gpu_get_tpp", "lc_gpu_set_graph", "lc_gpu_graph_captures", "lc_gpu_set_stream", "lc_gpu_stats",
-    "lc_gpu_set_stats",
+    "lc_gpu_set_stats", "lc_gpu_set_scan_limit",
     "lc_gpu_phase_times", "lc_gpu_phase_times4", "lc_gpu_neighbors_within", "lc_gpu_set_model", "lc_gpu_log_shells", "lc_gpu_training_rows",
     "lc_gpu_proposals",
     "lc_gpu_mlp_params", "lc_gpu_mlp_scratch_floats", "lc_gpu_mlp_forward", "lc_gpu_mlp_grad",
     "lc_gpu_mlp_adam",
     "lc_gpu_knearest_batch", "lc_gpu_knearest_noalloc", "lc_knearest_batch",
+    "lc_gpu_knearest_shard",
 )
 
 _lib = None
@@ -92,6 +93,7 @@ def load():
     L.lc_gpu_set_graph.argtypes = [vp, i]
     L.lc_gpu_graph_captures.argtypes = [vp]
     L.lc_gpu_set_stats.argtypes = [vp, i]
+    L.lc_gpu_set_scan_limit.argtypes = [vp, i, ctypes.c_longlong]
     L.lc_gpu_set_stream.argtypes = [vp, vp]
     L.lc_gpu_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), i, dp]
     L.lc_gpu_phase_times.argtypes = [vp, dp, dp, dp]
@@ -115,6 +117,7 @@ def load():
     L.lc_gpu_knearest_batch.argtypes = [vp, vp, ctypes.POINTER(LcFrame), sz, vp, vp, vp, i]
     L.lc_knearest_batch.argtypes = [vp, ctypes.POINTER(LcFrame), sz, vp, vp, vp]
     L.lc_gpu_knearest_noalloc.argtypes = [vp, sz, cp, sz, vp, d, vp, vp, vp, i]
+    L.lc_gpu_knearest_shard.argtypes = [vp, vp, sz, sz, cp, sz, vp, d, i, i, vp, vp, vp, i]
     _lib = L
     return L
 

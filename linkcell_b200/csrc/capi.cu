@@ -247,24 +247,6 @@ namespace {
   throw Error(m);
 }
 
-// All-masked batch: only the -1 / NaN fill (src/knearest.rs:293-296,370-375).
-bool device_mask_all_zero(const int *mask, std::size_t n, cudaStream_t s) {
-  std::vector<int> h(n);
-  cudaMemcpyAsync(h.data(), mask, n * sizeof(int), cudaMemcpyDeviceToHost, s);
-  cudaStreamSynchronize(s);
-  for (int v : h)
-    if (v != 0) return false;
-  return true;
-}
-
-void fill_device_outputs(int *out, double *out_d2, std::size_t need, cudaStream_t s) {
-  cudaMemsetAsync(out, 0xFF, need * sizeof(int), s);
-  if (out_d2) {
-    std::vector<double> nan(need, std::numeric_limits<double>::quiet_NaN());
-    cudaMemcpyAsync(out_d2, nan.data(), need * sizeof(double), cudaMemcpyHostToDevice, s);
-    cudaStreamSynchronize(s);
-  }
-}
 }  // namespace
 
 void Workspace::wait() {
@@ -309,8 +291,12 @@ void Workspace::knearest_into_many(const double *xyz, std::size_t n, std::size_t
   if (check_cell(raw) != Code::Ok) throw Error("bad cell");
   std::vector<FrameDesc> frames;
   Code pc = shared_frames(raw, n, nFrames, k, mask != nullptr, cell_hint, frames);
-  if (pc == Code::TooFine && mask && device_mask_all_zero(mask, n, impl_->ws.stream())) {
-    fill_device_outputs(out, out_d2, out_len, impl_->ws.stream());
+  if (pc == Code::TooFine && mask) {
+    // all-masked: -1 / NaN rows (src/knearest.rs:370-375), checked on the device
+    std::string detail;
+    const Code c = impl_->ws.too_fine_masked(mask, (long long)n, out, out_d2, (long long)out_len,
+                                             wait, detail);
+    if (c != Code::Ok) throw_code(c, detail);
     return;
   }
   if (pc != Code::Ok) throw_code(pc, "");
@@ -465,26 +451,55 @@ int lc_gpu_knearest_many(lc_gpu_workspace *ws, const double *xyz, size_t n, size
   const Code pc = shared_frames(*simbox, n, n_frames, k, mask != nullptr, cell_hint, frames);
   const size_t need = n * n_frames * k;
   if (pc == Code::TooFine && mask) {
-    std::vector<int> h(n);
-    const cudaStream_t s = ws->ws.stream();
-    cudaMemcpyAsync(h.data(), mask, n * sizeof(int), cudaMemcpyDeviceToHost, s);
-    cudaStreamSynchronize(s);
-    bool any = false;
-    for (int v : h) any = any || v != 0;
-    if (!any) {
-      cudaMemsetAsync(out_nn, 0xFF, need * sizeof(int), s);
-      if (out_d2) {
-        std::vector<double> nan(need, std::numeric_limits<double>::quiet_NaN());
-        cudaMemcpyAsync(out_d2, nan.data(), need * sizeof(double), cudaMemcpyHostToDevice, s);
-      }
-      cudaStreamSynchronize(s);
-      gpu_ok();
-      return 0;
-    }
+    // all-masked: -1 / NaN rows (src/knearest.rs:370-375), checked on the device
+    std::string detail;
+    const Code c = ws->ws.too_fine_masked(mask, (long long)n, out_nn, out_d2, (long long)need,
+                                          wait != 0, detail);
+    if (c != Code::Ok) return gpu_fail(c, detail);
+    gpu_ok();
+    return 0;
   }
   if (pc != Code::Ok) return gpu_fail(pc);
   std::string detail;
   const Code rc = ws->ws.run(frames, xyz, mask, out_nn, out_d2, wait != 0, detail);
+  if (rc != Code::Ok) return gpu_fail(rc, detail);
+  gpu_ok();
+  return 0;
+}
+
+int lc_gpu_knearest_shard(lc_gpu_workspace *ws, const double *xyz, size_t n, size_t n_frames,
+                          const lc_cell *simbox, size_t k, const int *mask, double cell_hint,
+                          int rank, int world, int *out_nn, double *out_d2, int *out_owned,
+                          int wait) {
+  if (!ws || !xyz || !simbox || !out_nn || !out_owned) return gpu_fail(Code::NullPointer);
+  if (n == 0 || n_frames == 0) return gpu_fail(Code::NoPoints);
+  if (k == 0) return gpu_fail(Code::ZeroK);
+  if (world < 1 || rank < 0 || rank >= world) return gpu_fail_msg("rank must lie in [0, world)");
+  const size_t smax = std::numeric_limits<size_t>::max();
+  if (n > smax / n_frames || n * n_frames > smax / k) return gpu_fail(Code::Overflow);
+  if (check_cell(*simbox) != Code::Ok) return gpu_fail(Code::BadCell);
+  std::vector<FrameDesc> frames;
+  const Code pc = shared_frames(*simbox, n, n_frames, k, mask != nullptr, cell_hint, frames);
+  const size_t need = n * n_frames * k;
+  std::string detail;
+  if (pc == Code::TooFine && mask) {
+    // all-masked: -1 / NaN rows on every rank, owned by rank 0
+    const Code c = ws->ws.too_fine_masked(mask, (long long)n, out_nn, out_d2, (long long)need,
+                                          false, detail);
+    if (c != Code::Ok) return gpu_fail(c, detail);
+    const cudaError_t e = cudaMemsetAsync(out_owned, rank == 0 ? 1 : 0,
+                                          n * n_frames * sizeof(int), ws->ws.stream());
+    if (e != cudaSuccess) return gpu_fail(Code::Cuda, cudaGetErrorString(e));
+    if (wait) {
+      const Code w = ws->ws.wait(detail);
+      if (w != Code::Ok) return gpu_fail(w, detail);
+    }
+    gpu_ok();
+    return 0;
+  }
+  if (pc != Code::Ok) return gpu_fail(pc);
+  const Code rc = ws->ws.run_shard(frames, xyz, mask, out_nn, out_d2, out_owned, rank, world,
+                                   wait != 0, detail);
   if (rc != Code::Ok) return gpu_fail(rc, detail);
   gpu_ok();
   return 0;
@@ -609,6 +624,13 @@ int lc_gpu_graph_captures(lc_gpu_workspace *ws) { return ws ? ws->ws.graph_captu
 int lc_gpu_set_stats(lc_gpu_workspace *ws, int on) {
   if (!ws) return gpu_fail(Code::NullPointer);
   ws->ws.opts.stats = on != 0;
+  return 0;
+}
+
+int lc_gpu_set_scan_limit(lc_gpu_workspace *ws, int spins, long long silent_tile) {
+  if (!ws) return gpu_fail(Code::NullPointer);
+  ws->ws.opts.scan_spin_limit = spins > 0 ? spins : 0;
+  ws->ws.opts.scan_silent_tile = silent_tile >= 0 ? silent_tile : -1;
   return 0;
 }
 

@@ -90,7 +90,12 @@ __global__ void __launch_bounds__(256)
 // Single-pass exclusive scan with decoupled look-back (Merrill & Garland).
 // Tile ids come from an atomic counter in launch order, so a tile only ever
 // waits on tiles that have already started; every wait is still bounded
-// and reports kStatusScanTimeout instead of hanging.
+// (spin_limit loads, kSpinLimit when it is 0) and reports kStatusScanTimeout
+// instead of hanging. A tile whose wait runs out sums its exclusive prefix
+// straight from the counts of the cells before it, so the offsets stay right
+// and no later kernel reads past its buffers. silent_tile >= 0 keeps that
+// tile from publishing its state, so that its successor's wait runs out: a
+// failure-detection test hook (lc_gpu_set_scan_limit), -1 in searches.
 constexpr unsigned long long kFlagA = 1ull << 62;  // aggregate published
 constexpr unsigned long long kFlagP = 2ull << 62;  // inclusive prefix published
 constexpr unsigned long long kValMask = (1ull << 62) - 1;
@@ -113,7 +118,9 @@ __device__ __forceinline__ void store_release(unsigned long long *p, unsigned lo
 __global__ void __launch_bounds__(kScanBlock)
     k_scan_cells(const uint32_t *__restrict__ count, uint32_t *__restrict__ off, long long ncells,
                  const long long *__restrict__ live, unsigned long long *__restrict__ tile_state,
-                 uint32_t *__restrict__ tile_counter, int *__restrict__ status) {
+                 uint32_t *__restrict__ tile_counter, int *__restrict__ status, int spin_limit,
+                 long long silent_tile) {
+  const int limit = spin_limit > 0 ? spin_limit : kSpinLimit;
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kScanBlock / 32];
   __shared__ unsigned long long s_excl;
@@ -164,7 +171,8 @@ __global__ void __launch_bounds__(kScanBlock)
 
     if (warp == 0) {
       // publish this tile's aggregate, then look back 32 predecessors at a time
-      if (lane == 0) store_release(&tile_state[tile], (tile == 0 ? kFlagP : kFlagA) | agg);
+      const bool publish = tile != silent_tile;
+      if (lane == 0 && publish) store_release(&tile_state[tile], (tile == 0 ? kFlagP : kFlagA) | agg);
       unsigned long long excl = 0;
       if (tile > 0) {
         long long end = tile;  // predecessors [end-32, end)
@@ -175,7 +183,7 @@ __global__ void __launch_bounds__(kScanBlock)
           if (t >= 0) {
             int spins = 0;
             w = load_acquire(&tile_state[t]);
-            while ((w >> 62) == 0 && spins < kSpinLimit) {
+            while ((w >> 62) == 0 && spins < limit) {
               ++spins;
               w = load_acquire(&tile_state[t]);
             }
@@ -194,8 +202,17 @@ __global__ void __launch_bounds__(kScanBlock)
           if (pm) done = true;
           end -= 32;
         }
-        if (timeout && lane == 0) atomicOr(status, kStatusScanTimeout);
-        if (lane == 0) store_release(&tile_state[tile], kFlagP | ((excl + agg) & kValMask));
+        if (timeout) {
+          // the counts are final (the histogram kernel has finished): sum them
+          unsigned long long sum = 0;
+          for (long long c = lane; c < tile * kScanTile; c += 32) sum += count[c];
+#pragma unroll
+          for (int d = 16; d > 0; d >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, d);
+          excl = sum;
+          if (lane == 0) atomicOr(status, kStatusScanTimeout);
+        }
+        if (lane == 0 && publish)
+          store_release(&tile_state[tile], kFlagP | ((excl + agg) & kValMask));
       }
       if (lane == 0) s_excl = excl;
     }
@@ -364,6 +381,26 @@ __global__ void k_count_active(const int *__restrict__ mask, long long n,
   if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, local);
 }
 
+// The rows of a search whose mesh is too fine, after k_count_active: with
+// no active point every slot becomes -1 / NaN, as the reference fills the
+// rows before it returns for an all-masked search (src/knearest.rs:293-296,
+// 370-375); otherwise the status word gets kStatusPlanTooFine and nothing
+// is written.
+__global__ void k_fill_if_inactive(const unsigned long long *__restrict__ active,
+                                   int *__restrict__ out_nn, double *__restrict__ out_d2,
+                                   long long need, int *__restrict__ status) {
+  if (*active != 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status, kStatusPlanTooFine);
+    return;
+  }
+  const double nan = __longlong_as_double(0x7ff8000000000000ll);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < need;
+       i += (long long)gridDim.x * blockDim.x) {
+    out_nn[i] = -1;
+    if (out_d2) out_d2[i] = nan;
+  }
+}
+
 int grid_for(long long n, int block) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -394,7 +431,8 @@ cudaError_t launch_scan(const BatchBuffers &b, cudaStream_t s) {
     grid = std::min<long long>(grid, (long long)sms * 4);
   }
   k_scan_cells<<<unsigned(grid), kScanBlock, 0, s>>>(b.count, b.off, b.ncells, b.live_cells,
-                                                      b.tile_state, b.tile_counter, b.status);
+                                                      b.tile_state, b.tile_counter, b.status,
+                                                      b.scan_spin_limit, b.scan_silent_tile);
   return cudaGetLastError();
 }
 
@@ -418,6 +456,16 @@ cudaError_t launch_place(const BatchBuffers &b, cudaStream_t s) {
 cudaError_t launch_count_active(const int *mask, long long n, unsigned long long *out,
                                 cudaStream_t s) {
   k_count_active<<<grid_for(n, 256), 256, 0, s>>>(mask, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_masked_too_fine(const int *mask, long long n, unsigned long long *active,
+                                   int *out_nn, double *out_d2, long long need, int *status,
+                                   cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(active, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  if ((e = launch_count_active(mask, n, active, s)) != cudaSuccess) return e;
+  k_fill_if_inactive<<<grid_for(need, 256), 256, 0, s>>>(active, out_nn, out_d2, need, status);
   return cudaGetLastError();
 }
 

@@ -2006,7 +2006,103 @@ __global__ void __launch_bounds__(kPartBlock)
     __syncthreads();
   }
 }
+
+// ---- a search split across ranks (one process per GPU, inputs replicated)
+// Expected work of sorted source p: its cell's occupancy times its proposed
+// cube in units of the 3x3x3 cube (shell 2 without a proposal), plus one,
+// capped so that the prefix over all sources fits 32 bits; zero past the
+// active sources.
+__global__ void k_shard_weights(BatchBuffers b, uint32_t *__restrict__ w, uint32_t cap) {
+  const long long total = b.off[b.ncells];
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < b.npts;
+       p += (long long)gridDim.x * blockDim.x) {
+    uint32_t v = 0;
+    if (p < total) {
+      const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
+      const long long c = b.frames[f].cell_base + (long long)b.scell[p];
+      const uint32_t occ = min(b.off[c + 1] - b.off[c], 64u);
+      int R = b.proposal ? int(b.proposal[p]) : 2;
+      R = R <= 0 ? 2 : min(R, 8);
+      const uint32_t cube = uint32_t((2 * R + 1) * (2 * R + 1) * (2 * R + 1));
+      v = 1u + min(cap - 1u, occ * cube / 27u);
+    }
+    w[p] = v;
+  }
+}
+
+// cut = this rank's [lo, hi): lo is the first sorted position whose prefix
+// weight reaches rank / world of the total (hi likewise for rank + 1), so
+// consecutive ranks' ranges meet and together cover every active source.
+__global__ void k_shard_cut(BatchBuffers b, const uint32_t *__restrict__ pre, int rank, int world,
+                            uint32_t *__restrict__ cut) {
+  if (threadIdx.x > 1) return;
+  const long long total = b.off[b.ncells];
+  const unsigned long long W = pre[b.npts];
+  const int r = rank + int(threadIdx.x);
+  if (r >= world) {
+    cut[1] = uint32_t(total);
+    return;
+  }
+  const unsigned long long target = W * (unsigned long long)r / (unsigned long long)world;
+  long long lo = 0, hi = total;  // first p in [0, total] with pre[p] >= target
+  while (lo < hi) {
+    const long long mid = (lo + hi) >> 1;
+    if ((unsigned long long)pre[mid] >= target)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  cut[threadIdx.x] = uint32_t(lo);
+}
+
+__global__ void k_shard_owned(BatchBuffers b, const uint32_t *__restrict__ cut, int rank,
+                              int *__restrict__ owned) {
+  const long long lo = cut[0], hi = cut[1];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long p = lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < hi; p += stride) {
+    const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
+    owned[b.frames[f].pt_base + b.sidx[p]] = 1;
+  }
+  if (rank == 0)
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < b.npts; i += stride)
+      if (b.cell_of[i] == kInactive) owned[i] = 1;
+}
 }  // namespace
+
+cudaError_t launch_shard_split(const BatchBuffers &b, int rank, int world, uint32_t *w,
+                               uint32_t *pre, unsigned long long *tile_state,
+                               uint32_t *tile_counter, uint32_t *cut, cudaStream_t s) {
+  if (world < 1 || rank < 0 || rank >= world || b.npts <= 0) return cudaErrorInvalidValue;
+  const unsigned long long per = 0xFFFFFFFFull / (unsigned long long)b.npts;
+  const uint32_t cap = uint32_t(per < 1 ? 1 : (per > 64 ? 64 : per));
+  const int g = int(std::min<long long>((b.npts + 255) / 256, (long long)sm_count() * 8));
+  k_shard_weights<<<g, 256, 0, s>>>(b, w, cap);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  BatchBuffers sb;  // prefix of the weights over the sorted positions
+  sb.count = w;
+  sb.off = pre;
+  sb.ncells = b.npts;
+  sb.tile_state = tile_state;
+  sb.tile_counter = tile_counter;
+  sb.status = b.status;
+  if ((e = cudaMemsetAsync(tile_state, 0, size_t(scan_tiles(sb.ncells)) * sizeof(unsigned long long),
+                           s)) != cudaSuccess ||
+      (e = cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), s)) != cudaSuccess)
+    return e;
+  if ((e = launch_scan(sb, s)) != cudaSuccess) return e;
+  k_shard_cut<<<1, 32, 0, s>>>(b, pre, rank, world, cut);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shard_owned(const BatchBuffers &b, const uint32_t *cut, int rank, int *owned,
+                               cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(owned, 0, size_t(b.npts) * sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  const int g = int(std::min<long long>((b.npts + 255) / 256, (long long)sm_count() * 8));
+  k_shard_owned<<<g, 256, 0, s>>>(b, cut, rank, owned);
+  return cudaGetLastError();
+}
 
 long long range_partition_blocks(long long sources) {
   const long long per = (long long)kPartBlock * kPartItems;

@@ -54,17 +54,24 @@ struct BatchBuffers {
   int shell_rmax = 0;
   // optional source order: when set, the walk visits sorted positions
   // src_order[*src_lo .. *src_hi) instead of all of them (the bounds are
-  // device values, written by the kernels that built the order)
+  // device values, written by the kernels that built the order); with
+  // src_lo / src_hi but no src_order, the sorted positions *src_lo ..
+  // *src_hi themselves (one rank's share of a split search)
   const int *src_order = nullptr;
   const uint32_t *src_lo = nullptr, *src_hi = nullptr;
+  // scan look-back: loads a wait may take (0: the default bound) and a tile
+  // that never publishes (-1: none); failure-detection tests only
+  int scan_spin_limit = 0;
+  long long scan_silent_tile = -1;
 };
 
 // Sources a walk launch visits, and the sorted position of the q-th.
 __device__ __forceinline__ long long walk_sources(const BatchBuffers &b) {
-  return b.src_order ? (long long)*b.src_hi - (long long)*b.src_lo : (long long)b.off[b.ncells];
+  return b.src_lo ? (long long)*b.src_hi - (long long)*b.src_lo : (long long)b.off[b.ncells];
 }
 __device__ __forceinline__ long long walk_source_at(const BatchBuffers &b, long long q) {
-  return b.src_order ? (long long)b.src_order[*b.src_lo + q] : q;
+  return b.src_order ? (long long)b.src_order[*b.src_lo + q]
+                     : (b.src_lo ? (long long)*b.src_lo + q : q);
 }
 
 // Walk statistics accumulated on the device (counters[...]).
@@ -139,6 +146,19 @@ long long range_partition_blocks(long long sources);
 cudaError_t launch_range_partition(const BatchBuffers &b, const RowCuts &cuts, uint32_t *cnt,
                                    uint32_t *off, unsigned long long *tile_state,
                                    uint32_t *tile_counter, int *order, cudaStream_t s);
+// One rank's share of a search split across ranks that hold the same
+// inputs: the sorted sources are cut into world contiguous ranges of equal
+// expected work (weight of a source: its cell's occupancy times its proposed
+// cube, plus one), and cut[0], cut[1] get rank's range. w (npts words), pre
+// (npts + 1), tile_state (scan tiles of npts) and tile_counter are scratch.
+cudaError_t launch_shard_split(const BatchBuffers &b, int rank, int world, uint32_t *w,
+                               uint32_t *pre, unsigned long long *tile_state,
+                               uint32_t *tile_counter, uint32_t *cut, cudaStream_t s);
+// owned[i] = 1 for every point whose row this rank wrote: its sources in
+// [cut[0], cut[1]), and on rank 0 every masked point (-1 / NaN rows on every
+// rank). owned has npts entries, zeroed here.
+cudaError_t launch_shard_owned(const BatchBuffers &b, const uint32_t *cut, int rank, int *owned,
+                               cudaStream_t s);
 // CSR of the entries within a cutoff of n x k rows (sorted ascending, -1 /
 // NaN padded): counts and row_off are rows + 1 scratch words, tile_state /
 // tile_counter the scan's scratch; row_ptr gets rows + 1 offsets, col /
@@ -156,5 +176,11 @@ cudaError_t walk_prepare(int mode, int kmax, int block);  // sets the dynamic sm
 // Counts active points (used to tell an all-masked batch from a bad mesh).
 cudaError_t launch_count_active(const int *mask, long long n, unsigned long long *out,
                                 cudaStream_t s);
+// A mesh too fine for the bin caps with a length-n mask: counts the active
+// points into *active; none: the need output slots become -1 / NaN; some:
+// kStatusPlanTooFine goes into *status (which the caller zeroed).
+cudaError_t launch_masked_too_fine(const int *mask, long long n, unsigned long long *active,
+                                   int *out_nn, double *out_d2, long long need, int *status,
+                                   cudaStream_t s);
 
 }  // namespace lc

@@ -17,16 +17,18 @@
 // overlap on the GPU (on different streams, or from different host threads
 // without ordering) race and must not be issued.
 //
-// The first call on a device, with that device current, looks up the
-// array's device address with cudaGetSymbolAddress (the array's name in host
-// code only stands in for the symbol; it is not a device pointer) and keeps
-// it for later calls on that device.
+// Every call, with the caller's device current, looks up the array's device
+// address with cudaGetSymbolAddress (the array's name in host code only
+// stands in for the symbol; it is not a device pointer). The first call on a
+// device also loads this library's kernels there (that is its set-up), so it
+// should come before any stream capture. Looking the address up again on
+// every call keeps it right after a cudaDeviceReset, which gives the array a
+// new context.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstring>
 #include <limits>
-#include <mutex>
 
 #include "../../include/linkcell_gpu.h"
 #include "lc_kernels.h"
@@ -59,7 +61,9 @@ constexpr Layout make_layout() {
   const size_t tiles = (C + lc::kScanTile - 1) / lc::kScanTile;
   l.frame = o; o += align256(sizeof(lc::FrameDesc));
   l.counters = o; o += align256(sizeof(long long) * lc::kNumCounters);
-  l.small = o; o += align256(8 * sizeof(uint32_t));  // tile counter, work, replay count, status, frame flags
+  // tile counter, work, replay count, status, frame flags; words 6-7: the
+  // active-point count of a masked search on a too-fine mesh
+  l.small = o; o += align256(8 * sizeof(uint32_t));
   l.cell_of = o; o += align256(P * 4);
   l.arank = o; o += align256(P * 4);
   l.tmp = o; o += align256(P * 8);
@@ -84,25 +88,12 @@ constexpr Layout kLayout = make_layout();
 // About 5.1 MB per device.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kLayout.total];
 
-std::mutex g_setup_mutex;
-constexpr int kMaxDevices = 64;
-unsigned char *g_scratch_addr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device (looked up
-// once per device).
+// Device address of the scratch array in the current device's context.
 cudaError_t scratch_base(unsigned char **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch_addr[dev] = static_cast<unsigned char *>(p);
-  }
-  *out = g_scratch_addr[dev];
+  *out = static_cast<unsigned char *>(p);
   return cudaSuccess;
 }
 
@@ -132,15 +123,12 @@ extern "C" int lc_gpu_knearest_noalloc(const double *xyz, size_t n, const struct
   lc::FrameDesc fd;
   const lc::Code pc = lc::plan_frame(rows, origin, cell_hint, int(k), fd);
   if (pc == lc::Code::BadCell) return fail("bad cell");
-  if (pc == lc::Code::TooFine) return fail("too many cells");
-  const long long ncells = (long long)fd.nx * fd.ny * fd.nz;
-  if (ncells > kNoAllocMaxCells) return fail("no-alloc search supports at most 65536 cells");
-  fd.n = (long long)n;
-  fd.has_mask = mask ? 1 : 0;
-  fd.mask_base = 0;
-  fd.out_base = 0;
-  fd.pt_base = 0;
-  fd.cell_base = 0;
+  const long long ncells = pc == lc::Code::Ok ? (long long)fd.nx * fd.ny * fd.nz : 0;
+  const char *mesh_error = pc == lc::Code::TooFine ? "too many cells"
+                           : ncells > kNoAllocMaxCells
+                               ? "no-alloc search supports at most 65536 cells"
+                               : nullptr;
+  if (mesh_error && !mask) return fail(mesh_error);
 
   unsigned char *base = nullptr;
   cudaError_t e = scratch_base(&base);
@@ -148,6 +136,31 @@ extern "C" int lc_gpu_knearest_noalloc(const double *xyz, size_t n, const struct
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   const Layout &L = kLayout;
   uint32_t *small = reinterpret_cast<uint32_t *>(base + L.small);
+
+  if (mesh_error) {
+    // The reference returns -1 / NaN rows for an all-masked search before it
+    // sizes the mesh (src/knearest.rs:370-375): the mask is checked on the
+    // device, and this call waits for that check whatever wait says.
+    int *status = reinterpret_cast<int *>(small + 3);
+    unsigned long long *active = reinterpret_cast<unsigned long long *>(small + 6);
+    int st = 0;
+    if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) != cudaSuccess ||
+        (e = lc::launch_masked_too_fine(mask, (long long)n, active, out_nn, out_d2,
+                                        (long long)(n * k), status, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, s)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+      return fail_cuda(e);
+    if (st != 0) return fail(mesh_error);
+    lc::set_gpu_error_message(nullptr);
+    return 0;
+  }
+  fd.n = (long long)n;
+  fd.has_mask = mask ? 1 : 0;
+  fd.mask_base = 0;
+  fd.out_base = 0;
+  fd.pt_base = 0;
+  fd.cell_base = 0;
 
   lc::BatchBuffers b;
   b.xyz = xyz;

@@ -158,7 +158,7 @@ void WorkspaceImpl::release_all() {
   rel(replay_d_); rel(rec_); rel(frames_); rel(counters_); rel(h_xyz_); rel(h_d2_);
   rel(h_mask_); rel(h_nn_); rel(active_); rel(proposal_); rel(cell_prop_); rel(stop_log_);
   rel(order_); rel(csr_counts_); rel(csr_off_); rel(live_); rel(part_cnt_); rel(part_off_);
-  rel(part_tiles_);
+  rel(part_tiles_); rel(shard_cut_);
   rel(model_); rel(shell_table_);
   shell_table_ready_ = false;
 }
@@ -305,6 +305,8 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   b.shell_rmax = kShellTableRmax;
   b.stop_log = opts.log_shells ? stop_log_.p : nullptr;
   b.proposal = learned ? proposal_.p : nullptr;
+  b.scan_spin_limit = opts.scan_spin_limit;
+  b.scan_silent_tile = opts.scan_silent_tile;
 
   // ---- 3. walk configuration: overrides, else the autotuned choice
   WalkLaunch wl;
@@ -362,7 +364,8 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
                        wl.block, has_model_ ? 1 : 0, opts.fixed_proposal, opts.log_shells,
                        opts.stats ? 1 : 0, dcell_.on ? dcell_.cell : nullptr,
                        dcell_.on ? dcell_.cell_n : 0,
-                       dcell_.on ? dcell_.hint : 0.0};
+                       dcell_.on ? dcell_.hint : 0.0, opts.scan_spin_limit,
+                       opts.scan_silent_tile};
     if (!graph_exec_ || !(key == graph_key_)) {
       if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
       graph_exec_ = nullptr;
@@ -410,6 +413,61 @@ Code WorkspaceImpl::read_status(std::string &detail) {
     detail = "device status " + std::to_string(st);
     return Code::DeviceStatus;
   }
+  return Code::Ok;
+}
+
+Code WorkspaceImpl::too_fine_masked(const int *mask, long long n, int *out_nn, double *out_d2,
+                                    long long need, bool wait, std::string &detail) {
+  const cudaStream_t s = stream();
+  if (done_pending_) {
+    LC_TRY(cudaEventSynchronize(ev_done_));
+    done_pending_ = false;
+  }
+  LC_TRY(grow(active_, 1));
+  LC_TRY(grow(status_, 1));
+  LC_TRY(cudaMemsetAsync(status_.p, 0, sizeof(int), s));
+  LC_TRY(launch_masked_too_fine(mask, n, active_.p, out_nn, out_d2, need, status_.p, s));
+  LC_TRY(cudaEventRecord(ev_done_, s));
+  last_stream_ = s;
+  done_pending_ = true;
+  if (!wait) return Code::Ok;
+  LC_TRY(cudaStreamSynchronize(s));
+  done_pending_ = false;
+  return read_status(detail);
+}
+
+Code WorkspaceImpl::run_shard(std::vector<FrameDesc> &frames, const double *xyz, const int *mask,
+                              int *out_nn, double *out_d2, int *owned, int rank, int world,
+                              bool wait, std::string &detail) {
+  if (world < 1 || rank < 0 || rank >= world || !owned) return Code::NullPointer;
+  long long P = 0;
+  for (const auto &fd : frames) P += fd.n;
+  LC_TRY(grow(part_cnt_, size_t(P)));
+  LC_TRY(grow(part_off_, size_t(P) + 1));
+  LC_TRY(grow(part_tiles_, size_t(scan_tiles(P))));
+  LC_TRY(grow(shard_cut_, 2));
+  const bool graph = opts.graph;
+  opts.graph = false;
+  shard_ = Shard{true, rank, world, owned};
+  const Code c = run(frames, xyz, mask, out_nn, out_d2, wait, detail);
+  shard_ = Shard();
+  opts.graph = graph;
+  return c;
+}
+
+Code WorkspaceImpl::walk_shard(BatchBuffers &b, const WalkLaunch &wl, cudaStream_t s, bool timed,
+                               std::string &detail) {
+  LC_TRY(launch_shard_split(b, shard_.rank, shard_.world, part_cnt_.p, part_off_.p, part_tiles_.p,
+                            tile_counter_.p, shard_cut_.p, s));
+  if (timed) LC_TRY(cudaEventRecord(ev_[4], s));
+  BatchBuffers br = b;
+  br.src_lo = shard_cut_.p;
+  br.src_hi = shard_cut_.p + 1;
+  LC_TRY(launch_walk(br, wl, s));
+  if (timed) LC_TRY(cudaEventRecord(ev_[2], s));
+  LC_TRY(launch_replay(br, s));
+  LC_TRY(launch_shard_owned(b, shard_cut_.p, shard_.rank, shard_.owned, s));
+  if (timed) LC_TRY(cudaEventRecord(ev_[3], s));
   return Code::Ok;
 }
 
@@ -470,6 +528,7 @@ Code WorkspaceImpl::enqueue(BatchBuffers &b, const WalkLaunch &wl, int nf, size_
     }
   }
   if (pipe_.on && !pipe_.done) return walk_in_row_ranges(b, wl, s, timed, detail);
+  if (shard_.on) return walk_shard(b, wl, s, timed, detail);
   if (timed) LC_TRY(cudaEventRecord(ev_[4], s));
   LC_TRY(launch_walk(b, wl, s));
   if (timed) LC_TRY(cudaEventRecord(ev_[2], s));

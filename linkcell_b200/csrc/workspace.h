@@ -66,6 +66,10 @@ struct WalkOptions {
   bool autotune = true;    // time the walk designs on the first batch of each kind
   bool graph = false;      // capture the launch sequence in a CUDA graph and replay it
   bool stats = false;      // the learned select walk counts its statistics (lc_gpu_stats)
+  // failure-detection tests (lc_gpu_set_scan_limit): the scan's wait bound
+  // (0: default) and a scan tile that never publishes (-1: none)
+  int scan_spin_limit = 0;
+  long long scan_silent_tile = -1;
 };
 
 struct Stats {
@@ -94,6 +98,14 @@ class WorkspaceImpl {
   Code run(std::vector<FrameDesc> &frames, const double *xyz, const int *mask, int *out_nn,
            double *out_d2, bool wait, std::string &detail);
 
+  // A mesh too fine for the bin caps with a length-n device mask. The
+  // reference returns -1 / NaN rows for an all-masked search before it sizes
+  // the mesh (src/knearest.rs:370-375), so the mask is checked on the device:
+  // no active point fills the need output slots; any active point reports
+  // TooFine when the call waits (else at the next wait()).
+  Code too_fine_masked(const int *mask, long long n, int *out_nn, double *out_d2, long long need,
+                       bool wait, std::string &detail);
+
   // Device-cell batch without a host read of the cell: nframes frames of n
   // points sharing the cell at the device pointer cell (cell_n = 3, 9 or 12
   // doubles), planned on the device at every launch (and every graph
@@ -104,6 +116,13 @@ class WorkspaceImpl {
   Code run_device_cell(const double *cell, int cell_n, long long n, int nframes, int k,
                        double hint, const double *xyz, const int *mask, int *out_nn,
                        double *out_d2, bool wait, std::string &detail);
+
+  // One rank's share of a search split across world ranks that hold the
+  // same inputs: the prep runs whole, the walk covers this rank's range of
+  // sorted sources (split by expected work), and owned (device, one int per
+  // point) marks the rows this rank wrote. Graphs are not used for it.
+  Code run_shard(std::vector<FrameDesc> &frames, const double *xyz, const int *mask, int *out_nn,
+                 double *out_d2, int *owned, int rank, int world, bool wait, std::string &detail);
 
   WalkOptions opts;
   bool collect_stats = true;
@@ -151,12 +170,15 @@ class WorkspaceImpl {
     const void *dcell = nullptr;  // device-planned batch: its cell and launch constants
     int cell_n = 0;
     double hint = 0.0;
+    int spin = 0;
+    long long silent = -1;
     bool operator==(const GraphKey &o) const {
       return npts == o.npts && ncells == o.ncells && nf == o.nf && kmax == o.kmax && xyz == o.xyz &&
              mask == o.mask && nn == o.nn && d2 == o.d2 && mode == o.mode && tpp == o.tpp &&
              block == o.block && model == o.model && fixed == o.fixed && log == o.log &&
              stats == o.stats &&
-             dcell == o.dcell && cell_n == o.cell_n && hint == o.hint;
+             dcell == o.dcell && cell_n == o.cell_n && hint == o.hint && spin == o.spin &&
+             silent == o.silent;
     }
   };
   // the device-cell batch being enqueued (run_device_cell)
@@ -195,6 +217,15 @@ class WorkspaceImpl {
   Buf<unsigned long long> part_tiles_;
   Code walk_in_row_ranges(BatchBuffers &b, const WalkLaunch &wl, cudaStream_t s, bool timed,
                           std::string &detail);
+  struct Shard {
+    bool on = false;
+    int rank = 0, world = 1;
+    int *owned = nullptr;
+  };
+  Shard shard_;
+  Buf<uint32_t> shard_cut_;
+  Code walk_shard(BatchBuffers &b, const WalkLaunch &wl, cudaStream_t s, bool timed,
+                  std::string &detail);
   Buf<uint32_t> csr_counts_, csr_off_;
 
  public:

@@ -703,7 +703,8 @@ int orc_walk_stats(const double *xyz, size_t n, const orc_cell *cell, size_t k, 
 
 int orc_knearest_subset(const double *xyz, size_t n, const orc_cell *cell, size_t k,
                         const int *mask, double cell_hint, const long long *sources,
-                        size_t count, int *out_nn, double *out_d2, int threads) {
+                        size_t count, int *out_nn, double *out_d2, int threads,
+                        long long *visits) {
   if (n == 0) return fail(Err::Empty);
   if (k == 0) return fail(Err::ZeroK);
   Cell c;
@@ -711,6 +712,8 @@ int orc_knearest_subset(const double *xyz, size_t n, const orc_cell *cell, size_
   for (size_t t = 0; t < count * k; ++t) out_nn[t] = -1;
   if (out_d2)
     for (size_t t = 0; t < count * k; ++t) out_d2[t] = std::numeric_limits<double>::quiet_NaN();
+  if (visits)
+    for (size_t t = 0; t < count; ++t) visits[t] = 0;
   std::vector<size_t> active;
   for (size_t i = 0; i < n; ++i)
     if (!mask || mask[i] != 0) active.push_back(i);
@@ -735,7 +738,7 @@ int orc_knearest_subset(const double *xyz, size_t n, const orc_cell *cell, size_
     const size_t i = size_t(src);
     if (mask && mask[i] == 0) return;
     KHeap &heap = heaps[size_t(w)];
-    walk_one(b, i, heap, nullptr);
+    walk_one(b, i, heap, visits ? &visits[t] : nullptr);
     heap.finish(rows[size_t(w)]);
     auto &pairs = rows[size_t(w)];
     for (size_t s = 0; s < pairs.size(); ++s) {

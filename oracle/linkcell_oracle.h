@@ -83,11 +83,13 @@ int orc_time_sample(const double *xyz, size_t n, const orc_cell *cell,
 
 /* Rows of the reference search for the listed sources only (fold, bin and
  * linked lists still cover all n points): row t of out_* belongs to
- * sources[t]. Used for full-size parity checks on a sample. */
+ * sources[t]. visits (NULL allowed) gets each listed source's heap pushes,
+ * the candidate pairs the reference walk evaluates for it. Used for
+ * full-size parity checks and pair counts on a sample. */
 int orc_knearest_subset(const double *xyz, size_t n, const orc_cell *cell,
                         size_t k, const int *mask, double cell_hint,
                         const long long *sources, size_t count, int *out_nn,
-                        double *out_d2, int threads);
+                        double *out_d2, int threads, long long *visits);
 
 const char *orc_version(void);
 

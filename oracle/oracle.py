@@ -54,7 +54,7 @@ def lib():
         L.orc_time_sample.argtypes = [dp, sz, cp, sz, ip, ctypes.c_double, sz, sz, sz, ctypes.c_int,
                                       dp, dp, llp, llp]
         L.orc_knearest_subset.argtypes = [dp, sz, cp, sz, ip, ctypes.c_double, llp, sz, ip, dp,
-                                          ctypes.c_int]
+                                          ctypes.c_int, llp]
         L.orc_version.restype = ctypes.c_char_p
         _lib = L
     return _lib
@@ -194,18 +194,23 @@ def time_sample(xyz, cell, k, mask=None, cell_hint=0.0, first=0, stride=1, count
     return dict(prep_s=prep.value, walk_s=walk.value, walked=walked.value, checksum=chk.value)
 
 
-def knearest_subset(xyz, cell, k, sources, mask=None, cell_hint=0.0, threads=0):
-    """Reference rows for the given source indices only: (len(sources), k)."""
+def knearest_subset(xyz, cell, k, sources, mask=None, cell_hint=0.0, threads=0,
+                    with_visits=False):
+    """Reference rows for the given source indices only: (len(sources), k).
+    with_visits also returns each source's heap pushes (the candidate pairs
+    the reference walk evaluates for it)."""
     xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
     n = xyz.shape[0]
     src = np.ascontiguousarray(sources, dtype=np.int64)
     m = None if mask is None else np.ascontiguousarray(mask, dtype=np.int32)
     nn = np.empty((src.size, k), dtype=np.int32)
     d2 = np.empty((src.size, k), dtype=np.float64)
+    visits = np.zeros(src.size, dtype=np.int64) if with_visits else None
     oc = make_cell(cell)
+    llp = ctypes.POINTER(ctypes.c_longlong)
     rc = lib().orc_knearest_subset(_dptr(xyz), n, ctypes.byref(oc), k, _iptr(m), float(cell_hint),
-                                   src.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), src.size,
-                                   _iptr(nn), _dptr(d2), threads)
+                                   src.ctypes.data_as(llp), src.size, _iptr(nn), _dptr(d2),
+                                   threads, None if visits is None else visits.ctypes.data_as(llp))
     if rc != 0:
         raise OracleError(last_error())
-    return nn, d2
+    return (nn, d2, visits) if with_visits else (nn, d2)
