@@ -544,6 +544,9 @@ def run_ours(args):
         L.lc_gpu_stats(ws, buf, 16, None)
         counters = {nm: int(buf[i]) for i, nm in enumerate(COUNTER_NAMES)}
         counters["tpp"] = int(L.lc_gpu_get_tpp(ws))  # walk design used (autotuned unless forced)
+        shp = (ctypes.c_int * 3)()
+        L.lc_gpu_walk_shape(ws, shp, None, 0)
+        counters["shape"] = list(shp)
         assert L.lc_gpu_set_proposal(ws, 0) == 0
         total = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), "cuda")
         return {"total_ms": total, "ms": total / steps, "walk_ms": statistics.mean(walk_ms),
@@ -660,6 +663,7 @@ def run_ours(args):
            "data": "synthetic",
            "config": {"workload": workload_name(n, k), "n": n, "k": k, "cell_hint": 3.0,
                       "mode": MODE_NAMES[best_mode], "tpp": head["counters"]["tpp"],
+                      "walk_shape": head["counters"]["shape"],
                       "tpp_source": "forced" if args.tpp else "autotuned",
                       "parallelism": f"replicas x{world}",
                       "l2": "flushed between timed steps (256 MB write)"},
@@ -749,7 +753,9 @@ def c3_block(args, steps, world, flush):
     value = whole_job_rate(active, steps, total_ms, world)
     plain_value = whole_job_rate(active, max(3, steps // 2), plain_ms, world)
     captures = int(L.lc_gpu_graph_captures(ws))
-    tuned = int(L.lc_gpu_get_tpp(ws))
+    shape = (ctypes.c_int * 3)()
+    trials = (ctypes.c_int * 48)()
+    ntrial = L.lc_gpu_walk_shape(ws, shape, trials, 16)
 
     # end to end through lc_knearest_batch: the same batch from host memory
     # (page-locked), rows back into page-locked buffers, which the library
@@ -780,7 +786,11 @@ def c3_block(args, steps, world, flush):
            "value": value, "unit": "sources/s", "steps": steps, "ms_per_step": total_ms / steps,
            "config": {"workload": "batched_256_frames_seed3", "frames": len(frames),
                       "points": int(moff), "active_sources": active, "k": ks, "mode": "learned",
-                      "graph": True, "graph_captures": captures, "tpp": tuned,
+                      "graph": True, "graph_captures": captures,
+                      "walk_shape": {"tpp": shape[0], "warps_per_block": shape[1],
+                                     "grab": shape[2], "source": "autotuned",
+                                     "candidates_timed": [list(trials[3 * i:3 * i + 3])
+                                                          for i in range(ntrial)]},
                       "l2": "flushed between timed steps (256 MB write)"},
            "e2e": {"value": whole_job_rate(active, steps, 1000.0 * e2e_s, world),
                    "unit": "sources/s", "h2d_bytes_per_step": int(xyz_h.nbytes + mask_h.nbytes),

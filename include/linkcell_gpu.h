@@ -145,6 +145,20 @@ int lc_gpu_mlp_adam(float *params, const float *grad, float *m, float *v, int st
 int lc_gpu_set_tpp(lc_gpu_workspace *ws, int tpp);
 int lc_gpu_get_tpp(lc_gpu_workspace *ws);
 
+/* Extension: the learned mode's cube select walk in a fixed block shape:
+ * warps per block (8 or 4 for k <= 32, 4 or 2 for k <= 64) and sources per
+ * work-queue grab (8, 16 or 32). 0, 0 hands both back to the autotuner,
+ * which times every such shape (and the thread-per-source walk) once on the
+ * first batch of each kind; LINKCELL_GRAB overrides the grab like
+ * LINKCELL_BLOCK the block. Results are the same in every shape. */
+int lc_gpu_set_walk_shape(lc_gpu_workspace *ws, int warps, int grab);
+
+/* Extension: the walk of the last search: shape3 = threads per source,
+ * warps per block, sources per grab (0 where they do not apply). trials
+ * (NULL allowed) gets up to max_trials triples of the candidates the last
+ * autotuning timed. Returns the number of candidates it timed (0: none). */
+int lc_gpu_walk_shape(lc_gpu_workspace *ws, int *shape3, int *trials, int max_trials);
+
 /* CUDA graphs: with on != 0 a search captures its whole launch sequence
  * (frame-table copy, memsets, kernels) in a CUDA graph and replays it while
  * the batch keeps its sizes, pointers and configuration; the frame table

@@ -41,7 +41,7 @@ EXPORTS = (
     "lc_gpu_mlp_params", "lc_gpu_mlp_scratch_floats", "lc_gpu_mlp_forward", "lc_gpu_mlp_grad",
     "lc_gpu_mlp_adam",
     "lc_gpu_knearest_batch", "lc_gpu_knearest_noalloc", "lc_knearest_batch",
-    "lc_gpu_knearest_shard",
+    "lc_gpu_knearest_shard", "lc_gpu_set_walk_shape", "lc_gpu_walk_shape",
 )
 
 _lib = None
@@ -90,6 +90,8 @@ def load():
     L.lc_gpu_set_proposal.argtypes = [vp, i]
     L.lc_gpu_set_tpp.argtypes = [vp, i]
     L.lc_gpu_get_tpp.argtypes = [vp]
+    L.lc_gpu_set_walk_shape.argtypes = [vp, i, i]
+    L.lc_gpu_walk_shape.argtypes = [vp, ip, ip, i]
     L.lc_gpu_set_graph.argtypes = [vp, i]
     L.lc_gpu_graph_captures.argtypes = [vp]
     L.lc_gpu_set_stats.argtypes = [vp, i]

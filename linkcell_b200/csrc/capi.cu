@@ -613,6 +613,35 @@ int lc_gpu_set_tpp(lc_gpu_workspace *ws, int tpp) {
 
 int lc_gpu_get_tpp(lc_gpu_workspace *ws) { return ws ? ws->ws.last_tpp : -1; }
 
+int lc_gpu_set_walk_shape(lc_gpu_workspace *ws, int warps, int grab) {
+  if (!ws) return gpu_fail(Code::NullPointer);
+  if (!(warps == 0 || warps == 2 || warps == 4 || warps == 8))
+    return gpu_fail_msg("warps per block must be 2, 4 or 8 (0: autotune)");
+  if (!(grab == 0 || grab == 8 || grab == 16 || grab == 32))
+    return gpu_fail_msg("sources per grab must be 8, 16 or 32 (0: autotune)");
+  ws->ws.opts.sel_warps = warps;
+  ws->ws.opts.sel_grab = grab;
+  return 0;
+}
+
+int lc_gpu_walk_shape(lc_gpu_workspace *ws, int *shape3, int *trials, int max_trials) {
+  if (!ws) return gpu_fail(Code::NullPointer);
+  const lc::WalkShape &l = ws->ws.last_shape;
+  if (shape3) {
+    shape3[0] = l.tpp;
+    shape3[1] = l.warps;
+    shape3[2] = l.grab;
+  }
+  const auto &t = ws->ws.trial_shapes_;
+  if (trials)
+    for (int i = 0; i < max_trials && size_t(i) < t.size(); ++i) {
+      trials[3 * i] = t[size_t(i)].tpp;
+      trials[3 * i + 1] = t[size_t(i)].warps;
+      trials[3 * i + 2] = t[size_t(i)].grab;
+    }
+  return int(t.size());
+}
+
 int lc_gpu_set_graph(lc_gpu_workspace *ws, int on) {
   if (!ws) return gpu_fail(Code::NullPointer);
   ws->ws.opts.graph = on != 0;

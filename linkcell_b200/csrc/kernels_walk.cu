@@ -994,11 +994,13 @@ __global__ void __launch_bounds__(256, 2) k_team_walk(BatchBuffers b) {
 // (64 entries for k <= 32, 128 for k <= 64) sends
 // the source to the literal replay.
 constexpr int kSelCap = 512;   // FP32-filtered candidates per warp
-// Warps per block: 8 for k <= 32 (3 blocks per SM, register bound); 4 for
-// k <= 64, whose larger S buffers fit 5 smaller blocks per SM where only 2 of 8
-// warps would.
+// Warps per block (the autotuner picks among two per S size): 8 or 4 for
+// k <= 32 (24 warps per SM, register bound), 4 or 2 for k <= 64 (20 warps
+// per SM, bound by the larger S buffers in shared memory).
 template <int SN>
-constexpr int sel_warps() { return SN == 2 ? 8 : 4; }
+constexpr int sel_warps_per_sm() { return SN == 2 ? 24 : 20; }
+template <int SN>
+constexpr int sel_default_warps() { return SN == 2 ? 8 : 4; }
 
 struct __align__(16) SelRow {  // one non-empty row of the cube
   int excl;                    // first candidate position of the row
@@ -1425,18 +1427,37 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
     }
   }
   __syncwarp();
-  // 4. rank of each element in (d2, index) order; the first k are the row
+  // 4. rank of each element in (d2, index) order; the first k are the row.
+  // Element q sits in lane q % 32, group q / 32. A group of many elements
+  // counts in one pass over S, each lane for its own element; a group of a
+  // few (the elements past 32 when S barely exceeds k = 32) is ranked one
+  // element at a time by the whole warp: every lane compares its elements
+  // with it and a warp sum adds the comparisons up. (Empty slots hold
+  // (+inf, INT_MAX) and never count.)
   int rk[SN];
 #pragma unroll
-  for (int h = 0; h < SN; ++h) rk[h] = 0;
-  if (nS <= 32) {  // the common case: one element per lane
-    for (int e = 0; e < nS; ++e) rk[0] += lex_less(sh.sd[e], sh.sj[e], ed[0], ej[0]) ? 1 : 0;
-  } else {
-    for (int e = 0; e < nS; ++e) {
-      const double de = sh.sd[e];
-      const int je = sh.sj[e];
+  for (int h = 0; h < SN; ++h) {
+    rk[h] = 0;
+    const int cnt = min(nS - 32 * h, 32);
+    if (cnt <= 0) continue;
+    if (cnt >= 16) {
+      int e = 0;
+      for (; e + 2 <= nS; e += 2) {
+        const double d0 = sh.sd[e], d1 = sh.sd[e + 1];
+        const int j0 = sh.sj[e], j1 = sh.sj[e + 1];
+        rk[h] += (lex_less(d0, j0, ed[h], ej[h]) ? 1 : 0) + (lex_less(d1, j1, ed[h], ej[h]) ? 1 : 0);
+      }
+      if (e < nS) rk[h] += lex_less(sh.sd[e], sh.sj[e], ed[h], ej[h]) ? 1 : 0;
+    } else {
+      for (int q = 32 * h; q < 32 * h + cnt; ++q) {
+        const double dq = sh.sd[q];
+        const int jq = sh.sj[q];
+        int c = 0;
 #pragma unroll
-      for (int h = 0; h < SN; ++h) rk[h] += lex_less(de, je, ed[h], ej[h]) ? 1 : 0;
+        for (int g = 0; g < SN; ++g) c += lex_less(ed[g], ej[g], dq, jq) ? 1 : 0;
+        const int r = int(__reduce_add_sync(kFull, unsigned(c)));
+        if (lane == q - 32 * h) rk[h] = r;
+      }
     }
   }
   const FrameDesc &frr = fr;
@@ -1468,21 +1489,23 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   return true;
 }
 
-template <int SN, bool STATS>
-__global__ void __launch_bounds__(sel_warps<SN>() * 32, SN == 2 ? 3 : 5) k_select_walk(BatchBuffers b) {
+// grab: consecutive sources a warp takes from the work queue at a time
+// (they share most candidates, which then stay in L1).
+template <int SN, bool STATS, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, sel_warps_per_sm<SN>() / WARPS)
+    k_select_walk(BatchBuffers b, int grab) {
   extern __shared__ __align__(16) unsigned char sel_smem[];
   SelShared<SN> &sh = reinterpret_cast<SelShared<SN> *>(sel_smem)[threadIdx.x >> 5];
   const long long total = walk_sources(b);
   const int lane = threadIdx.x & 31;
   if (lane < kWcSlots) sh.wc[lane] = 0;
   __syncwarp();
-  constexpr int kGrab = 16;  // consecutive sources share most candidates (L1 reuse)
   for (;;) {
     uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(b.work, uint32_t(kGrab));
+    if (lane == 0) base = atomicAdd(b.work, uint32_t(grab));
     base = __shfl_sync(kFull, base, 0);
     if ((long long)base >= total) break;
-    for (int q = 0; q < kGrab; ++q) {
+    for (int q = 0; q < grab; ++q) {
       if ((long long)base + q >= total) break;
       const long long p = walk_source_at(b, (long long)base + q);
       if (p < 0) continue;
@@ -1512,24 +1535,34 @@ __global__ void __launch_bounds__(sel_warps<SN>() * 32, SN == 2 ? 3 : 5) k_selec
 
 int sm_count();
 
-template <int SN, bool STATS>
+template <int SN, bool STATS, int WARPS>
 cudaError_t launch_select_as(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
-  const size_t smem = sizeof(SelShared<SN>) * sel_warps<SN>();
-  cudaError_t e = cudaFuncSetAttribute(k_select_walk<SN, STATS>,
+  const size_t smem = sizeof(SelShared<SN>) * WARPS;
+  cudaError_t e = cudaFuncSetAttribute(k_select_walk<SN, STATS, WARPS>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk<SN, STATS>, sel_warps<SN>() * 32,
-                                                smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk<SN, STATS, WARPS>,
+                                                WARPS * 32, smem);
   if (per_sm < 1) per_sm = 1;
   const int grid = w.grid > 0 ? w.grid : sm_count() * per_sm;
-  k_select_walk<SN, STATS><<<grid, sel_warps<SN>() * 32, smem, s>>>(b);
+  const int grab = w.grab == 8 || w.grab == 32 ? w.grab : 16;
+  k_select_walk<SN, STATS, WARPS><<<grid, WARPS * 32, smem, s>>>(b, grab);
   return cudaGetLastError();
 }
 
+template <int SN, int WARPS>
+cudaError_t launch_select_w(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
+  return w.stats ? launch_select_as<SN, true, WARPS>(b, w, s)
+                 : launch_select_as<SN, false, WARPS>(b, w, s);
+}
+
+// The select walk in the block shape w.warps asks for (one of the two its S
+// size allows; anything else takes the default).
 template <int SN>
 cudaError_t launch_select(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
-  return w.stats ? launch_select_as<SN, true>(b, w, s) : launch_select_as<SN, false>(b, w, s);
+  constexpr int W = sel_default_warps<SN>();
+  return w.warps == W / 2 ? launch_select_w<SN, W / 2>(b, w, s) : launch_select_w<SN, W>(b, w, s);
 }
 
 // Warp-parallel literal replay of the reference heap for one source (finite

@@ -124,7 +124,15 @@ struct WalkLaunch {
   int prune = 1;
   bool stats = false;  // the learned select walk counts its statistics
   const int8_t *proposal = nullptr;  // per sorted source proposed shell (learned mode)
+  // select walk shape: warps per block (k <= 32: 8 or 4; k <= 64: 4 or 2;
+  // 0 = the default) and sources per work grab (8, 16 or 32; 0 = 16)
+  int warps = 0;
+  int grab = 0;
 };
+
+// Walk shapes the autotuner times for the select walk of k <= kmax.
+constexpr int kSelGrabs[3] = {8, 16, 32};
+inline int sel_warps_for(int kmax, int i) { return kmax <= 32 ? (i ? 4 : 8) : (i ? 2 : 4); }
 
 cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s);
 cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s);

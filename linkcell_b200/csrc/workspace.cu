@@ -79,6 +79,10 @@ WorkspaceImpl::WorkspaceImpl() {
     const int v = std::atoi(b);
     if (v == 32 || v == 64 || v == 128 || v == 256) opts.block = v;
   }
+  if (const char *g = std::getenv("LINKCELL_GRAB")) {
+    const int v = std::atoi(g);
+    if (v == 8 || v == 16 || v == 32) opts.sel_grab = v;
+  }
   cudaGetDevice(&device_);
   cudaStreamCreateWithFlags(&own_, cudaStreamNonBlocking);
   for (auto &e : ev_) cudaEventCreate(&e);
@@ -316,35 +320,56 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   wl.stats = opts.stats;
   const int kclass = kmax <= 32 ? 0 : (kmax <= 64 ? 1 : (kmax <= 128 ? 2 : 3));
   const int tkey = (wl.mode * 4 + kclass) * 2 + (nf > 1 ? 1 : 0);
-  auto set_tpp = [&](int tpp) {
-    wl.tpp = tpp;
+  const bool select = wl.mode == kModeLearned && kmax <= 64 && learned;  // the cube select walk
+  auto set_shape = [&](const WalkShape &sh) {
+    wl.tpp = sh.tpp;
     const int maxblk = walk_max_block(wl.mode, kmax);
     wl.block = opts.block > 0 ? std::min(opts.block, maxblk) : maxblk;
+    wl.warps = sh.warps;
+    wl.grab = sh.grab;
   };
   bool done = false;  // the batch's results are already in place
-  if (opts.tpp_forced || !opts.autotune || wl.mode == kModeReplayAll) {
-    set_tpp(opts.tpp);
+  const bool forced = opts.tpp_forced || opts.sel_warps > 0 || opts.sel_grab > 0;
+  if (forced || !opts.autotune || wl.mode == kModeReplayAll) {
+    // overrides (API or LINKCELL_TPP / LINKCELL_BLOCK / LINKCELL_GRAB); the
+    // rest at its default
+    int warps = opts.sel_warps;
+    if (warps == 0 && opts.block > 0 && select &&
+        (opts.block / 32 == sel_warps_for(kmax, 0) || opts.block / 32 == sel_warps_for(kmax, 1)))
+      warps = opts.block / 32;
+    set_shape(WalkShape{opts.tpp_forced ? opts.tpp : 32, warps, opts.sel_grab});
   } else if (tuned_.count(tkey)) {
-    set_tpp(tuned_[tkey]);
+    set_shape(tuned_[tkey]);
   } else {
-    // time both walk designs once on this batch (their results are
-    // identical) and keep the faster one for every later batch of this kind
-    const int cand[2] = {32, 1};
-    float ms[2] = {0.f, 0.f};
+    // time every candidate design and shape once on this batch (their
+    // results are identical) and keep the fastest for every later batch of
+    // this kind: warp per source (for the select walk, in two block sizes and
+    // three work-grab sizes) and thread per source
+    std::vector<WalkShape> cand;
+    if (select)
+      for (int wi = 0; wi < 2; ++wi)
+        for (int g : kSelGrabs) cand.push_back(WalkShape{32, sel_warps_for(kmax, wi), g});
+    else
+      cand.push_back(WalkShape{32, 0, 0});
+    cand.push_back(WalkShape{1, 0, 0});
+    std::vector<float> ms(cand.size(), 0.f);
     const bool piping = pipe_.on;
     pipe_.on = false;  // the trials run whole searches
-    for (int c = 0; c < 2; ++c) {
-      set_tpp(cand[c]);
+    for (size_t c = 0; c < cand.size(); ++c) {
+      set_shape(cand[c]);
       const Code rc = enqueue(b, wl, nf, C, tiles, s, true, detail);
       if (rc != Code::Ok) return rc;
       LC_TRY(cudaEventSynchronize(ev_[3]));
       LC_TRY(cudaEventElapsedTime(&ms[c], ev_[1], ev_[2]));
     }
     pipe_.on = piping;
-    const int best = ms[1] < ms[0] ? 1 : 0;
+    size_t best = 0;
+    for (size_t c = 1; c < cand.size(); ++c)
+      if (ms[c] < ms[best]) best = c;
     tuned_[tkey] = cand[best];
-    set_tpp(cand[best]);
-    done = best == 1 && !opts.graph;  // the last run used the winner
+    set_shape(cand[best]);
+    trial_shapes_ = cand;
+    done = best + 1 == cand.size() && !opts.graph;  // the last run used the winner
     if (!done && !opts.graph) {
       const Code rc = enqueue(b, wl, nf, C, tiles, s, collect_stats, detail);
       if (rc != Code::Ok) return rc;
@@ -354,6 +379,9 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
     graph_total_ = false;
   }
   last_tpp = wl.tpp;
+  last_shape = WalkShape{wl.tpp,
+                         wl.tpp == 32 && select ? (wl.warps ? wl.warps : sel_warps_for(kmax, 0)) : 0,
+                         wl.tpp == 32 && select ? (wl.grab ? wl.grab : 16) : 0};
 
   // ---- 4. enqueue: direct launches, or a CUDA graph replayed while the
   // batch signature (sizes, pointers, configuration) stays the same
@@ -361,7 +389,8 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
     // autotuning left this batch's results and stats in place
   } else if (opts.graph) {
     const GraphKey key{npts, ncells, nf, kmax, xyz, mask, out_nn, out_d2, wl.mode, wl.tpp,
-                       wl.block, has_model_ ? 1 : 0, opts.fixed_proposal, opts.log_shells,
+                       wl.block + 1024 * wl.warps + 65536 * wl.grab, has_model_ ? 1 : 0,
+                       opts.fixed_proposal, opts.log_shells,
                        opts.stats ? 1 : 0, dcell_.on ? dcell_.cell : nullptr,
                        dcell_.on ? dcell_.cell_n : 0,
                        dcell_.on ? dcell_.hint : 0.0, opts.scan_spin_limit,

@@ -53,12 +53,20 @@ cudaError_t launch_plan_device_cell(const double *cell, int cell_n, long long n,
 // Device address of page-locked host memory, or null.
 void *mapped_host(const void *p);
 
+// A walk design and shape: threads per source (32 or 1) and, for the cube
+// select walk, warps per block and sources per work grab (0: default).
+struct WalkShape {
+  int tpp = 32, warps = 0, grab = 0;
+};
+
 // Options that pick the walk.
 struct WalkOptions {
   // the learned walk: results equal every other mode's, and it is the fastest
   int mode = kModeLearned;
   int tpp = 32;    // threads per source: 32 (warp team) or 1 (one thread, heap in shared memory)
   int block = 0;   // 0: autotune / default
+  int sel_warps = 0;  // select walk warps per block (lc_gpu_set_walk_shape), 0: autotune
+  int sel_grab = 0;   // select walk sources per grab (or LINKCELL_GRAB), 0: autotune
   int prune = 1;
   int fixed_proposal = 0;  // learned walk: > 0 proposes this shell for every source
   int log_shells = 0;      // record the settled shell of every source (training data)
@@ -127,6 +135,8 @@ class WorkspaceImpl {
   WalkOptions opts;
   bool collect_stats = true;
   int last_tpp = 0;          // walk design of the last batch
+  WalkShape last_shape;      // design and shape of the last batch's walk
+  std::vector<WalkShape> trial_shapes_;  // the candidates the last autotuning timed
   int last_host_rows = 0;  // how the last host-pointer search returned its rows (0 copy, 1 ranges, 2 mapped)
   int graph_captures = 0;    // CUDA graphs captured so far
   // Counters and phase times of the last run (waits for it to finish).
@@ -195,7 +205,7 @@ class WorkspaceImpl {
   GraphKey graph_key_;
   cudaGraphExec_t graph_exec_ = nullptr;
   bool graph_total_ = false;
-  std::map<int, int> tuned_;
+  std::map<int, WalkShape> tuned_;
   FrameDesc *h_frames_ = nullptr;
   size_t h_frames_cap_ = 0;
   cudaEvent_t ev_done_ = nullptr;
