@@ -993,7 +993,8 @@ __global__ void __launch_bounds__(256, 2) k_team_walk(BatchBuffers b) {
 // overflow, a cube that wraps the box, k > 64 or an S larger than its buffer
 // (64 entries for k <= 32, 128 for k <= 64) sends
 // the source to the literal replay.
-constexpr int kSelCap = 512;   // FP32-filtered candidates per warp
+constexpr int kSelCap = 480;   // FP32-filtered candidates per warp
+constexpr int kSelWin = 2;     // 32-candidate windows a gather trip loads at once
 // Warps per block (the autotuner picks among two per S size): 8 or 4 for
 // k <= 32 (24 warps per SM, register bound), 4 or 2 for k <= 64 (20 warps
 // per SM, bound by the larger S buffers in shared memory).
@@ -1002,14 +1003,15 @@ constexpr int sel_warps_per_sm() { return SN == 2 ? 24 : 20; }
 template <int SN>
 constexpr int sel_default_warps() { return SN == 2 ? 8 : 4; }
 
-struct __align__(16) SelRow {  // one non-empty row of the cube
-  int excl;                    // first candidate position of the row
-  int startA, lenA;            // sorted range of the cells inside the box
-  int startB;                  // sorted range of the cells wrapped in x, minus lenA
-  int xoffA, xoffB;            // dx = candidate cell x + xoff (A: no x wrap, B: wrapped)
-  int metaA, metaB;            // wrap counts of a candidate (A / B) in SelShared::m layout
-  float Dx, Dy, Dz;            // dy e_b + dz e_c (FP32)
-  int syz;                     // max(1, |dy|, |dz|)
+// One contiguous run of sorted points of a cube row: the cells of the row
+// inside the box, or the ones across the x boundary (a row yields one or two).
+struct __align__(16) SelSeg {
+  int excl;        // first candidate position of the run
+  int start;       // its first sorted position
+  int xoff;        // dx = candidate cell x + xoff
+  uint32_t meta;   // wrap counts of its candidates in SelShared::m layout
+  float Dx, Dy, Dz;  // dy e_b + dz e_c (FP32)
+  int syz;           // max(1, |dy|, |dz|)
 };
 
 // SN: elements of S per lane (S holds at most 32 SN; k <= 16 SN).
@@ -1018,7 +1020,7 @@ struct SelShared {
   float d[kSelCap];
   int t[kSelCap];
   uint32_t m[kSelCap];  // shell | wa + 1 << 8 | wb + 1 << 10 | wc + 1 << 12
-  SelRow rows[32];
+  SelSeg segs[64];
   double sd[32 * SN];
   int sj[32 * SN];
   int si[32 * SN];
@@ -1039,6 +1041,32 @@ __device__ __forceinline__ float axis_gap(int d, float f) {
   return d > 0 ? float(d) - f : (d < 0 ? f + float(-d - 1) : 0.f);
 }
 
+// Ascending bitonic sort of 64 unsigned keys held two per lane: position q
+// is lane q % 32's ka (q < 32) or kb (q >= 32). Element q trades with q ^ j
+// and keeps the smaller key when (q < q ^ j) matches the ascending blocks of
+// the stage ((q & kk) == 0).
+__device__ __forceinline__ void bitonic64(uint32_t &ka, uint32_t &kb, int lane) {
+#pragma unroll
+  for (int kk = 2; kk <= 64; kk <<= 1) {
+#pragma unroll
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      if (j == 32) {
+        const uint32_t lo = min(ka, kb), hi = max(ka, kb);
+        ka = lo;
+        kb = hi;
+      } else {
+        const uint32_t pa = __shfl_xor_sync(kFull, ka, j);
+        const uint32_t pb = __shfl_xor_sync(kFull, kb, j);
+        const bool low = (lane & j) == 0;
+        const bool upa = (lane & kk) == 0;
+        const bool upb = ((lane + 32) & kk) == 0;
+        ka = low == upa ? min(ka, pa) : max(ka, pa);
+        kb = low == upb ? min(kb, pb) : max(kb, pb);
+      }
+    }
+  }
+}
+
 // Walk statistics of a warp, kept in shared memory (lane 0 or shared
 // atomics update them) so that they hold no registers.
 enum SelWarpCounter {
@@ -1052,6 +1080,144 @@ __device__ __forceinline__ uint32_t quot(uint32_t x, uint32_t n, double inv) {
   if (q * n > x) --q;
   else if ((q + 1) * n <= x) ++q;
   return q;
+}
+
+// Steps 3-4 of the select walk when the gathered buffer holds at most 64
+// candidates (k <= 32): a sort instead of histograms and ranking.
+//  - Every eligible candidate (shell <= R*, d32 within the histogram path's
+//    bound) gets the key bits(d32) with its low 6 bits replaced by its buffer
+//    slot: unique, and |key - d32| <= 2^-17 d32. The 64 keys are sorted.
+//  - K = the k-th smallest key: k candidates have d32 <= Tup = K (1 + 2^-16),
+//    so the k-th smallest exact distance v is at most Tup + band(Tup). S =
+//    the sorted prefix with key <= (Tup + 3 band(Tup)) (1 + 2^-16): it holds
+//    every candidate whose exact distance is at most Tup + band(Tup) (the k
+//    smallest and everything tied with v), and nothing outside S can tie v
+//    -- the histogram path's argument with the key's error added.
+//  - S is recomputed in exact FP64. Sorted by key, two neighbours can be out
+//    of exact (d2, index) order only if their keys lie within twice the
+//    error bound band''(x) = band(x) + 2^-16 x of each other; the runs of
+//    such linked neighbours (clusters, almost always single elements) are
+//    ranked exactly inside, and every other position is already its rank.
+//  - A tie across the k-th slot (equal k-th and (k+1)-th exact values) sends
+//    the source to the literal replay, as in the histogram path.
+template <int SN, bool STATS>
+__device__ bool select_sorted(const BatchBuffers &b, long long p, int lane, SelShared<SN> &sh,
+                              const FrameDesc &fr, int total, int Rs, int Rp, bool partial) {
+  const int k = fr.k;
+  const float Bs_hi = (partial && Rs == Rp) ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rs];
+  const float beta_s = fr.sel_beta[Rs];
+  uint32_t ka = 0xffffffffu, kb = 0xffffffffu;
+  if (lane < total) {
+    const float d = sh.d[lane];
+    if (int(sh.m[lane] & 255u) <= Rs && d <= Bs_hi) ka = (__float_as_uint(d) & ~63u) | uint32_t(lane);
+  }
+  if (lane + 32 < total) {
+    const float d = sh.d[lane + 32];
+    if (int(sh.m[lane + 32] & 255u) <= Rs && d <= Bs_hi)
+      kb = (__float_as_uint(d) & ~63u) | uint32_t(lane + 32);
+  }
+  bitonic64(ka, kb, lane);
+  const uint32_t kth = __shfl_sync(kFull, k <= 32 ? ka : kb, (k - 1) & 31);
+  if (kth == 0xffffffffu) return false;  // cannot happen: R* guarantees k eligible candidates
+  const float Tup = __fmul_ru(__uint_as_float(kth), 1.f + 1.f / 65536.f);
+  const float TSk = __fmul_ru(__fadd_ru(Tup, __fmul_ru(3.f, __fmaf_ru(Tup, 8.f * kU32, beta_s))),
+                              1.f + 1.f / 65536.f);
+  const uint32_t tsb = __float_as_uint(TSk);
+  const bool inA = ka <= tsb, inB = kb <= tsb;
+  const int nS = __popc(__ballot_sync(kFull, inA)) + __popc(__ballot_sync(kFull, inB));
+  if (nS < k) return false;  // cannot happen
+  if (STATS && lane == 0) sh.wc[kWcRerank] += unsigned(nS);
+  // exact distances and indices of S (positions lane and lane + 32)
+  auto exact_at = [&](uint32_t key, double &d, int &j) {
+    const int i = int(key & 63u);
+    const int t = sh.t[i];
+    const uint32_t m = sh.m[i];
+    double shx, shy, shz;
+    lattice_shift(fr, int((m >> 8) & 3u) - 1, int((m >> 10) & 3u) - 1, int((m >> 12) & 3u) - 1,
+                  shx, shy, shz);
+    d = dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], shx, shy, shz);
+    j = b.sidx[t];
+  };
+  double da = pinf(), db = pinf();
+  int ja = 0x7fffffff, jb = 0x7fffffff;
+  if (inA) exact_at(ka, da, ja);
+  if (nS > 32 && inB) exact_at(kb, db, jb);
+  // clusters: position q is linked to q - 1 when their keys lie within
+  // 2.01 band''(key_q); starts = positions not linked to their predecessor
+  auto linked = [&](uint32_t kq, uint32_t kprev) -> bool {
+    const float xq = __uint_as_float(kq), xp = __uint_as_float(kprev);
+    const float bq = __fmaf_ru(xq, 8.f * kU32 + 1.f / 65536.f, beta_s);
+    return __fsub_ru(xq, xp) <= __fmul_ru(2.01f, bq);
+  };
+  const uint32_t upA = __shfl_up_sync(kFull, ka, 1);
+  const uint32_t lastA = __shfl_sync(kFull, ka, 31);
+  const uint32_t upB = __shfl_up_sync(kFull, kb, 1);
+  const uint32_t prevB = lane == 0 ? lastA : upB;
+  const bool linkA = lane > 0 && lane < nS && linked(ka, upA);
+  const bool linkB = lane + 32 < nS && linked(kb, prevB);
+  const unsigned long long starts =
+      (unsigned long long)__ballot_sync(kFull, !linkA) |
+      ((unsigned long long)__ballot_sync(kFull, !linkB) << 32);
+  const unsigned long long inS = nS >= 64 ? ~0ull : ((1ull << nS) - 1);
+  int rkA = lane, rkB = lane + 32;
+  if (~starts & inS) {
+    // cluster [a, e] of position q: a = the last start <= q, e = the next start - 1
+    auto bounds = [&](int q, int &a, int &e) {
+      const unsigned long long upto = q == 63 ? ~0ull : ((2ull << q) - 1);
+      a = 63 - __clzll(starts & upto);
+      const unsigned long long after = starts & ~upto & inS;
+      e = after ? __ffsll(after) - 2 : nS - 1;
+    };
+    int a0, e0, a1, e1;
+    bounds(lane, a0, e0);
+    bounds(lane + 32, a1, e1);
+    const int s0 = lane < nS ? e0 - a0 + 1 : 1;
+    const int s1 = lane + 32 < nS ? e1 - a1 + 1 : 1;
+    const int M = int(__reduce_max_sync(kFull, unsigned(max(s0, s1))));
+    int c0 = 0, c1 = 0;
+    for (int r = 0; r < M; ++r) {
+      // member r of each element's cluster (positions past the cluster are skipped)
+      const int p0 = min(a0 + r, 63), p1 = min(a1 + r, 63);
+      const double x0a = __shfl_sync(kFull, da, p0 & 31), x0b = __shfl_sync(kFull, db, p0 & 31);
+      const int y0a = __shfl_sync(kFull, ja, p0 & 31), y0b = __shfl_sync(kFull, jb, p0 & 31);
+      const double x1a = __shfl_sync(kFull, da, p1 & 31), x1b = __shfl_sync(kFull, db, p1 & 31);
+      const int y1a = __shfl_sync(kFull, ja, p1 & 31), y1b = __shfl_sync(kFull, jb, p1 & 31);
+      const double x0 = p0 < 32 ? x0a : x0b, x1 = p1 < 32 ? x1a : x1b;
+      const int y0 = p0 < 32 ? y0a : y0b, y1 = p1 < 32 ? y1a : y1b;
+      if (a0 + r <= e0 && lex_less(x0, y0, da, ja)) ++c0;
+      if (a1 + r <= e1 && lex_less(x1, y1, db, jb)) ++c1;
+    }
+    if (lane < nS) rkA = a0 + c0;
+    if (lane + 32 < nS) rkB = a1 + c1;
+  }
+  // a tie across the k-th slot: the k-th and (k+1)-th exact values are equal
+  if (nS > k) {
+    if (lane < nS && rkA == k - 1) sh.hmax[0] = __double2loint(da), sh.hmax[1] = __double2hiint(da);
+    if (lane + 32 < nS && rkB == k - 1) sh.hmax[0] = __double2loint(db), sh.hmax[1] = __double2hiint(db);
+    if (lane < nS && rkA == k) sh.hmax[2] = __double2loint(da), sh.hmax[3] = __double2hiint(da);
+    if (lane + 32 < nS && rkB == k) sh.hmax[2] = __double2loint(db), sh.hmax[3] = __double2hiint(db);
+    __syncwarp();
+    const bool tie = sh.hmax[0] == sh.hmax[2] && sh.hmax[1] == sh.hmax[3];
+    __syncwarp();
+    if (tie) {
+      if (STATS && lane == 0) ++sh.wc[kWcReplays];
+      return false;
+    }
+  }
+  const int i = b.sidx[p];
+  int *row = b.out_nn + fr.out_base + (long long)i * k;
+  double *drow = b.out_d2 ? b.out_d2 + fr.out_base + (long long)i * k : nullptr;
+  if (lane < nS && rkA < k) {
+    row[rkA] = ja;
+    if (drow) drow[rkA] = da;
+  }
+  if (lane + 32 < nS && rkB < k) {
+    row[rkB] = jb;
+    if (drow) drow[rkB] = db;
+  }
+  if (b.stop_log && lane == 0) b.stop_log[p] = int8_t(Rs);
+  if (STATS && lane == 0) sh.wc[kWcInserts] += unsigned(k);
+  return true;
 }
 
 // One source; false: the source must go to the literal replay. STATS: count
@@ -1107,10 +1273,11 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   const float invW = 1.f / float(W);
   const int nrow = W * W;
   total = 0;
+  const unsigned lt = lanemask_lt();
   for (int r0 = 0; r0 < nrow; r0 += 32) {
     const int row = r0 + lane;
-    int lenA = 0, lenB = 0, pruned = 0;
-    SelRow rw;
+    int lenA = 0, lenB = 0, pruned = 0, startA = 0, sB = 0, wrapB = 0, wbc = 0, syz = 0;
+    float Dx = 0.f, Dy = 0.f, Dz = 0.f;
     if (row < nrow) {
       const int qz = int((float(row) + 0.5f) * invW);  // exact: row < 289, W <= 17
       const int dy = row - qz * W - Rp, dz = qz - Rp;
@@ -1138,12 +1305,10 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
         // the cells inside the box, then the ones across the x boundary (one
         // side only: the range spans at most 2 Rp + 1 <= nx cells)
         const int a0 = max(xl, 0), a1 = min(xh, nx - 1);
-        rw.startA = 0;
         if (a0 <= a1) {
-          rw.startA = int(o[a0]);
-          lenA = int(o[a1 + 1]) - rw.startA;
+          startA = int(o[a0]);
+          lenA = int(o[a1 + 1]) - startA;
         }
-        int wrapB = 0, sB = 0;
         if (xl < 0 && xl <= xh) {
           const int b1 = min(xh, -1);
           sB = int(o[xl + nx]);
@@ -1155,18 +1320,12 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
           lenB = int(o[xh - nx + 1]) - sB;
           wrapB = 1;
         }
-        rw.lenA = lenA;
-        rw.startB = sB - lenA;
-        rw.xoffA = -ix;
-        rw.xoffB = -ix + wrapB * nx;
-        const int wbc = ((wb + 1) << 10) | ((wc + 1) << 12);
-        rw.metaA = (1 << 8) | wbc;
-        rw.metaB = ((wrapB + 1) << 8) | wbc;
+        wbc = ((wb + 1) << 10) | ((wc + 1) << 12);
         const float fdy = float(dy), fdz = float(dz);
-        rw.Dx = fdy * fr.ev[3] + fdz * fr.ev[6];
-        rw.Dy = fdy * fr.ev[4] + fdz * fr.ev[7];
-        rw.Dz = fdy * fr.ev[5] + fdz * fr.ev[8];
-        rw.syz = max(1, max(abs(dy), abs(dz)));
+        Dx = fdy * fr.ev[3] + fdz * fr.ev[6];
+        Dy = fdy * fr.ev[4] + fdz * fr.ev[7];
+        Dz = fdy * fr.ev[5] + fdz * fr.ev[8];
+        syz = max(1, max(abs(dy), abs(dz)));
       } else {
         pruned = W;
       }
@@ -1176,8 +1335,8 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
       const unsigned pr = __reduce_add_sync(kFull, unsigned(pruned));
       if (lane == 0) sh.wc[kWcPruned] += pr;
     }
-    const unsigned ne = __ballot_sync(kFull, len > 0);
-    if (!ne) continue;
+    const unsigned hasA = __ballot_sync(kFull, lenA > 0), hasB = __ballot_sync(kFull, lenB > 0);
+    if (!(hasA | hasB)) continue;
     int incl = len;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -1185,68 +1344,89 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
       if (lane >= o) incl += y;
     }
     const int tot = __shfl_sync(kFull, incl, 31);
-    const int excl = incl - len;
+    const int excl = incl - len;  // first candidate position of the row
+    const int exclB = excl + lenA;
     if (STATS && lane == 0) sh.wc[kWcPairs] += unsigned(tot);  // the source itself included
     __syncwarp();
-    if (len > 0) {
-      rw.excl = excl;
-      sh.rows[__popc(ne & lanemask_lt())] = rw;
+    {
+      // the row's runs as segments, in candidate order
+      const int si = __popc(hasA & lt) + __popc(hasB & lt);
+      if (lenA > 0) {
+        SelSeg sg;
+        sg.excl = excl;
+        sg.start = startA;
+        sg.xoff = -ix;
+        sg.meta = (1u << 8) | uint32_t(wbc);
+        sg.Dx = Dx, sg.Dy = Dy, sg.Dz = Dz, sg.syz = syz;
+        sh.segs[si] = sg;
+      }
+      if (lenB > 0) {
+        SelSeg sg;
+        sg.excl = exclB;
+        sg.start = sB;
+        sg.xoff = -ix + wrapB * nx;
+        sg.meta = (uint32_t(wrapB + 1) << 8) | uint32_t(wbc);
+        sg.Dx = Dx, sg.Dy = Dy, sg.Dz = Dz, sg.syz = syz;
+        sh.segs[si + (lenA > 0 ? 1 : 0)] = sg;
+      }
     }
     __syncwarp();
-    // two 32-candidate windows per trip, so their loads are in flight together
-    int before = 0;  // non-empty rows that start before the window
-    const unsigned le = lanemask_lt() | (1u << lane);
-    for (int g0 = 0; g0 < tot; g0 += 64) {
-      const unsigned sa = __reduce_or_sync(
-          kFull, (len > 0 && excl >= g0 && excl < g0 + 32) ? (1u << (excl - g0)) : 0u);
-      const unsigned sb = __reduce_or_sync(
-          kFull, (len > 0 && excl >= g0 + 32 && excl < g0 + 64) ? (1u << (excl - g0 - 32)) : 0u);
-      int t[2], xo[2], owner[2];
-      uint32_t meta[2];
-      bool live[2];
-      owner[0] = before + __popc(sa & le) - 1;
-      owner[1] = before + __popc(sa) + __popc(sb & le) - 1;
-      before += __popc(sa) + __popc(sb);
+    // kSelWin 32-candidate windows per trip, so that their loads are in
+    // flight together; the segment of candidate g is the last one starting
+    // at or before g: one OR-reduction of the segment starts in the window
+    int before = 0;  // segments that start before the window
+    const unsigned le = lt | (1u << lane);
+    auto starts_in = [&](int w0) -> unsigned {
+      unsigned bits = 0;
+      if (lenA > 0 && excl >= w0 && excl < w0 + 32) bits |= 1u << (excl - w0);
+      if (lenB > 0 && exclB >= w0 && exclB < w0 + 32) bits |= 1u << (exclB - w0);
+      return __reduce_or_sync(kFull, bits);
+    };
+    for (int g0 = 0; g0 < tot; g0 += 32 * kSelWin) {
+      int owner[kSelWin];
 #pragma unroll
-      for (int w = 0; w < 2; ++w) {
+      for (int w = 0; w < kSelWin; ++w) {
+        const unsigned sw = starts_in(g0 + 32 * w);
+        owner[w] = before + __popc(sw & le) - 1;
+        before += __popc(sw);
+      }
+      int t[kSelWin];
+      bool live[kSelWin];
+#pragma unroll
+      for (int w = 0; w < kSelWin; ++w) {
         const int g = g0 + 32 * w + lane;
         live[w] = g < tot;
         t[w] = 0;
-        xo[w] = 0;
-        meta[w] = 0;
         if (live[w]) {
-          const SelRow &R = sh.rows[owner[w]];
-          const int loc = g - R.excl;
-          const bool inA = loc < R.lenA;
-          t[w] = (inA ? R.startA : R.startB) + loc;
-          xo[w] = inA ? R.xoffA : R.xoffB;
-          meta[w] = uint32_t(inA ? R.metaA : R.metaB);
+          const SelSeg &S = sh.segs[owner[w]];
+          t[w] = S.start + (g - S.excl);
           live[w] = (long long)t[w] != p;
         }
       }
-      float4 q[2];
+      float4 q[kSelWin];
 #pragma unroll
-      for (int w = 0; w < 2; ++w) q[w] = live[w] ? b.rec[t[w]] : make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int w = 0; w < kSelWin; ++w)
+        q[w] = live[w] ? b.rec[t[w]] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-      for (int w = 0; w < 2; ++w) {
+      for (int w = 0; w < kSelWin; ++w) {
         bool keep = false;
         float d32 = 0.f;
         uint32_t mm = 0;
         if (live[w]) {
-          const SelRow &R = sh.rows[owner[w]];
-          const int dx = __float_as_int(q[w].w) + xo[w];  // the candidate cell's x index
+          const SelSeg &S = sh.segs[owner[w]];
+          const int dx = __float_as_int(q[w].w) + S.xoff;  // the candidate cell's x offset
           const float fdx = float(dx);
-          const float ex = (q[w].x - plx) + fmaf(fdx, ev0, R.Dx);
-          const float ey = (q[w].y - ply) + fmaf(fdx, ev1, R.Dy);
-          const float ez = (q[w].z - plz) + fmaf(fdx, ev2, R.Dz);
+          const float ex = (q[w].x - plx) + fmaf(fdx, ev0, S.Dx);
+          const float ey = (q[w].y - ply) + fmaf(fdx, ev1, S.Dy);
+          const float ez = (q[w].z - plz) + fmaf(fdx, ev2, S.Dz);
           d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
           keep = !(d32 > thr);
-          mm = uint32_t(max(abs(dx), R.syz)) | meta[w];
+          mm = uint32_t(max(abs(dx), S.syz)) | S.meta;
         }
         const unsigned km = __ballot_sync(kFull, keep);
         if (total + __popc(km) > kSelCap) return false;
         if (keep) {
-          const int pos = total + __popc(km & lanemask_lt());
+          const int pos = total + __popc(km & lt);
           sh.d[pos] = d32;
           sh.t[pos] = t[w];
           sh.m[pos] = mm;
@@ -1263,13 +1443,16 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   unsigned long long klo = 0, khi = 0;
   unsigned in_rho = 0;  // first gather: candidates with exact distance <= rho2
   // the level-1 histogram of step 3 for R* = R_p (the common case) on the way
+  // (not needed when the sorted selection takes the buffer: k <= 32 and at
+  // most 64 candidates)
+  const bool use_hist = !(SN == 2 && total <= 64);
   const float spec_hi = partial ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rp];
   const float spec_scale = 32.f / spec_hi;
-  sh.hist[lane] = 0;
+  if (use_hist) sh.hist[lane] = 0;
   __syncwarp();
   for (int i = lane; i < total; i += 32) {
     const float d32 = sh.d[i];
-    if (d32 <= spec_hi) atomicAdd(&sh.hist[min(31, int(d32 * spec_scale))], 1);
+    if (use_hist && d32 <= spec_hi) atomicAdd(&sh.hist[min(31, int(d32 * spec_scale))], 1);
     const int s = int(sh.m[i] & 255u);
     const float rr = sqrtf(d32) * inv_c;
     const float rc = ceilf(rr);
@@ -1308,8 +1491,11 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   }
   const unsigned c12 = __reduce_add_sync(kFull, unsigned(klo));
   const unsigned c34 = __reduce_add_sync(kFull, unsigned(klo >> 32));
-  const unsigned c56 = __reduce_add_sync(kFull, unsigned(khi));
-  const unsigned c78 = __reduce_add_sync(kFull, unsigned(khi >> 32));
+  unsigned c56 = 0, c78 = 0;  // keys above 4 exist only when R_p > 4
+  if (Rp > 4) {
+    c56 = __reduce_add_sync(kFull, unsigned(khi));
+    c78 = __reduce_add_sync(kFull, unsigned(khi >> 32));
+  }
   {
     // reaches below R_p are exact in both gathers; R_p itself from the
     // whole ball, or from the candidates within rho2 after the first
@@ -1335,6 +1521,8 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   else
     { if (STATS && lane == 0) ++sh.wc[kWcExact]; }
   if (STATS && lane == 0) sh.wc[kWcShells] += unsigned(Rs);
+  if (SN == 2 && total <= 64)
+    return select_sorted<SN, STATS>(b, p, lane, sh, fr, total, Rs, Rp, partial);
 
   // 3. select: two-level histogram over candidates of shells <= R* within
   // B(R*) (within rho2 when the first gather settled R* = R_p)

@@ -52,16 +52,19 @@ def test_batched_frames_full_size(gpu, lib, oracle_mod):
     try:
         learn.attach(ws)
         assert lib.lc_gpu_set_graph(ws, 1) == 0
+        # one pair of output buffers: a graph replays while pointers and sizes repeat
+        nn = torch.empty((out_total,), dtype=torch.int32, device="cuda")
+        d2 = torch.empty((out_total,), dtype=torch.float64, device="cuda")
 
         def run(mode):
             assert lib.lc_gpu_set_mode(ws, mode) == 0
-            nn = torch.full((out_total,), -9, dtype=torch.int32, device="cuda")
-            d2 = torch.zeros((out_total,), dtype=torch.float64, device="cuda")
+            nn.fill_(-9)
+            d2.zero_()
             torch.cuda.synchronize()
             rc = lib.lc_gpu_knearest_batch(ws, x.data_ptr(), arr, len(frames), m.data_ptr(),
                                            nn.data_ptr(), d2.data_ptr(), 1)
             assert rc == 0, _capi.gpu_error()
-            return nn, d2
+            return nn.clone(), d2.clone()
 
         nn1, d21 = run(2)
         nn2, d22 = run(2)  # replays the graph captured by the first call
