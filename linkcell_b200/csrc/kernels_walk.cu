@@ -1448,57 +1448,6 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   const bool use_hist = !(SN == 2 && total <= 64);
   const float spec_hi = partial ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rp];
   const float spec_scale = 32.f / spec_hi;
-  // After the first gather, reach R < R_p stops the walk only if at least k
-  // candidates of shells <= R lie within B(R); U_R = #{shell <= R, d32 <=
-  // thr(B(R))} bounds that count from above. When every U_R is below k (the
-  // usual case), only the count within rho2 decides, and the exact reach of
-  // each candidate is not needed.
-  bool settled = false;
-  if (partial) {
-    unsigned long long ulo = 0, uhi = 0;
-    if (use_hist) sh.hist[lane] = 0;
-    __syncwarp();
-    for (int i = lane; i < total; i += 32) {
-      const float d32 = sh.d[i];
-      if (use_hist && d32 <= spec_hi) atomicAdd(&sh.hist[min(31, int(d32 * spec_scale))], 1);
-      const int s = int(sh.m[i] & 255u);
-      for (int R = max(1, s); R < Rp; ++R) {
-        if (d32 <= fr.sel_thr[R]) {
-          const unsigned long long one = 1ull << (16 * ((R - 1) & 3));
-          if (R <= 4)
-            ulo += one;
-          else
-            uhi += one;
-        }
-      }
-      if (d32 <= fr.sel_rho_lo[Rp]) {
-        ++in_rho;
-      } else if (!(d32 > fr.sel_rho_hi[Rp])) {
-        const double dex = exact(i);
-        if (STATS) atomicAdd(&sh.wc[kWcRerank], 1ull);
-        in_rho += dex <= fr.sel_rho2[Rp] ? 1u : 0u;
-      }
-    }
-    unsigned u[8];
-    const unsigned u12 = __reduce_add_sync(kFull, unsigned(ulo));
-    const unsigned u34 = __reduce_add_sync(kFull, unsigned(ulo >> 32));
-    unsigned u56 = 0, u78 = 0;
-    if (Rp > 5) {
-      u56 = __reduce_add_sync(kFull, unsigned(uhi));
-      u78 = __reduce_add_sync(kFull, unsigned(uhi >> 32));
-    }
-    u[0] = u12 & 0xffffu, u[1] = u12 >> 16, u[2] = u34 & 0xffffu, u[3] = u34 >> 16;
-    u[4] = u56 & 0xffffu, u[5] = u56 >> 16, u[6] = u78 & 0xffffu, u[7] = u78 >> 16;
-    bool maybe_below = false;
-#pragma unroll
-    for (int R = 1; R < 8; ++R) maybe_below |= R < Rp && u[R - 1] >= unsigned(k);
-    if (!maybe_below) {
-      settled = true;
-      if (__reduce_add_sync(kFull, in_rho) >= unsigned(k)) Rs = Rp;
-    }
-    in_rho = 0;
-  }
-  if (!settled) {
   if (use_hist) sh.hist[lane] = 0;
   __syncwarp();
   for (int i = lane; i < total; i += 32) {
@@ -1559,7 +1508,6 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
     }
   }
   if (Rs == 0 && partial && __reduce_add_sync(kFull, in_rho) >= unsigned(k)) Rs = Rp;
-  }  // exact reaches
   if (Rs != 0) break;
   if (!partial) {
     if (STATS && lane == 0) ++sh.wc[kWcUnder];
