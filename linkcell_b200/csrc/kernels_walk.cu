@@ -1132,10 +1132,8 @@ __device__ bool select_sorted(const BatchBuffers &b, long long p, int lane, SelS
     const int i = int(key & 63u);
     const int t = sh.t[i];
     const uint32_t m = sh.m[i];
-    double shx, shy, shz;
-    lattice_shift(fr, int((m >> 8) & 3u) - 1, int((m >> 10) & 3u) - 1, int((m >> 12) & 3u) - 1,
-                  shx, shy, shz);
-    d = dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], shx, shy, shz);
+    const double *sh3 = fr.shift27[((m >> 8) & 3u) * 9 + ((m >> 10) & 3u) * 3 + ((m >> 12) & 3u)];
+    d = dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], sh3[0], sh3[1], sh3[2]);
     j = b.sidx[t];
   };
   double da = pinf(), db = pinf();
@@ -1251,10 +1249,9 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   auto exact = [&](int i) -> double {
     const int t = sh.t[i];
     const uint32_t m = sh.m[i];
-    double shx, shy, shz;
-    lattice_shift(fr, int((m >> 8) & 3u) - 1, int((m >> 10) & 3u) - 1, int((m >> 12) & 3u) - 1, shx,
-                  shy, shz);
-    return dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], shx, shy, shz);
+    const double *sh3 = fr.shift27[((m >> 8) & 3u) * 9 + ((m >> 10) & 3u) * 3 + ((m >> 12) & 3u)];
+    return dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], sh3[0], sh3[1],
+                         sh3[2]);
   };
   // The first gather covers only rho2 = max(B(R_p - 1), q B(R_p)): every
   // candidate of the reaches below R_p, and usually the k nearest. It
@@ -1424,14 +1421,15 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
           mm = uint32_t(max(abs(dx), S.syz)) | S.meta;
         }
         const unsigned km = __ballot_sync(kFull, keep);
-        if (total + __popc(km) > kSelCap) return false;
+        const int nk = __popc(km);
+        if (total + nk > kSelCap) return false;
         if (keep) {
           const int pos = total + __popc(km & lt);
           sh.d[pos] = d32;
           sh.t[pos] = t[w];
           sh.m[pos] = mm;
         }
-        total += __popc(km);
+        total += nk;
       }
     }
   }
@@ -1693,9 +1691,9 @@ __global__ void __launch_bounds__(WARPS * 32, sel_warps_per_sm<SN>() / WARPS)
     if (lane == 0) base = atomicAdd(b.work, uint32_t(grab));
     base = __shfl_sync(kFull, base, 0);
     if ((long long)base >= total) break;
-    for (int q = 0; q < grab; ++q) {
-      if ((long long)base + q >= total) break;
-      const long long p = walk_source_at(b, (long long)base + q);
+    const long long end = min(total, (long long)base + grab);
+    for (long long src = base; src < end; ++src) {
+      const long long p = walk_source_at(b, src);
       if (p < 0) continue;
       const unsigned long long tie = STATS ? sh.wc[kWcReplays] : 0ull;
       if (!select_source<SN, STATS>(b, p, lane, sh)) {

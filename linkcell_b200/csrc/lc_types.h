@@ -84,6 +84,9 @@ struct FrameDesc {
   double sel_rho2[9];
   float sel_rho_thr[9], sel_rho_qlim[9], sel_rho_lo[9], sel_rho_hi[9], sel_rho_bhi[9];
   double inv_nx, inv_nxy;  // 1 / nx, 1 / (nx ny) for exact quotient estimates
+  // Cell::lattice_shift of the 27 wrap triples (na, nb, nc) in {-1, 0, 1}^3
+  // at index (na + 1) 9 + (nb + 1) 3 + (nc + 1), in the reference expression
+  double shift27[27][3];
 };
 
 // ------------------------------------------------------------ exact FP64

@@ -232,6 +232,9 @@ __host__ __device__ int plan_cell(const double *rows, const double *origin, doub
   // generous: 2^-36 of the largest coordinate / shift magnitude per unit wrap
   fd.eps64 = ldexp(mag, -36);
   fill_select(fd, rho_q);
+  for (int t = 0; t < 27; ++t)
+    lattice_shift(fd, t / 9 - 1, (t / 3) % 3 - 1, t % 3 - 1, fd.shift27[t][0], fd.shift27[t][1],
+                  fd.shift27[t][2]);
   return kPlanOk;
 }
 
