@@ -996,10 +996,12 @@ __global__ void __launch_bounds__(256, 2) k_team_walk(BatchBuffers b) {
 constexpr int kSelCap = 256;   // FP32-filtered candidates per warp (smem left to L1)
 constexpr int kSelWin = 2;     // 32-candidate windows a gather trip loads at once
 // Warps per block (the autotuner picks among two per S size): 8 or 4 for
-// k <= 32 (24 warps per SM, register bound), 4 or 2 for k <= 64 (20 warps
-// per SM, bound by the larger S buffers in shared memory).
+// k <= 32, 4 or 2 for k <= 64. Resident warps per SM: 32 for k <= 32 (64
+// registers, a few bytes spilled) and 28 for k <= 64; more warps hide the
+// walk's dependency chains better than the registers they cost (4M k = 32:
+// 8.28 ms at 24 warps, 7.99 ms at 32; k = 64: 16.0 ms at 20, 14.5 ms at 28).
 template <int SN>
-constexpr int sel_warps_per_sm() { return SN == 2 ? 24 : 20; }
+constexpr int sel_warps_per_sm() { return SN == 2 ? 32 : 28; }
 template <int SN>
 constexpr int sel_default_warps() { return SN == 2 ? 8 : 4; }
 
@@ -1102,18 +1104,19 @@ __device__ __forceinline__ uint32_t quot(uint32_t x, uint32_t n, double inv) {
 //    the source to the literal replay, as in the histogram path.
 template <int SN, bool STATS>
 __device__ bool select_sorted(const BatchBuffers &b, long long p, int lane, SelShared<SN> &sh,
-                              const FrameDesc &fr, int total, int Rs, int Rp, bool partial) {
+                              const FrameDesc &fr, int o, int total, int Rs, int Rp, bool partial) {
   const int k = fr.k;
   const float Bs_hi = (partial && Rs == Rp) ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rs];
   const float beta_s = fr.sel_beta[Rs];
   uint32_t ka = 0xffffffffu, kb = 0xffffffffu;
   if (lane < total) {
-    const float d = sh.d[lane];
-    if (int(sh.m[lane] & 255u) <= Rs && d <= Bs_hi) ka = (__float_as_uint(d) & ~63u) | uint32_t(lane);
+    const float d = sh.d[o + lane];
+    if (int(sh.m[o + lane] & 255u) <= Rs && d <= Bs_hi)
+      ka = (__float_as_uint(d) & ~63u) | uint32_t(lane);
   }
   if (lane + 32 < total) {
-    const float d = sh.d[lane + 32];
-    if (int(sh.m[lane + 32] & 255u) <= Rs && d <= Bs_hi)
+    const float d = sh.d[o + lane + 32];
+    if (int(sh.m[o + lane + 32] & 255u) <= Rs && d <= Bs_hi)
       kb = (__float_as_uint(d) & ~63u) | uint32_t(lane + 32);
   }
   bitonic64(ka, kb, lane);
@@ -1129,7 +1132,7 @@ __device__ bool select_sorted(const BatchBuffers &b, long long p, int lane, SelS
   if (STATS && lane == 0) sh.wc[kWcRerank] += unsigned(nS);
   // exact distances and indices of S (positions lane and lane + 32)
   auto exact_at = [&](uint32_t key, double &d, int &j) {
-    const int i = int(key & 63u);
+    const int i = o + int(key & 63u);
     const int t = sh.t[i];
     const uint32_t m = sh.m[i];
     const double *sh3 = fr.shift27[((m >> 8) & 3u) * 9 + ((m >> 10) & 3u) * 3 + ((m >> 12) & 3u)];
@@ -1218,6 +1221,274 @@ __device__ bool select_sorted(const BatchBuffers &b, long long p, int lane, SelS
   return true;
 }
 
+// Step 2 of the select walk for the candidates of buffer entries
+// [o, o + total) of source p: the stop reach R* (0 when no reach up to the
+// proposal qualifies from this gather).
+template <int SN, bool STATS>
+__device__ int sel_reach(const BatchBuffers &b, long long p, int lane, SelShared<SN> &sh,
+                         const FrameDesc &fr, int o, int total, int Rp, bool partial) {
+  const int k = fr.k;
+  const double cell_min = fr.cell_min;
+  // exact distance of buffer entry i (absolute index)
+  auto exact = [&](int i) -> double {
+    const int t = sh.t[i];
+    const uint32_t m = sh.m[i];
+    const double *sh3 = fr.shift27[((m >> 8) & 3u) * 9 + ((m >> 10) & 3u) * 3 + ((m >> 12) & 3u)];
+    return dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], sh3[0], sh3[1],
+                         sh3[2]);
+  };
+  int Rs = 0;
+  // 2. stop reach: key counts packed 16 bits per reach (reaches 1-4 | 5-8)
+  const float inv_c = 1.f / float(cell_min);
+  const float eps_r = fr.sel_epsr[Rp];
+  unsigned long long klo = 0, khi = 0;
+  unsigned in_rho = 0;  // first gather: candidates with exact distance <= rho2
+  // the level-1 histogram of step 3 for R* = R_p (the common case) on the way
+  // (not needed when the sorted selection takes the buffer: k <= 32 and at
+  // most 64 candidates)
+  const bool use_hist = !(SN == 2 && total <= 64);
+  const float spec_hi = partial ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rp];
+  const float spec_scale = 32.f / spec_hi;
+  if (use_hist) sh.hist[lane] = 0;
+  __syncwarp();
+  for (int i = lane; i < total; i += 32) {
+    const float d32 = sh.d[o + i];
+    if (use_hist && d32 <= spec_hi) atomicAdd(&sh.hist[min(31, int(d32 * spec_scale))], 1);
+    const int s = int(sh.m[o + i] & 255u);
+    const float rr = sqrtf(d32) * inv_c;
+    const float rc = ceilf(rr);
+    int bR;
+    double dex = -1.0;
+    if (rr <= 1.f - eps_r) {
+      bR = 1;
+    } else if (rc - rr < eps_r || rr - (rc - 1.f) < eps_r) {
+      dex = exact(o + i);
+      if (STATS) atomicAdd(&sh.wc[kWcRerank], 1ull);
+      int R = max(1, int(rc) - 1);
+      while (R <= Rp && !(dex <= stop_bound(R, cell_min))) ++R;
+      bR = R;
+    } else {
+      bR = int(rc);
+    }
+    if (partial) {
+      if (d32 <= fr.sel_rho_lo[Rp]) {
+        ++in_rho;
+      } else if (!(d32 > fr.sel_rho_hi[Rp])) {
+        if (dex < 0.0) {
+          dex = exact(o + i);
+          if (STATS) atomicAdd(&sh.wc[kWcRerank], 1ull);
+        }
+        in_rho += dex <= fr.sel_rho2[Rp] ? 1u : 0u;
+      }
+    }
+    const int key = max(s, bR);
+    if (key <= Rp) {
+      const unsigned long long one = 1ull << (16 * ((key - 1) & 3));
+      if (key <= 4)
+        klo += one;
+      else
+        khi += one;
+    }
+  }
+  const unsigned c12 = __reduce_add_sync(kFull, unsigned(klo));
+  const unsigned c34 = __reduce_add_sync(kFull, unsigned(klo >> 32));
+  unsigned c56 = 0, c78 = 0;  // keys above 4 exist only when R_p > 4
+  if (Rp > 4) {
+    c56 = __reduce_add_sync(kFull, unsigned(khi));
+    c78 = __reduce_add_sync(kFull, unsigned(khi >> 32));
+  }
+  {
+    // reaches below R_p are exact in both gathers; R_p itself from the
+    // whole ball, or from the candidates within rho2 after the first
+    unsigned cum = 0;
+#pragma unroll
+    for (int R = 1; R <= 8; ++R) {
+      const unsigned w = R <= 2 ? c12 : (R <= 4 ? c34 : (R <= 6 ? c56 : c78));
+      cum += (R & 1) ? (w & 0xffffu) : (w >> 16);
+      if (Rs == 0 && (partial ? R < Rp : R <= Rp) && cum >= unsigned(k)) Rs = R;
+    }
+  }
+  if (Rs == 0 && partial && __reduce_add_sync(kFull, in_rho) >= unsigned(k)) Rs = Rp;
+  return Rs;
+}
+
+// Steps 3-4 of the select walk for the candidates of buffer entries
+// [o, o + total) of source p with stop reach Rs: writes the row, or returns
+// false when the source must go to the literal replay.
+template <int SN, bool STATS>
+__device__ bool sel_finish(const BatchBuffers &b, long long p, int lane, SelShared<SN> &sh,
+                           const FrameDesc &fr, int o, int total, int Rs, int Rp, bool partial) {
+  const int k = fr.k;
+  const double cell_min = fr.cell_min;
+  // exact distance of buffer entry i (absolute index)
+  auto exact = [&](int i) -> double {
+    const int t = sh.t[i];
+    const uint32_t m = sh.m[i];
+    const double *sh3 = fr.shift27[((m >> 8) & 3u) * 9 + ((m >> 10) & 3u) * 3 + ((m >> 12) & 3u)];
+    return dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], sh3[0], sh3[1],
+                         sh3[2]);
+  };
+  if (Rs < Rp)
+    { if (STATS && lane == 0) ++sh.wc[kWcOver]; }
+  else
+    { if (STATS && lane == 0) ++sh.wc[kWcExact]; }
+  if (STATS && lane == 0) sh.wc[kWcShells] += unsigned(Rs);
+  if (SN == 2 && total <= 64)
+    return select_sorted<SN, STATS>(b, p, lane, sh, fr, o, total, Rs, Rp, partial);
+
+  // 3. select: two-level histogram over candidates of shells <= R* within
+  // B(R*) (within rho2 when the first gather settled R* = R_p)
+  const float Bs_hi = (partial && Rs == Rp) ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rs];
+  const float beta_s = fr.sel_beta[Rs];  // candidates of shells <= R* have offsets <= R*
+  const float scale = 32.f / Bs_hi;
+  sh.hmax[lane] = 0u;
+  __syncwarp();
+  if (Rs != Rp) {  // the histogram built with the stop reach assumed R* = R_p
+    sh.hist[lane] = 0;
+    __syncwarp();
+    for (int i = lane; i < total; i += 32) {
+      const float d32 = sh.d[o + i];
+      if (int(sh.m[o + i] & 255u) <= Rs && d32 <= Bs_hi)
+        atomicAdd(&sh.hist[min(31, int(d32 * scale))], 1);
+    }
+    __syncwarp();
+  }
+  int bstar, need;
+  {
+    const int c = sh.hist[lane];
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const unsigned reach = __ballot_sync(kFull, incl >= k);
+    if (!reach) return false;  // cannot happen: R* guarantees k candidates within B(R*)
+    bstar = __ffs(reach) - 1;
+    need = k - (__shfl_sync(kFull, incl, bstar) - __shfl_sync(kFull, c, bstar));
+  }
+  __syncwarp();
+  sh.hist[lane] = 0;
+  __syncwarp();
+  for (int i = lane; i < total; i += 32) {
+    const float d32 = sh.d[o + i];
+    if (int(sh.m[o + i] & 255u) > Rs || !(d32 <= Bs_hi)) continue;
+    const float x = d32 * scale;
+    if (min(31, int(x)) != bstar) continue;
+    const int sub = min(31, int((x - float(bstar)) * 32.f));
+    atomicAdd(&sh.hist[sub], 1);
+    atomicMax(&sh.hmax[sub], __float_as_uint(d32));
+  }
+  __syncwarp();
+  float T;
+  {
+    const int c = sh.hist[lane];
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const unsigned reach = __ballot_sync(kFull, incl >= need);
+    if (!reach) return false;  // cannot happen
+    const int b2 = __ffs(reach) - 1;
+    // buckets below bstar hold smaller values than every value of bstar
+    T = __uint_as_float(__reduce_max_sync(kFull, lane <= b2 ? sh.hmax[lane] : 0u));
+  }
+  const float TS = fminf(__fadd_ru(T, __fmul_ru(3.f, __fmaf_ru(T, 8.f * kU32, beta_s))), Bs_hi);
+
+  // S = shells <= R*, d32 <= TS: buffer positions compacted first, then every
+  // lane recomputes its S elements in exact FP64 at once
+  int nS = 0;
+  for (int i0 = 0; i0 < total; i0 += 32) {
+    const int i = i0 + lane;
+    const bool in = i < total && int(sh.m[o + i] & 255u) <= Rs && sh.d[o + i] <= TS;
+    const unsigned m = __ballot_sync(kFull, in);
+    if (nS + __popc(m) > 32 * SN) return false;  // S larger than the row buffer
+    if (in) sh.si[nS + __popc(m & lanemask_lt())] = o + i;
+    nS += __popc(m);
+  }
+  __syncwarp();
+  if (nS < k) return false;  // cannot happen: T bounds k candidates
+  if (STATS && lane == 0) sh.wc[kWcRerank] += unsigned(nS);
+  double ed[SN];
+  int ej[SN];
+#pragma unroll
+  for (int h = 0; h < SN; ++h) {
+    const int q = lane + 32 * h;
+    ed[h] = pinf();
+    ej[h] = 0x7fffffff;
+    if (q < nS) {
+      const int i = sh.si[q];
+      ed[h] = exact(i);
+      ej[h] = b.sidx[sh.t[i]];
+      sh.sd[q] = ed[h];
+      sh.sj[q] = ej[h];
+    }
+  }
+  __syncwarp();
+  // 4. rank of each element in (d2, index) order; the first k are the row.
+  // Element q sits in lane q % 32, group q / 32. A group of many elements
+  // counts in one pass over S, each lane for its own element; a group of a
+  // few (the elements past 32 when S barely exceeds k = 32) is ranked one
+  // element at a time by the whole warp: every lane compares its elements
+  // with it and a warp sum adds the comparisons up. (Empty slots hold
+  // (+inf, INT_MAX) and never count.)
+  int rk[SN];
+#pragma unroll
+  for (int h = 0; h < SN; ++h) {
+    rk[h] = 0;
+    const int cnt = min(nS - 32 * h, 32);
+    if (cnt <= 0) continue;
+    if (cnt >= 16) {
+      int e = 0;
+      for (; e + 2 <= nS; e += 2) {
+        const double d0 = sh.sd[e], d1 = sh.sd[e + 1];
+        const int j0 = sh.sj[e], j1 = sh.sj[e + 1];
+        rk[h] += (lex_less(d0, j0, ed[h], ej[h]) ? 1 : 0) + (lex_less(d1, j1, ed[h], ej[h]) ? 1 : 0);
+      }
+      if (e < nS) rk[h] += lex_less(sh.sd[e], sh.sj[e], ed[h], ej[h]) ? 1 : 0;
+    } else {
+      for (int q = 32 * h; q < 32 * h + cnt; ++q) {
+        const double dq = sh.sd[q];
+        const int jq = sh.sj[q];
+        int c = 0;
+#pragma unroll
+        for (int g = 0; g < SN; ++g) c += lex_less(ed[g], ej[g], dq, jq) ? 1 : 0;
+        const int r = int(__reduce_add_sync(kFull, unsigned(c)));
+        if (lane == q - 32 * h) rk[h] = r;
+      }
+    }
+  }
+  const FrameDesc &frr = fr;
+  const int i = b.sidx[p];
+  int *row = b.out_nn + frr.out_base + (long long)i * k;
+  double *drow = b.out_d2 ? b.out_d2 + frr.out_base + (long long)i * k : nullptr;
+#pragma unroll
+  for (int h = 0; h < SN; ++h) {
+    if (lane + 32 * h < nS) {
+      if (rk[h] == k - 1) sh.hmax[0] = __double2loint(ed[h]), sh.hmax[1] = __double2hiint(ed[h]);
+      if (rk[h] == k) sh.hmax[2] = __double2loint(ed[h]), sh.hmax[3] = __double2hiint(ed[h]);
+    }
+  }
+  __syncwarp();
+  // a tie across the k-th slot: the k-th and (k+1)-th values are equal
+  if (nS > k && sh.hmax[0] == sh.hmax[2] && sh.hmax[1] == sh.hmax[3]) {
+    if (STATS && lane == 0) ++sh.wc[kWcReplays];
+    return false;
+  }
+#pragma unroll
+  for (int h = 0; h < SN; ++h) {
+    if (lane + 32 * h < nS && rk[h] < k) {
+      row[rk[h]] = ej[h];
+      if (drow) drow[rk[h]] = ed[h];
+    }
+  }
+  if (b.stop_log && lane == 0) b.stop_log[p] = int8_t(Rs);
+  if (STATS && lane == 0) sh.wc[kWcInserts] += unsigned(k);
+  return true;
+}
+
 // One source; false: the source must go to the literal replay. STATS: count
 // the walk statistics (lc_gpu_set_stats; they cost about 3 % of the walk).
 template <int SN, bool STATS>
@@ -1237,22 +1508,12 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   const int iy = int(qy - iz_ * uint32_t(ny));
   const int iz = int(iz_);
   const long long cb = fr.cell_base;
-  const double cell_min = fr.cell_min;
   const float4 r = b.rec[p];
   const float plx = r.x, ply = r.y, plz = r.z;
   const float fa = fr.nhinv[0] * plx + fr.nhinv[1] * ply + fr.nhinv[2] * plz;
   const float fb = fr.nhinv[3] * plx + fr.nhinv[4] * ply + fr.nhinv[5] * plz;
   const float fc = fr.nhinv[6] * plx + fr.nhinv[7] * ply + fr.nhinv[8] * plz;
   const float ev0 = fr.ev[0], ev1 = fr.ev[1], ev2 = fr.ev[2];
-  // exact distance of buffer entry i (the source's coordinates read when
-  // needed: they stay out of the registers the gather uses)
-  auto exact = [&](int i) -> double {
-    const int t = sh.t[i];
-    const uint32_t m = sh.m[i];
-    const double *sh3 = fr.shift27[((m >> 8) & 3u) * 9 + ((m >> 10) & 3u) * 3 + ((m >> 12) & 3u)];
-    return dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], sh3[0], sh3[1],
-                         sh3[2]);
-  };
   // The first gather covers only rho2 = max(B(R_p - 1), q B(R_p)): every
   // candidate of the reaches below R_p, and usually the k nearest. It
   // settles R* = R_p when at least k candidates lie within rho2 (their
@@ -1435,77 +1696,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   }
   __syncwarp();
 
-  // 2. stop reach: key counts packed 16 bits per reach (reaches 1-4 | 5-8)
-  const float inv_c = 1.f / float(cell_min);
-  const float eps_r = fr.sel_epsr[Rp];
-  unsigned long long klo = 0, khi = 0;
-  unsigned in_rho = 0;  // first gather: candidates with exact distance <= rho2
-  // the level-1 histogram of step 3 for R* = R_p (the common case) on the way
-  // (not needed when the sorted selection takes the buffer: k <= 32 and at
-  // most 64 candidates)
-  const bool use_hist = !(SN == 2 && total <= 64);
-  const float spec_hi = partial ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rp];
-  const float spec_scale = 32.f / spec_hi;
-  if (use_hist) sh.hist[lane] = 0;
-  __syncwarp();
-  for (int i = lane; i < total; i += 32) {
-    const float d32 = sh.d[i];
-    if (use_hist && d32 <= spec_hi) atomicAdd(&sh.hist[min(31, int(d32 * spec_scale))], 1);
-    const int s = int(sh.m[i] & 255u);
-    const float rr = sqrtf(d32) * inv_c;
-    const float rc = ceilf(rr);
-    int bR;
-    double dex = -1.0;
-    if (rr <= 1.f - eps_r) {
-      bR = 1;
-    } else if (rc - rr < eps_r || rr - (rc - 1.f) < eps_r) {
-      dex = exact(i);
-      if (STATS) atomicAdd(&sh.wc[kWcRerank], 1ull);
-      int R = max(1, int(rc) - 1);
-      while (R <= Rp && !(dex <= stop_bound(R, cell_min))) ++R;
-      bR = R;
-    } else {
-      bR = int(rc);
-    }
-    if (partial) {
-      if (d32 <= fr.sel_rho_lo[Rp]) {
-        ++in_rho;
-      } else if (!(d32 > fr.sel_rho_hi[Rp])) {
-        if (dex < 0.0) {
-          dex = exact(i);
-          if (STATS) atomicAdd(&sh.wc[kWcRerank], 1ull);
-        }
-        in_rho += dex <= fr.sel_rho2[Rp] ? 1u : 0u;
-      }
-    }
-    const int key = max(s, bR);
-    if (key <= Rp) {
-      const unsigned long long one = 1ull << (16 * ((key - 1) & 3));
-      if (key <= 4)
-        klo += one;
-      else
-        khi += one;
-    }
-  }
-  const unsigned c12 = __reduce_add_sync(kFull, unsigned(klo));
-  const unsigned c34 = __reduce_add_sync(kFull, unsigned(klo >> 32));
-  unsigned c56 = 0, c78 = 0;  // keys above 4 exist only when R_p > 4
-  if (Rp > 4) {
-    c56 = __reduce_add_sync(kFull, unsigned(khi));
-    c78 = __reduce_add_sync(kFull, unsigned(khi >> 32));
-  }
-  {
-    // reaches below R_p are exact in both gathers; R_p itself from the
-    // whole ball, or from the candidates within rho2 after the first
-    unsigned cum = 0;
-#pragma unroll
-    for (int R = 1; R <= 8; ++R) {
-      const unsigned w = R <= 2 ? c12 : (R <= 4 ? c34 : (R <= 6 ? c56 : c78));
-      cum += (R & 1) ? (w & 0xffffu) : (w >> 16);
-      if (Rs == 0 && (partial ? R < Rp : R <= Rp) && cum >= unsigned(k)) Rs = R;
-    }
-  }
-  if (Rs == 0 && partial && __reduce_add_sync(kFull, in_rho) >= unsigned(k)) Rs = Rp;
+  Rs = sel_reach<SN, STATS>(b, p, lane, sh, fr, 0, total, Rp, partial);
   if (Rs != 0) break;
   if (!partial) {
     if (STATS && lane == 0) ++sh.wc[kWcUnder];
@@ -1514,165 +1705,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   if (STATS && lane == 0) ++sh.wc[kWcRegather];
   __syncwarp();
   }  // gathers
-  if (Rs < Rp)
-    { if (STATS && lane == 0) ++sh.wc[kWcOver]; }
-  else
-    { if (STATS && lane == 0) ++sh.wc[kWcExact]; }
-  if (STATS && lane == 0) sh.wc[kWcShells] += unsigned(Rs);
-  if (SN == 2 && total <= 64)
-    return select_sorted<SN, STATS>(b, p, lane, sh, fr, total, Rs, Rp, partial);
-
-  // 3. select: two-level histogram over candidates of shells <= R* within
-  // B(R*) (within rho2 when the first gather settled R* = R_p)
-  const float Bs_hi = (partial && Rs == Rp) ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rs];
-  const float beta_s = fr.sel_beta[Rs];  // candidates of shells <= R* have offsets <= R*
-  const float scale = 32.f / Bs_hi;
-  sh.hmax[lane] = 0u;
-  __syncwarp();
-  if (Rs != Rp) {  // the histogram built with the stop reach assumed R* = R_p
-    sh.hist[lane] = 0;
-    __syncwarp();
-    for (int i = lane; i < total; i += 32) {
-      const float d32 = sh.d[i];
-      if (int(sh.m[i] & 255u) <= Rs && d32 <= Bs_hi)
-        atomicAdd(&sh.hist[min(31, int(d32 * scale))], 1);
-    }
-    __syncwarp();
-  }
-  int bstar, need;
-  {
-    const int c = sh.hist[lane];
-    int incl = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o) incl += y;
-    }
-    const unsigned reach = __ballot_sync(kFull, incl >= k);
-    if (!reach) return false;  // cannot happen: R* guarantees k candidates within B(R*)
-    bstar = __ffs(reach) - 1;
-    need = k - (__shfl_sync(kFull, incl, bstar) - __shfl_sync(kFull, c, bstar));
-  }
-  __syncwarp();
-  sh.hist[lane] = 0;
-  __syncwarp();
-  for (int i = lane; i < total; i += 32) {
-    const float d32 = sh.d[i];
-    if (int(sh.m[i] & 255u) > Rs || !(d32 <= Bs_hi)) continue;
-    const float x = d32 * scale;
-    if (min(31, int(x)) != bstar) continue;
-    const int sub = min(31, int((x - float(bstar)) * 32.f));
-    atomicAdd(&sh.hist[sub], 1);
-    atomicMax(&sh.hmax[sub], __float_as_uint(d32));
-  }
-  __syncwarp();
-  float T;
-  {
-    const int c = sh.hist[lane];
-    int incl = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o) incl += y;
-    }
-    const unsigned reach = __ballot_sync(kFull, incl >= need);
-    if (!reach) return false;  // cannot happen
-    const int b2 = __ffs(reach) - 1;
-    // buckets below bstar hold smaller values than every value of bstar
-    T = __uint_as_float(__reduce_max_sync(kFull, lane <= b2 ? sh.hmax[lane] : 0u));
-  }
-  const float TS = fminf(__fadd_ru(T, __fmul_ru(3.f, __fmaf_ru(T, 8.f * kU32, beta_s))), Bs_hi);
-
-  // S = shells <= R*, d32 <= TS: buffer positions compacted first, then every
-  // lane recomputes its S elements in exact FP64 at once
-  int nS = 0;
-  for (int i0 = 0; i0 < total; i0 += 32) {
-    const int i = i0 + lane;
-    const bool in = i < total && int(sh.m[i] & 255u) <= Rs && sh.d[i] <= TS;
-    const unsigned m = __ballot_sync(kFull, in);
-    if (nS + __popc(m) > 32 * SN) return false;  // S larger than the row buffer
-    if (in) sh.si[nS + __popc(m & lanemask_lt())] = i;
-    nS += __popc(m);
-  }
-  __syncwarp();
-  if (nS < k) return false;  // cannot happen: T bounds k candidates
-  if (STATS && lane == 0) sh.wc[kWcRerank] += unsigned(nS);
-  double ed[SN];
-  int ej[SN];
-#pragma unroll
-  for (int h = 0; h < SN; ++h) {
-    const int q = lane + 32 * h;
-    ed[h] = pinf();
-    ej[h] = 0x7fffffff;
-    if (q < nS) {
-      const int i = sh.si[q];
-      ed[h] = exact(i);
-      ej[h] = b.sidx[sh.t[i]];
-      sh.sd[q] = ed[h];
-      sh.sj[q] = ej[h];
-    }
-  }
-  __syncwarp();
-  // 4. rank of each element in (d2, index) order; the first k are the row.
-  // Element q sits in lane q % 32, group q / 32. A group of many elements
-  // counts in one pass over S, each lane for its own element; a group of a
-  // few (the elements past 32 when S barely exceeds k = 32) is ranked one
-  // element at a time by the whole warp: every lane compares its elements
-  // with it and a warp sum adds the comparisons up. (Empty slots hold
-  // (+inf, INT_MAX) and never count.)
-  int rk[SN];
-#pragma unroll
-  for (int h = 0; h < SN; ++h) {
-    rk[h] = 0;
-    const int cnt = min(nS - 32 * h, 32);
-    if (cnt <= 0) continue;
-    if (cnt >= 16) {
-      int e = 0;
-      for (; e + 2 <= nS; e += 2) {
-        const double d0 = sh.sd[e], d1 = sh.sd[e + 1];
-        const int j0 = sh.sj[e], j1 = sh.sj[e + 1];
-        rk[h] += (lex_less(d0, j0, ed[h], ej[h]) ? 1 : 0) + (lex_less(d1, j1, ed[h], ej[h]) ? 1 : 0);
-      }
-      if (e < nS) rk[h] += lex_less(sh.sd[e], sh.sj[e], ed[h], ej[h]) ? 1 : 0;
-    } else {
-      for (int q = 32 * h; q < 32 * h + cnt; ++q) {
-        const double dq = sh.sd[q];
-        const int jq = sh.sj[q];
-        int c = 0;
-#pragma unroll
-        for (int g = 0; g < SN; ++g) c += lex_less(ed[g], ej[g], dq, jq) ? 1 : 0;
-        const int r = int(__reduce_add_sync(kFull, unsigned(c)));
-        if (lane == q - 32 * h) rk[h] = r;
-      }
-    }
-  }
-  const FrameDesc &frr = fr;
-  const int i = b.sidx[p];
-  int *row = b.out_nn + frr.out_base + (long long)i * k;
-  double *drow = b.out_d2 ? b.out_d2 + frr.out_base + (long long)i * k : nullptr;
-#pragma unroll
-  for (int h = 0; h < SN; ++h) {
-    if (lane + 32 * h < nS) {
-      if (rk[h] == k - 1) sh.hmax[0] = __double2loint(ed[h]), sh.hmax[1] = __double2hiint(ed[h]);
-      if (rk[h] == k) sh.hmax[2] = __double2loint(ed[h]), sh.hmax[3] = __double2hiint(ed[h]);
-    }
-  }
-  __syncwarp();
-  // a tie across the k-th slot: the k-th and (k+1)-th values are equal
-  if (nS > k && sh.hmax[0] == sh.hmax[2] && sh.hmax[1] == sh.hmax[3]) {
-    if (STATS && lane == 0) ++sh.wc[kWcReplays];
-    return false;
-  }
-#pragma unroll
-  for (int h = 0; h < SN; ++h) {
-    if (lane + 32 * h < nS && rk[h] < k) {
-      row[rk[h]] = ej[h];
-      if (drow) drow[rk[h]] = ed[h];
-    }
-  }
-  if (b.stop_log && lane == 0) b.stop_log[p] = int8_t(Rs);
-  if (STATS && lane == 0) sh.wc[kWcInserts] += unsigned(k);
-  return true;
+  return sel_finish<SN, STATS>(b, p, lane, sh, fr, 0, total, Rs, Rp, partial);
 }
 
 // grab: consecutive sources a warp takes from the work queue at a time
