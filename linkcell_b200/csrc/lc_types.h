@@ -65,7 +65,7 @@ struct FrameDesc {
   long long cell_base;  // first cell of the frame in the batch
   long long out_base;   // first output element (row 0, slot 0)
   long long mask_base;  // offset of the frame's mask (shared masks repeat 0)
-  long long seg_base;  // first 32-cell row segment of the frame (shell proposals)
+  long long tile_base;  // first 32 x 4-cell tile of the frame (shell proposals)
   // Cube select walk, per reach R = 1..8 (index R): the FP32 filter at
   // B(R) = (R cell_min)^2, the row-trimming limit thr / (0.99 lam_min), the
   // FP32 error offset beta (rounded up), B(R) + 2 band(B(R)) rounded up,

@@ -274,6 +274,7 @@ __global__ void k_training_rows(BatchBuffers b, const int8_t *__restrict__ stop_
 // the 16-byte K chunks LBO apart (LBO = rows x 16 B).
 constexpr int kUmmaThreads = 256;   // two warps per lane quarter of tensor memory
 constexpr int kHaloW = 40;          // halves per halo row (36 used: x0 - 2 .. x0 + 33)
+constexpr int kHaloRows = 40;       // halo rows of a tile: 8 y x 5 z
 constexpr uint32_t kTmemCols = 64;  // D1, D2 and D3 share the same columns
 constexpr int kMbarSpin = 1 << 22;  // bounded wait for the tensor cores
 
@@ -282,7 +283,7 @@ struct UmmaShared {
   __half w1[64 * 128];  // chunk c at c * 1024 B, row n at n * 16 B
   __half w2[64 * 64];   // chunk c at c * 1024 B
   __half w3[16 * 64];   // rows 8..15 zero; chunk c at c * 256 B
-  __half halo[4][25 * kHaloW];
+  __half halo[kHaloRows * kHaloW];
   float b1[64], b2[64], b3[16];
   float lg1p[64];       // log(1 + c) for occupancies c < 64
   unsigned long long mbar;
@@ -405,28 +406,28 @@ __device__ __forceinline__ void hidden_to_a(uint32_t taddr, const float *bias, _
   }
 }
 
-// Segment geometry of row segment seg: cells inside the frame (0 past the
-// last segment), first cell, and the frame.
-struct SegInfo {
+// A tile of the shell-proposal network: 32 cells along x (x0 .. x0 + 31)
+// in each of 4 rows y0 .. y0 + 3 of one z plane of one frame (quarter q of
+// the 128 matrix rows = row y0 + q). Tiles are numbered frame by frame
+// (FrameDesc::tile_base), x fastest, then y in steps of 4, then z.
+struct TileInfo {
   const FrameDesc *fr;
-  int ncl, x0, cy, cz;
-  long long c0;
+  int ncl, x0, y0, z0;  // ncl: cells of each row inside the frame (0 past the last tile)
 };
 
-__device__ __forceinline__ SegInfo segment_info(const FrameDesc *__restrict__ frames, int nframes,
-                                                long long seg, long long segs) {
-  SegInfo g;
+__device__ __forceinline__ TileInfo tile_info(const FrameDesc *__restrict__ frames, int nframes,
+                                              long long tile, long long tiles) {
+  TileInfo g;
   g.fr = frames;
   g.ncl = 0;
-  g.x0 = g.cy = g.cz = 0;
-  g.c0 = 0;
-  if (seg >= segs) return g;
+  g.x0 = g.y0 = g.z0 = 0;
+  if (tile >= tiles) return g;
   int f = 0;
   if (nframes > 1) {
     int lo = 0, hi = nframes - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (frames[mid].seg_base <= seg)
+      if (frames[mid].tile_base <= tile)
         lo = mid;
       else
         hi = mid - 1;
@@ -435,41 +436,49 @@ __device__ __forceinline__ SegInfo segment_info(const FrameDesc *__restrict__ fr
   }
   g.fr = &frames[f];
   const FrameDesc &fr = *g.fr;
-  const int per_row = (fr.nx + 31) / 32;
-  const long long ls = seg - fr.seg_base;
-  const int row = int(ls / per_row);
-  g.x0 = int(ls - (long long)row * per_row) * 32;
-  g.cy = row % fr.ny;
-  g.cz = row / fr.ny;
+  const int per_x = (fr.nx + 31) / 32, per_y = (fr.ny + 3) / 4;
+  const long long lt = tile - fr.tile_base;
+  const long long row = lt / per_x;  // (z, y / 4)
+  g.x0 = int(lt - row * per_x) * 32;
+  g.y0 = int(row % per_y) * 4;
+  g.z0 = int(row / per_y);
   g.ncl = min(32, fr.nx - g.x0);
-  g.c0 = fr.cell_base + (long long)row * fr.nx + g.x0;
   return g;
 }
 
-// Rows [y0, y1) of a segment's halo of log(1 + count): 36 columns
-// x0 - 2 .. x0 + 33 of the 5 x 5 (dy, dz) rows around it.
-__device__ __forceinline__ void stage_halo(const SegInfo &g, const uint32_t *__restrict__ count,
-                                           const float *lg1p, __half *halo, int y0, int y1,
-                                           int lane) {
+// The tile's halo of log(1 + count): 36 columns x0 - 2 .. x0 + 33 of the
+// 8 x 5 rows (y0 - 2 .. y0 + 5, z0 - 2 .. z0 + 2), row (yi, zi) at halo row
+// yi * 5 + zi. All threads of the CTA stage it, every load issued before
+// the first is used.
+constexpr int kHaloPer = (kHaloRows * 36 + kUmmaThreads - 1) / kUmmaThreads;
+__device__ __forceinline__ void stage_halo(const TileInfo &g, const uint32_t *__restrict__ count,
+                                           const float *lg1p, __half *halo) {
   if (g.ncl == 0) {
-    for (int yz = y0; yz < y1; ++yz)
-      for (int x = lane; x < 36; x += 32) halo[yz * kHaloW + x] = __float2half_rn(0.f);
+    for (int e = threadIdx.x; e < kHaloRows * 36; e += kUmmaThreads)
+      halo[(e / 36) * kHaloW + e % 36] = __float2half_rn(0.f);
     return;
   }
   const FrameDesc &fr = *g.fr;
   const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
-  const int xa = (nx >= 36) ? wrap_near(g.x0 + lane - 2, nx) : rem_euclid(g.x0 + lane - 2, nx);
-  const int xb = (nx >= 36) ? wrap_near(g.x0 + lane + 30, nx) : rem_euclid(g.x0 + lane + 30, nx);
-  for (int yz = y0; yz < y1; ++yz) {
-    const int jy = wrap_near(g.cy + yz / 5 - 2, ny);
-    const int jz = wrap_near(g.cz + yz % 5 - 2, nz);
-    const uint32_t *crow = count + fr.cell_base + ((long long)jz * ny + jy) * (long long)nx;
-    const uint32_t ca = crow[xa];
-    halo[yz * kHaloW + lane] = __float2half_rn(ca < 64u ? lg1p[ca] : log1pf(float(ca)));
-    if (lane < 4) {
-      const uint32_t cb = crow[xb];
-      halo[yz * kHaloW + 32 + lane] = __float2half_rn(cb < 64u ? lg1p[cb] : log1pf(float(cb)));
+  uint32_t c[kHaloPer];
+#pragma unroll
+  for (int i = 0; i < kHaloPer; ++i) {
+    const int e = threadIdx.x + i * kUmmaThreads;
+    c[i] = 0u;
+    if (e < kHaloRows * 36) {
+      const int r = e / 36, col = e % 36;
+      const int jy = rem_euclid(g.y0 + r / 5 - 2, ny);
+      const int jz = rem_euclid(g.z0 + r % 5 - 2, nz);
+      const int jx = rem_euclid(g.x0 + col - 2, nx);
+      c[i] = count[fr.cell_base + ((long long)jz * ny + jy) * (long long)nx + jx];
     }
+  }
+#pragma unroll
+  for (int i = 0; i < kHaloPer; ++i) {
+    const int e = threadIdx.x + i * kUmmaThreads;
+    if (e < kHaloRows * 36)
+      halo[(e / 36) * kHaloW + e % 36] =
+          __float2half_rn(c[i] < 64u ? lg1p[c[i]] : log1pf(float(c[i])));
   }
 }
 
@@ -555,7 +564,7 @@ __device__ __forceinline__ void write_proposal(uint32_t taddr, const float *b3, 
 // memory (rows 32 w .. 32 w + 31, one 32-cell row segment): each stages half
 // of the segment's halo and features, and takes half of the accumulator
 // columns in the epilogues.
-__global__ void __launch_bounds__(kUmmaThreads, 1) k_cell_proposal_tc(
+__global__ void __launch_bounds__(kUmmaThreads, 3) k_cell_proposal_tc(
     const float *__restrict__ params, const FrameDesc *__restrict__ frames, int nframes,
     const uint32_t *__restrict__ count, float tau, int8_t *__restrict__ cell_prop,
     int *__restrict__ status) {
@@ -605,7 +614,8 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) k_cell_proposal_tc(
   const uint32_t tmem = sh.tmem_base;
   const uint32_t tlane = tmem + (uint32_t(quarter * 32) << 16);  // this warp's lane quarter
   const int m = quarter * 32 + lane;                              // A row = accumulator lane
-  __half *halo = sh.halo[quarter];
+  // this quarter's row y0 + quarter reads halo rows (quarter + dy + 2) 5 + dz + 2
+  const __half *halo = sh.halo + quarter * 5 * kHaloW;
   uint32_t phase = 0;
   bool ok = true;
   auto sync_issue = [&](int layer) {
@@ -623,12 +633,12 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) k_cell_proposal_tc(
   };
 
   const FrameDesc &last = frames[nframes - 1];
-  const long long segs = last.seg_base + (long long)((last.nx + 31) / 32) * last.ny * last.nz;
-  const long long ctas = (segs + 3) / 4;
-  for (long long ct = blockIdx.x; ct < ctas; ct += gridDim.x) {
-    const SegInfo g = segment_info(frames, nframes, ct * 4 + quarter, segs);
-    stage_halo(g, count, sh.lg1p, halo, half ? 13 : 0, half ? 25 : 13, lane);
-    __syncthreads();  // both halves of every halo are in place
+  const long long tiles =
+      last.tile_base + (long long)((last.nx + 31) / 32) * ((last.ny + 3) / 4) * last.nz;
+  for (long long ct = blockIdx.x; ct < tiles; ct += gridDim.x) {
+    const TileInfo g = tile_info(frames, nframes, ct, tiles);
+    stage_halo(g, count, sh.lg1p, sh.halo);
+    __syncthreads();  // the halo is in place
     const unsigned short kfeat = __half_as_ushort(__float2half_rn(float(g.fr->k) / 64.0f));
     if (half)
       build_a1<8, 16>(halo, sh.a, m, lane, kfeat);
@@ -642,7 +652,14 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) k_cell_proposal_tc(
     hidden_to_a(tlane, sh.b2, sh.a, m, half);
     sync_issue(2);
     if (!(ok = wait_products())) break;
-    if (half == 0) write_proposal(tlane, sh.b3, tau, cell_prop, g.c0 + lane, lane < g.ncl);
+    if (half == 0) {
+      const int y = g.y0 + quarter;
+      const FrameDesc &tf = *g.fr;
+      const bool valid = lane < g.ncl && y < tf.ny;
+      const long long cell =
+          tf.cell_base + ((long long)g.z0 * tf.ny + (valid ? y : 0)) * tf.nx + g.x0 + lane;
+      write_proposal(tlane, sh.b3, tau, cell_prop, cell, valid);
+    }
     // the next tile rewrites the halos, A and the accumulators
     tmem_fence_before();
     __syncthreads();

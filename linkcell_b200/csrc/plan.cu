@@ -297,12 +297,12 @@ __global__ void __launch_bounds__(256)
   }
   __syncthreads();
   const long long ncell = (long long)s_fd.nx * s_fd.ny * s_fd.nz;
-  const long long segs = (long long)((s_fd.nx + 31) / 32) * s_fd.ny * s_fd.nz;
+  const long long tiles = (long long)((s_fd.nx + 31) / 32) * ((s_fd.ny + 3) / 4) * s_fd.nz;
   for (int f = threadIdx.x; f < nframes; f += blockDim.x) {
     FrameDesc fd = s_fd;
     fd.pt_base = (long long)f * n;
     fd.cell_base = (long long)f * ncell;
-    fd.seg_base = (long long)f * segs;
+    fd.tile_base = (long long)f * tiles;
     fd.out_base = (long long)f * n * k;
     frames[f] = fd;
   }

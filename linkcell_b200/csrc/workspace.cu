@@ -179,13 +179,13 @@ void WorkspaceImpl::release_all() {
 Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const int *mask,
                         int *out_nn, double *out_d2, bool wait, std::string &detail) {
   const int nf = int(frames.size());
-  long long npts = 0, ncells = 0, segs = 0;
+  long long npts = 0, ncells = 0, ptiles = 0;
   int kmax = 1;
   for (auto &fd : frames) {
     fd.pt_base = npts;
     fd.cell_base = ncells;
-    fd.seg_base = segs;
-    segs += (long long)((fd.nx + 31) / 32) * fd.ny * fd.nz;
+    fd.tile_base = ptiles;  // shell-proposal tiles
+    ptiles += (long long)((fd.nx + 31) / 32) * ((fd.ny + 3) / 4) * fd.nz;
     npts += fd.n;
     ncells += (long long)fd.nx * fd.ny * fd.nz;
     kmax = std::max(kmax, fd.k);
