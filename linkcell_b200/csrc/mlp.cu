@@ -367,18 +367,22 @@ __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// SiLU with the fast division (inference only).
-__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
-
-__device__ __forceinline__ uint32_t pack_h2(float lo, float hi) {
-  const __half2 h = __floats2half2_rn(lo, hi);
-  return *reinterpret_cast<const uint32_t *>(&h);
-}
-
 // Periodic coordinate c for |c - [0, n)| <= 2.
 __device__ __forceinline__ int wrap_near(int c, int n) {
   if (n < 3) return rem_euclid(c, n);
   return c < 0 ? c + n : (c >= n ? c - n : c);
+}
+
+// SiLU of two FP16 values at once: x sigmoid(x) = x (1/2 + tanh(x / 2) / 2),
+// with the hardware tanh approximation on half2.
+__device__ __forceinline__ uint32_t silu_h2(float lo, float hi) {
+  const __half2 x = __floats2half2_rn(lo, hi);
+  const __half2 half = __float2half2_rn(0.5f);
+  const __half2 xh = __hmul2(x, half);
+  uint32_t t;
+  asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(*reinterpret_cast<const uint32_t *>(&xh)));
+  const __half2 y = __hmul2(x, __hfma2(*reinterpret_cast<const __half2 *>(&t), half, half));
+  return *reinterpret_cast<const uint32_t *>(&y);
 }
 
 // Hidden layer epilogue: 32 of row m's 64 accumulators (columns
@@ -392,15 +396,13 @@ __device__ __forceinline__ void hidden_to_a(uint32_t taddr, const float *bias, _
     tmem_wait_ld();
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
+      const float *bq = bias + 16 * q + 8 * h;
+      const float *vq = v + 8 * h;
       uint4 w;
-      w.x = pack_h2(silu_fast(v[8 * h + 0] + bias[16 * q + 8 * h + 0]),
-                    silu_fast(v[8 * h + 1] + bias[16 * q + 8 * h + 1]));
-      w.y = pack_h2(silu_fast(v[8 * h + 2] + bias[16 * q + 8 * h + 2]),
-                    silu_fast(v[8 * h + 3] + bias[16 * q + 8 * h + 3]));
-      w.z = pack_h2(silu_fast(v[8 * h + 4] + bias[16 * q + 8 * h + 4]),
-                    silu_fast(v[8 * h + 5] + bias[16 * q + 8 * h + 5]));
-      w.w = pack_h2(silu_fast(v[8 * h + 6] + bias[16 * q + 8 * h + 6]),
-                    silu_fast(v[8 * h + 7] + bias[16 * q + 8 * h + 7]));
+      w.x = silu_h2(vq[0] + bq[0], vq[1] + bq[1]);
+      w.y = silu_h2(vq[2] + bq[2], vq[3] + bq[3]);
+      w.z = silu_h2(vq[4] + bq[4], vq[5] + bq[5]);
+      w.w = silu_h2(vq[6] + bq[6], vq[7] + bq[7]);
       *reinterpret_cast<uint4 *>(a + (2 * q + h) * 1024 + m * 8) = w;
     }
   }
