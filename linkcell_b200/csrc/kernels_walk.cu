@@ -1043,27 +1043,35 @@ __device__ __forceinline__ float axis_gap(int d, float f) {
   return d > 0 ? float(d) - f : (d < 0 ? f + float(-d - 1) : 0.f);
 }
 
-// Ascending bitonic sort of 64 unsigned keys held two per lane: position q
-// is lane q % 32's ka (q < 32) or kb (q >= 32). Element q trades with q ^ j
-// and keeps the smaller key when (q < q ^ j) matches the ascending blocks of
-// the stage ((q & kk) == 0).
-__device__ __forceinline__ void bitonic64(uint32_t &ka, uint32_t &kb, int lane) {
+// Ascending bitonic sort of 32 H unsigned keys held H per lane: position q
+// is lane q % 32's key[q / 32]. Element q trades with q ^ j and keeps the
+// smaller key when (q < q ^ j) matches the ascending blocks of the stage
+// ((q & kk) == 0); partners 32 or more apart sit in the same lane.
+template <int H>
+__device__ __forceinline__ void bitonic_sort(uint32_t (&key)[H], int lane) {
 #pragma unroll
-  for (int kk = 2; kk <= 64; kk <<= 1) {
+  for (int kk = 2; kk <= 32 * H; kk <<= 1) {
 #pragma unroll
     for (int j = kk >> 1; j > 0; j >>= 1) {
-      if (j == 32) {
-        const uint32_t lo = min(ka, kb), hi = max(ka, kb);
-        ka = lo;
-        kb = hi;
+      if (j >= 32) {
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+          const int hp = h ^ (j >> 5);
+          if (hp > h) {
+            const bool asc = ((lane + 32 * h) & kk) == 0;
+            const uint32_t lo = min(key[h], key[hp]), hi = max(key[h], key[hp]);
+            key[h] = asc ? lo : hi;
+            key[hp] = asc ? hi : lo;
+          }
+        }
       } else {
-        const uint32_t pa = __shfl_xor_sync(kFull, ka, j);
-        const uint32_t pb = __shfl_xor_sync(kFull, kb, j);
-        const bool low = (lane & j) == 0;
-        const bool upa = (lane & kk) == 0;
-        const bool upb = ((lane + 32) & kk) == 0;
-        ka = low == upa ? min(ka, pa) : max(ka, pa);
-        kb = low == upb ? min(kb, pb) : max(kb, pb);
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+          const uint32_t pk = __shfl_xor_sync(kFull, key[h], j);
+          const bool low = (lane & j) == 0;
+          const bool up = ((lane + 32 * h) & kk) == 0;
+          key[h] = low == up ? min(key[h], pk) : max(key[h], pk);
+        }
       }
     }
   }
@@ -1084,119 +1092,180 @@ __device__ __forceinline__ uint32_t quot(uint32_t x, uint32_t n, double inv) {
   return q;
 }
 
-// Steps 3-4 of the select walk when the gathered buffer holds at most 64
-// candidates (k <= 32): a sort instead of histograms and ranking.
+// Steps 3-4 of the select walk when the gathered buffer holds at most 32 H
+// candidates (H = 2 for k <= 32, 4 for k <= 64): a sort instead of
+// histograms and ranking. With s = 6 slot bits for H = 2 and 7 for H = 4,
+// and e = 2^(s - 23) the relative slot error:
 //  - Every eligible candidate (shell <= R*, d32 within the histogram path's
-//    bound) gets the key bits(d32) with its low 6 bits replaced by its buffer
-//    slot: unique, and |key - d32| <= 2^-17 d32. The 64 keys are sorted.
-//  - K = the k-th smallest key: k candidates have d32 <= Tup = K (1 + 2^-16),
+//    bound) gets the key bits(d32) with its low s bits replaced by its buffer
+//    slot: unique, and |key - d32| <= e d32. The 32 H keys are sorted.
+//  - K = the k-th smallest key: k candidates have d32 <= Tup = K (1 + 2e),
 //    so the k-th smallest exact distance v is at most Tup + band(Tup). S =
-//    the sorted prefix with key <= (Tup + 3 band(Tup)) (1 + 2^-16): it holds
+//    the sorted prefix with key <= (Tup + 3 band(Tup)) (1 + 2e): it holds
 //    every candidate whose exact distance is at most Tup + band(Tup) (the k
 //    smallest and everything tied with v), and nothing outside S can tie v
 //    -- the histogram path's argument with the key's error added.
 //  - S is recomputed in exact FP64. Sorted by key, two neighbours can be out
 //    of exact (d2, index) order only if their keys lie within twice the
-//    error bound band''(x) = band(x) + 2^-16 x of each other; the runs of
-//    such linked neighbours (clusters, almost always single elements) are
-//    ranked exactly inside, and every other position is already its rank.
+//    error bound band''(x) = band(x) + 2e x of each other; the runs of such
+//    linked neighbours (clusters, almost always single elements) are ranked
+//    exactly inside, and every other position is already its rank.
 //  - A tie across the k-th slot (equal k-th and (k+1)-th exact values) sends
 //    the source to the literal replay, as in the histogram path.
-template <int SN, bool STATS>
+// The sorted selection takes the buffers of k <= 32 with at most 64
+// candidates (two keys per lane), the histogram path the rest. (Four keys
+// per lane for k <= 64 gave the same rows but a slower 4M walk: 14.88 ms
+// against 14.49 ms with the histograms.)
+template <int SN>
+__device__ __forceinline__ bool sorted_fits(int total) {
+  return SN == 2 && total <= 64;
+}
+
+template <int H, int SN, bool STATS>
 __device__ bool select_sorted(const BatchBuffers &b, long long p, int lane, SelShared<SN> &sh,
                               const FrameDesc &fr, int o, int total, int Rs, int Rp, bool partial) {
+  // kRel = 2e: 2^-16 (H = 2) or 2^-15 (H = 4)
+  constexpr uint32_t kSlotMask = H == 2 ? 63u : 127u;
+  constexpr float kRel = H == 2 ? 1.f / 65536.f : 1.f / 32768.f;
   const int k = fr.k;
   const float Bs_hi = (partial && Rs == Rp) ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rs];
   const float beta_s = fr.sel_beta[Rs];
-  uint32_t ka = 0xffffffffu, kb = 0xffffffffu;
-  if (lane < total) {
-    const float d = sh.d[o + lane];
-    if (int(sh.m[o + lane] & 255u) <= Rs && d <= Bs_hi)
-      ka = (__float_as_uint(d) & ~63u) | uint32_t(lane);
+  uint32_t key[H];
+#pragma unroll
+  for (int h = 0; h < H; ++h) {
+    const int idx = lane + 32 * h;
+    key[h] = 0xffffffffu;
+    if (idx < total) {
+      const float d = sh.d[o + idx];
+      if (int(sh.m[o + idx] & 255u) <= Rs && d <= Bs_hi)
+        key[h] = (__float_as_uint(d) & ~kSlotMask) | uint32_t(idx);
+    }
   }
-  if (lane + 32 < total) {
-    const float d = sh.d[o + lane + 32];
-    if (int(sh.m[o + lane + 32] & 255u) <= Rs && d <= Bs_hi)
-      kb = (__float_as_uint(d) & ~63u) | uint32_t(lane + 32);
-  }
-  bitonic64(ka, kb, lane);
-  const uint32_t kth = __shfl_sync(kFull, k <= 32 ? ka : kb, (k - 1) & 31);
+  bitonic_sort<H>(key, lane);
+  uint32_t kv = key[0];
+#pragma unroll
+  for (int h = 1; h < H; ++h)
+    if (h == (k - 1) >> 5) kv = key[h];
+  const uint32_t kth = __shfl_sync(kFull, kv, (k - 1) & 31);
   if (kth == 0xffffffffu) return false;  // cannot happen: R* guarantees k eligible candidates
-  const float Tup = __fmul_ru(__uint_as_float(kth), 1.f + 1.f / 65536.f);
-  const float TSk = __fmul_ru(__fadd_ru(Tup, __fmul_ru(3.f, __fmaf_ru(Tup, 8.f * kU32, beta_s))),
-                              1.f + 1.f / 65536.f);
+  const float Tup = __fmul_ru(__uint_as_float(kth), 1.f + kRel);
+  const float TSk =
+      __fmul_ru(__fadd_ru(Tup, __fmul_ru(3.f, __fmaf_ru(Tup, 8.f * kU32, beta_s))), 1.f + kRel);
   const uint32_t tsb = __float_as_uint(TSk);
-  const bool inA = ka <= tsb, inB = kb <= tsb;
-  const int nS = __popc(__ballot_sync(kFull, inA)) + __popc(__ballot_sync(kFull, inB));
+  bool in[H];
+  int nS = 0;
+#pragma unroll
+  for (int h = 0; h < H; ++h) {
+    in[h] = key[h] <= tsb;
+    nS += __popc(__ballot_sync(kFull, in[h]));
+  }
   if (nS < k) return false;  // cannot happen
   if (STATS && lane == 0) sh.wc[kWcRerank] += unsigned(nS);
-  // exact distances and indices of S (positions lane and lane + 32)
-  auto exact_at = [&](uint32_t key, double &d, int &j) {
-    const int i = o + int(key & 63u);
-    const int t = sh.t[i];
-    const uint32_t m = sh.m[i];
-    const double *sh3 = fr.shift27[((m >> 8) & 3u) * 9 + ((m >> 10) & 3u) * 3 + ((m >> 12) & 3u)];
-    d = dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], sh3[0], sh3[1], sh3[2]);
-    j = b.sidx[t];
-  };
-  double da = pinf(), db = pinf();
-  int ja = 0x7fffffff, jb = 0x7fffffff;
-  if (inA) exact_at(ka, da, ja);
-  if (nS > 32 && inB) exact_at(kb, db, jb);
+  // exact distances and indices of S (position lane + 32 h)
+  double dd[H];
+  int jj[H];
+#pragma unroll
+  for (int h = 0; h < H; ++h) {
+    dd[h] = pinf();
+    jj[h] = 0x7fffffff;
+    if (32 * h < nS && in[h]) {
+      const int i = o + int(key[h] & kSlotMask);
+      const int t = sh.t[i];
+      const uint32_t m = sh.m[i];
+      const double *sh3 =
+          fr.shift27[((m >> 8) & 3u) * 9 + ((m >> 10) & 3u) * 3 + ((m >> 12) & 3u)];
+      dd[h] = dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], sh3[0], sh3[1],
+                            sh3[2]);
+      jj[h] = b.sidx[t];
+    }
+  }
   // clusters: position q is linked to q - 1 when their keys lie within
-  // 2.01 band''(key_q); starts = positions not linked to their predecessor
+  // 2.01 band''(key_q); starts[h] bit l =
+  // position l + 32 h does not link to its predecessor
   auto linked = [&](uint32_t kq, uint32_t kprev) -> bool {
     const float xq = __uint_as_float(kq), xp = __uint_as_float(kprev);
-    const float bq = __fmaf_ru(xq, 8.f * kU32 + 1.f / 65536.f, beta_s);
+    const float bq = __fmaf_ru(xq, 8.f * kU32 + kRel, beta_s);
     return __fsub_ru(xq, xp) <= __fmul_ru(2.01f, bq);
   };
-  const uint32_t upA = __shfl_up_sync(kFull, ka, 1);
-  const uint32_t lastA = __shfl_sync(kFull, ka, 31);
-  const uint32_t upB = __shfl_up_sync(kFull, kb, 1);
-  const uint32_t prevB = lane == 0 ? lastA : upB;
-  const bool linkA = lane > 0 && lane < nS && linked(ka, upA);
-  const bool linkB = lane + 32 < nS && linked(kb, prevB);
-  const unsigned long long starts =
-      (unsigned long long)__ballot_sync(kFull, !linkA) |
-      ((unsigned long long)__ballot_sync(kFull, !linkB) << 32);
-  const unsigned long long inS = nS >= 64 ? ~0ull : ((1ull << nS) - 1);
-  int rkA = lane, rkB = lane + 32;
-  if (~starts & inS) {
-    // cluster [a, e] of position q: a = the last start <= q, e = the next start - 1
-    auto bounds = [&](int q, int &a, int &e) {
-      const unsigned long long upto = q == 63 ? ~0ull : ((2ull << q) - 1);
-      a = 63 - __clzll(starts & upto);
-      const unsigned long long after = starts & ~upto & inS;
-      e = after ? __ffsll(after) - 2 : nS - 1;
-    };
-    int a0, e0, a1, e1;
-    bounds(lane, a0, e0);
-    bounds(lane + 32, a1, e1);
-    const int s0 = lane < nS ? e0 - a0 + 1 : 1;
-    const int s1 = lane + 32 < nS ? e1 - a1 + 1 : 1;
-    const int M = int(__reduce_max_sync(kFull, unsigned(max(s0, s1))));
-    int c0 = 0, c1 = 0;
-    for (int r = 0; r < M; ++r) {
-      // member r of each element's cluster (positions past the cluster are skipped)
-      const int p0 = min(a0 + r, 63), p1 = min(a1 + r, 63);
-      const double x0a = __shfl_sync(kFull, da, p0 & 31), x0b = __shfl_sync(kFull, db, p0 & 31);
-      const int y0a = __shfl_sync(kFull, ja, p0 & 31), y0b = __shfl_sync(kFull, jb, p0 & 31);
-      const double x1a = __shfl_sync(kFull, da, p1 & 31), x1b = __shfl_sync(kFull, db, p1 & 31);
-      const int y1a = __shfl_sync(kFull, ja, p1 & 31), y1b = __shfl_sync(kFull, jb, p1 & 31);
-      const double x0 = p0 < 32 ? x0a : x0b, x1 = p1 < 32 ? x1a : x1b;
-      const int y0 = p0 < 32 ? y0a : y0b, y1 = p1 < 32 ? y1a : y1b;
-      if (a0 + r <= e0 && lex_less(x0, y0, da, ja)) ++c0;
-      if (a1 + r <= e1 && lex_less(x1, y1, db, jb)) ++c1;
+  unsigned starts[H];
+  bool any_link = false;
+#pragma unroll
+  for (int h = 0; h < H; ++h) {
+    const uint32_t up = __shfl_up_sync(kFull, key[h], 1);
+    const uint32_t last = __shfl_sync(kFull, key[h > 0 ? h - 1 : 0], 31);
+    const uint32_t prev = lane == 0 ? last : up;
+    const int q = lane + 32 * h;
+    const bool link = q > 0 && q < nS && linked(key[h], prev);
+    starts[h] = __ballot_sync(kFull, !link);
+    any_link |= starts[h] != 0xffffffffu && 32 * h < nS;
+  }
+  int rk[H];
+#pragma unroll
+  for (int h = 0; h < H; ++h) rk[h] = lane + 32 * h;
+  if (any_link) {
+    // cluster [a, e] of position q = lane + 32 h: a = the last start <= q,
+    // e = the next start - 1 (or the last position of S)
+    int a[H], e[H], sz = 1;
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+      const unsigned upto = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
+      a[h] = 0;
+      bool found = false;
+#pragma unroll
+      for (int g = H - 1; g >= 0; --g) {
+        if (g > h || found) continue;
+        const unsigned mk = g == h ? (starts[g] & upto) : starts[g];
+        if (mk) {
+          a[h] = 32 * g + 31 - __clz(mk);
+          found = true;
+        }
+      }
+      e[h] = nS - 1;
+      found = false;
+#pragma unroll
+      for (int g = 0; g < H; ++g) {
+        if (g < h || found) continue;
+        const unsigned mk = g == h ? (starts[g] & ~upto) : starts[g];
+        if (mk) {
+          e[h] = min(nS - 1, 32 * g + __ffs(mk) - 2);
+          found = true;
+        }
+      }
+      if (lane + 32 * h < nS) sz = max(sz, e[h] - a[h] + 1);
     }
-    if (lane < nS) rkA = a0 + c0;
-    if (lane + 32 < nS) rkB = a1 + c1;
+    const int M = int(__reduce_max_sync(kFull, unsigned(sz)));
+    int c[H];
+#pragma unroll
+    for (int h = 0; h < H; ++h) c[h] = 0;
+    for (int r = 0; r < M; ++r) {
+#pragma unroll
+      for (int h = 0; h < H; ++h) {
+        // member r of this element's cluster (positions past it are skipped)
+        const int pq = min(a[h] + r, 32 * H - 1);
+        double x = 0.0;
+        int y = 0;
+#pragma unroll
+        for (int g = 0; g < H; ++g) {
+          const double xg = __shfl_sync(kFull, dd[g], pq & 31);
+          const int yg = __shfl_sync(kFull, jj[g], pq & 31);
+          if (g == (pq >> 5)) x = xg, y = yg;
+        }
+        if (a[h] + r <= e[h] && lex_less(x, y, dd[h], jj[h])) ++c[h];
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < H; ++h)
+      if (lane + 32 * h < nS) rk[h] = a[h] + c[h];
   }
   // a tie across the k-th slot: the k-th and (k+1)-th exact values are equal
   if (nS > k) {
-    if (lane < nS && rkA == k - 1) sh.hmax[0] = __double2loint(da), sh.hmax[1] = __double2hiint(da);
-    if (lane + 32 < nS && rkB == k - 1) sh.hmax[0] = __double2loint(db), sh.hmax[1] = __double2hiint(db);
-    if (lane < nS && rkA == k) sh.hmax[2] = __double2loint(da), sh.hmax[3] = __double2hiint(da);
-    if (lane + 32 < nS && rkB == k) sh.hmax[2] = __double2loint(db), sh.hmax[3] = __double2hiint(db);
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+      if (lane + 32 * h < nS && rk[h] == k - 1)
+        sh.hmax[0] = __double2loint(dd[h]), sh.hmax[1] = __double2hiint(dd[h]);
+      if (lane + 32 * h < nS && rk[h] == k)
+        sh.hmax[2] = __double2loint(dd[h]), sh.hmax[3] = __double2hiint(dd[h]);
+    }
     __syncwarp();
     const bool tie = sh.hmax[0] == sh.hmax[2] && sh.hmax[1] == sh.hmax[3];
     __syncwarp();
@@ -1208,13 +1277,12 @@ __device__ bool select_sorted(const BatchBuffers &b, long long p, int lane, SelS
   const int i = b.sidx[p];
   int *row = b.out_nn + fr.out_base + (long long)i * k;
   double *drow = b.out_d2 ? b.out_d2 + fr.out_base + (long long)i * k : nullptr;
-  if (lane < nS && rkA < k) {
-    row[rkA] = ja;
-    if (drow) drow[rkA] = da;
-  }
-  if (lane + 32 < nS && rkB < k) {
-    row[rkB] = jb;
-    if (drow) drow[rkB] = db;
+#pragma unroll
+  for (int h = 0; h < H; ++h) {
+    if (lane + 32 * h < nS && rk[h] < k) {
+      row[rk[h]] = jj[h];
+      if (drow) drow[rk[h]] = dd[h];
+    }
   }
   if (b.stop_log && lane == 0) b.stop_log[p] = int8_t(Rs);
   if (STATS && lane == 0) sh.wc[kWcInserts] += unsigned(k);
@@ -1244,9 +1312,8 @@ __device__ int sel_reach(const BatchBuffers &b, long long p, int lane, SelShared
   unsigned long long klo = 0, khi = 0;
   unsigned in_rho = 0;  // first gather: candidates with exact distance <= rho2
   // the level-1 histogram of step 3 for R* = R_p (the common case) on the way
-  // (not needed when the sorted selection takes the buffer: k <= 32 and at
-  // most 64 candidates)
-  const bool use_hist = !(SN == 2 && total <= 64);
+  // (not needed when the sorted selection takes the buffer)
+  const bool use_hist = !sorted_fits<SN>(total);
   const float spec_hi = partial ? fr.sel_rho_bhi[Rp] : fr.sel_bhi[Rp];
   const float spec_scale = 32.f / spec_hi;
   if (use_hist) sh.hist[lane] = 0;
@@ -1333,8 +1400,8 @@ __device__ bool sel_finish(const BatchBuffers &b, long long p, int lane, SelShar
   else
     { if (STATS && lane == 0) ++sh.wc[kWcExact]; }
   if (STATS && lane == 0) sh.wc[kWcShells] += unsigned(Rs);
-  if (SN == 2 && total <= 64)
-    return select_sorted<SN, STATS>(b, p, lane, sh, fr, o, total, Rs, Rp, partial);
+  if (sorted_fits<SN>(total))
+    return select_sorted<2, SN, STATS>(b, p, lane, sh, fr, o, total, Rs, Rp, partial);
 
   // 3. select: two-level histogram over candidates of shells <= R* within
   // B(R*) (within rho2 when the first gather settled R* = R_p)
