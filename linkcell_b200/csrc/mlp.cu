@@ -277,9 +277,15 @@ constexpr int kHaloW = 40;          // halves per halo row (36 used: x0 - 2 .. x
 constexpr int kHaloRows = 40;       // halo rows of a tile: 8 y x 5 z
 constexpr uint32_t kTmemCols = 64;  // D1, D2 and D3 share the same columns
 constexpr int kMbarSpin = 1 << 22;  // bounded wait for the tensor cores
+// Layer 1's A operand (128 x 128) built and multiplied in two K halves in
+// one 16 KB buffer: shared memory for four CTAs per SM, for one more round
+// trip to the tensor cores per tile.
+constexpr bool kA1Split = true;
+constexpr int kAChunks = kA1Split ? 8 : 16;  // 16-byte K chunks the A buffer holds
+constexpr int kUmmaCtas = kA1Split ? 4 : 3;  // resident CTAs per SM
 
 struct UmmaShared {
-  __half a[128 * 128];  // A1, then A2 and A3 (aliased): chunk c at c * 2048 B, row m at m * 16 B
+  __half a[128 * 8 * kAChunks];  // A1 (or its halves), then A2 and A3: chunk c at c * 2048 B, row m at m * 16 B
   __half w1[64 * 128];  // chunk c at c * 1024 B, row n at n * 16 B
   __half w2[64 * 64];   // chunk c at c * 1024 B
   __half w3[16 * 64];   // rows 8..15 zero; chunk c at c * 256 B
@@ -373,15 +379,14 @@ __device__ __forceinline__ int wrap_near(int c, int n) {
   return c < 0 ? c + n : (c >= n ? c - n : c);
 }
 
-// SiLU of two FP16 values at once: x sigmoid(x) = x (1/2 + tanh(x / 2) / 2),
-// with the hardware tanh approximation on half2.
-__device__ __forceinline__ uint32_t silu_h2(float lo, float hi) {
-  const __half2 x = __floats2half2_rn(lo, hi);
-  const __half2 half = __float2half2_rn(0.5f);
-  const __half2 xh = __hmul2(x, half);
+// SiLU of two values from their halves u = z / 2 (the hidden layers' weights
+// and biases are stored halved): z sigmoid(z) = u (1 + tanh(u)), with the
+// hardware tanh approximation on half2.
+__device__ __forceinline__ uint32_t silu_h2(float ulo, float uhi) {
+  const __half2 u = __floats2half2_rn(ulo, uhi);
   uint32_t t;
-  asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(*reinterpret_cast<const uint32_t *>(&xh)));
-  const __half2 y = __hmul2(x, __hfma2(*reinterpret_cast<const __half2 *>(&t), half, half));
+  asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(*reinterpret_cast<const uint32_t *>(&u)));
+  const __half2 y = __hfma2(u, *reinterpret_cast<const __half2 *>(&t), u);
   return *reinterpret_cast<const uint32_t *>(&y);
 }
 
@@ -438,49 +443,55 @@ __device__ __forceinline__ TileInfo tile_info(const FrameDesc *__restrict__ fram
   }
   g.fr = &frames[f];
   const FrameDesc &fr = *g.fr;
-  const int per_x = (fr.nx + 31) / 32, per_y = (fr.ny + 3) / 4;
-  const long long lt = tile - fr.tile_base;
-  const long long row = lt / per_x;  // (z, y / 4)
+  // a frame has fewer than 2^31 cells, so its tile numbers fit 32 bits
+  const uint32_t per_x = uint32_t(fr.nx + 31) / 32u, per_y = uint32_t(fr.ny + 3) / 4u;
+  const uint32_t lt = uint32_t(tile - fr.tile_base);
+  const uint32_t row = lt / per_x;  // (z, y / 4)
+  const uint32_t zq = row / per_y;
   g.x0 = int(lt - row * per_x) * 32;
-  g.y0 = int(row % per_y) * 4;
-  g.z0 = int(row / per_y);
+  g.y0 = int(row - zq * per_y) * 4;
+  g.z0 = int(zq);
   g.ncl = min(32, fr.nx - g.x0);
   return g;
 }
 
+// Periodic coordinate: one add or subtract for |c - [0, n)| < n, the
+// general remainder otherwise (tiny boxes).
+__device__ __forceinline__ int wrap_cell(int c, int n) {
+  c = c < 0 ? c + n : (c >= n ? c - n : c);
+  return unsigned(c) < unsigned(n) ? c : rem_euclid(c, n);
+}
+
 // The tile's halo of log(1 + count): 36 columns x0 - 2 .. x0 + 33 of the
 // 8 x 5 rows (y0 - 2 .. y0 + 5, z0 - 2 .. z0 + 2), row (yi, zi) at halo row
-// yi * 5 + zi. All threads of the CTA stage it, every load issued before
-// the first is used.
-constexpr int kHaloPer = (kHaloRows * 36 + kUmmaThreads - 1) / kUmmaThreads;
+// yi * 5 + zi. Warp w stages the five rows of yi = w: lane l column l, and
+// lanes 0-3 columns 32-35, all ten loads in flight before the first store.
 __device__ __forceinline__ void stage_halo(const TileInfo &g, const uint32_t *__restrict__ count,
                                            const float *lg1p, __half *halo) {
-  if (g.ncl == 0) {
-    for (int e = threadIdx.x; e < kHaloRows * 36; e += kUmmaThreads)
-      halo[(e / 36) * kHaloW + e % 36] = __float2half_rn(0.f);
-    return;
-  }
-  const FrameDesc &fr = *g.fr;
-  const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
-  uint32_t c[kHaloPer];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t c[10];
 #pragma unroll
-  for (int i = 0; i < kHaloPer; ++i) {
-    const int e = threadIdx.x + i * kUmmaThreads;
-    c[i] = 0u;
-    if (e < kHaloRows * 36) {
-      const int r = e / 36, col = e % 36;
-      const int jy = rem_euclid(g.y0 + r / 5 - 2, ny);
-      const int jz = rem_euclid(g.z0 + r % 5 - 2, nz);
-      const int jx = rem_euclid(g.x0 + col - 2, nx);
-      c[i] = count[fr.cell_base + ((long long)jz * ny + jy) * (long long)nx + jx];
+  for (int i = 0; i < 10; ++i) c[i] = 0u;
+  if (g.ncl > 0) {
+    const FrameDesc &fr = *g.fr;
+    const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
+    const int jy = wrap_cell(g.y0 + warp - 2, ny);
+    const int jx0 = wrap_cell(g.x0 + lane - 2, nx);
+    const int jx1 = wrap_cell(g.x0 + lane + 30, nx);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const int jz = wrap_cell(g.z0 + j - 2, nz);
+      const uint32_t *row = count + fr.cell_base + ((long long)jz * ny + jy) * (long long)nx;
+      c[j] = row[jx0];
+      if (lane < 4) c[5 + j] = row[jx1];
     }
   }
+  auto feat = [&](uint32_t v) { return __float2half_rn(v < 64u ? lg1p[v] : log1pf(float(v))); };
+  __half *h = halo + warp * 5 * kHaloW + lane;
 #pragma unroll
-  for (int i = 0; i < kHaloPer; ++i) {
-    const int e = threadIdx.x + i * kUmmaThreads;
-    if (e < kHaloRows * 36)
-      halo[(e / 36) * kHaloW + e % 36] =
-          __float2half_rn(c[i] < 64u ? lg1p[c[i]] : log1pf(float(c[i])));
+  for (int j = 0; j < 5; ++j) {
+    h[j * kHaloW] = feat(c[j]);
+    if (lane < 4) h[j * kHaloW + 32] = feat(c[5 + j]);
   }
 }
 
@@ -504,21 +515,24 @@ __device__ __forceinline__ void build_a1(const __half *halo, __half *a, int m, i
     w.y = v[2] | (v[3] << 16);
     w.z = v[4] | (v[5] << 16);
     w.w = v[6] | (v[7] << 16);
-    *reinterpret_cast<uint4 *>(a + c * 1024 + m * 8) = w;
+    *reinterpret_cast<uint4 *>(a + (c % kAChunks) * 1024 + m * 8) = w;
   }
 }
 
 // Layer L (0, 1, 2) of one tile: products of A (128 x K) and the layer's
 // weights into tensor-memory columns [tcol, tcol + N), then a commit to mbar.
-// Called by one thread.
+// Layer 0 in two halves (kA1Split): layer 3 = its second K half, whose A
+// chunks sit where the first half's did. Called by one thread.
 __device__ __forceinline__ void issue_layer(int layer, const UmmaShared &sh, const __half *a,
                                             uint32_t tcol, uint32_t mbar) {
   tmem_fence_after();
-  if (layer == 0) {
+  if (layer == 0 || layer == 3) {
+    const int s_lo = layer == 3 ? 4 : 0, s_hi = kA1Split && layer == 0 ? 4 : 8;
 #pragma unroll
     for (int s2 = 0; s2 < 8; ++s2)
-      umma_f16(tcol, umma_desc(a + s2 * 2 * 1024, 2048, 128),
-               umma_desc(sh.w1 + s2 * 2 * 512, 1024, 128), umma_idesc(128, 64), s2 > 0);
+      if (s2 >= s_lo && s2 < s_hi)
+        umma_f16(tcol, umma_desc(a + (s2 % (kAChunks / 2)) * 2 * 1024, 2048, 128),
+                 umma_desc(sh.w1 + s2 * 2 * 512, 1024, 128), umma_idesc(128, 64), s2 > 0);
   } else if (layer == 1) {
 #pragma unroll
     for (int s2 = 0; s2 < 4; ++s2)
@@ -552,12 +566,14 @@ __device__ __forceinline__ void write_proposal(uint32_t taddr, const float *b3, 
     e[o] = __expf(lg[o] - mx);
     sum += e[o];
   }
+  // the first o with P(1..o) >= tau, compared unnormalised
+  const float lim = tau * sum;
   int prop = kMlpOut;
   float cum = 0.f;
 #pragma unroll
   for (int o = 0; o < 8; ++o) {
-    cum += e[o] / sum;
-    if (cum >= tau && prop == kMlpOut) prop = o + 1;
+    cum += e[o];
+    if (cum >= lim && prop == kMlpOut) prop = o + 1;
   }
   cell_prop[cell] = int8_t(prop >= kMlpOut ? 0 : prop);
 }
@@ -566,7 +582,7 @@ __device__ __forceinline__ void write_proposal(uint32_t taddr, const float *b3, 
 // memory (rows 32 w .. 32 w + 31, one 32-cell row segment): each stages half
 // of the segment's halo and features, and takes half of the accumulator
 // columns in the epilogues.
-__global__ void __launch_bounds__(kUmmaThreads, 3) k_cell_proposal_tc(
+__global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
     const float *__restrict__ params, const FrameDesc *__restrict__ frames, int nframes,
     const uint32_t *__restrict__ count, float tau, int8_t *__restrict__ cell_prop,
     int *__restrict__ status) {
@@ -577,14 +593,16 @@ __global__ void __launch_bounds__(kUmmaThreads, 3) k_cell_proposal_tc(
   const float *W1 = params, *B1 = W1 + kMlpHidden * kMlpIn;
   const float *W2 = B1 + kMlpHidden, *B2 = W2 + kMlpHidden * kMlpHidden;
   const float *W3 = B2 + kMlpHidden, *B3 = W3 + kMlpOut * kMlpHidden;
-  // weights as FP16 K-major operands
+  // weights as FP16 K-major operands; the hidden layers' weights and biases
+  // halved (exact), so that their accumulators hold z / 2 for the SiLU
   for (int t = threadIdx.x; t < 64 * 128; t += kUmmaThreads) {
     const int n = t >> 7, k = t & 127;
-    sh.w1[(k >> 3) * 512 + n * 8 + (k & 7)] = __float2half_rn(k < kMlpIn ? W1[n * kMlpIn + k] : 0.f);
+    sh.w1[(k >> 3) * 512 + n * 8 + (k & 7)] =
+        __float2half_rn(k < kMlpIn ? 0.5f * W1[n * kMlpIn + k] : 0.f);
   }
   for (int t = threadIdx.x; t < 64 * 64; t += kUmmaThreads) {
     const int n = t >> 6, k = t & 63;
-    sh.w2[(k >> 3) * 512 + n * 8 + (k & 7)] = __float2half_rn(W2[n * kMlpHidden + k]);
+    sh.w2[(k >> 3) * 512 + n * 8 + (k & 7)] = __float2half_rn(0.5f * W2[n * kMlpHidden + k]);
   }
   for (int t = threadIdx.x; t < 16 * 64; t += kUmmaThreads) {
     const int n = t >> 6, k = t & 63;
@@ -592,8 +610,8 @@ __global__ void __launch_bounds__(kUmmaThreads, 3) k_cell_proposal_tc(
         __float2half_rn(n < kMlpOut ? W3[n * kMlpHidden + k] : 0.f);
   }
   if (threadIdx.x < 64) {
-    sh.b1[threadIdx.x] = B1[threadIdx.x];
-    sh.b2[threadIdx.x] = B2[threadIdx.x];
+    sh.b1[threadIdx.x] = 0.5f * B1[threadIdx.x];
+    sh.b2[threadIdx.x] = 0.5f * B2[threadIdx.x];
     sh.lg1p[threadIdx.x] = log1pf(float(threadIdx.x));
   }
   if (threadIdx.x < 16) sh.b3[threadIdx.x] = threadIdx.x < kMlpOut ? B3[threadIdx.x] : 0.f;
@@ -626,8 +644,10 @@ __global__ void __launch_bounds__(kUmmaThreads, 3) k_cell_proposal_tc(
     __syncthreads();
     if (threadIdx.x == 0) issue_layer(layer, sh, sh.a, tmem, mbar);
   };
+  // one thread polls the barrier; the others wait at the CTA barrier
   auto wait_products = [&]() -> bool {
-    const bool w = mbar_wait(mbar, phase);
+    bool w = true;
+    if (threadIdx.x == 0) w = mbar_wait(mbar, phase);
     phase ^= 1u;
     const bool all = __syncthreads_and(w);
     tmem_fence_after();
@@ -642,11 +662,25 @@ __global__ void __launch_bounds__(kUmmaThreads, 3) k_cell_proposal_tc(
     stage_halo(g, count, sh.lg1p, sh.halo);
     __syncthreads();  // the halo is in place
     const unsigned short kfeat = __half_as_ushort(__float2half_rn(float(g.fr->k) / 64.0f));
-    if (half)
-      build_a1<8, 16>(halo, sh.a, m, lane, kfeat);
-    else
-      build_a1<0, 8>(halo, sh.a, m, lane, kfeat);
-    sync_issue(0);
+    if (kA1Split) {
+      if (half)
+        build_a1<4, 8>(halo, sh.a, m, lane, kfeat);
+      else
+        build_a1<0, 4>(halo, sh.a, m, lane, kfeat);
+      sync_issue(0);
+      if (!(ok = wait_products())) break;
+      if (half)
+        build_a1<12, 16>(halo, sh.a, m, lane, kfeat);
+      else
+        build_a1<8, 12>(halo, sh.a, m, lane, kfeat);
+      sync_issue(3);
+    } else {
+      if (half)
+        build_a1<8, 16>(halo, sh.a, m, lane, kfeat);
+      else
+        build_a1<0, 8>(halo, sh.a, m, lane, kfeat);
+      sync_issue(0);
+    }
     if (!(ok = wait_products())) break;
     hidden_to_a(tlane, sh.b1, sh.a, m, half);
     sync_issue(1);
@@ -766,7 +800,7 @@ cudaError_t mlp_training_rows(const BatchBuffers &b, const int8_t *stop_log, lon
 cudaError_t mlp_propose(const float *params, const BatchBuffers &b, int8_t *cell_prop,
                         int8_t *source_prop, float tau, cudaStream_t s) {
   if (b.nframes <= 0 || b.ncells <= 0) return cudaSuccess;
-  const size_t sm = sizeof(UmmaShared) + 1024;  // room to align the base to 1024 B
+  const size_t sm = sizeof(UmmaShared);  // operands without swizzle need 16-byte alignment only
   cudaError_t e =
       cudaFuncSetAttribute(k_cell_proposal_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
   if (e != cudaSuccess) return e;
