@@ -1044,33 +1044,35 @@ __device__ __forceinline__ float axis_gap(int d, float f) {
 }
 
 // Ascending bitonic sort of 32 H unsigned keys held H per lane: position q
-// is lane q % 32's key[q / 32]. Element q trades with q ^ j and keeps the
-// smaller key when (q < q ^ j) matches the ascending blocks of the stage
-// ((q & kk) == 0); partners 32 or more apart sit in the same lane.
+// is lane q % 32's key[q / 32]. Every comparator is ascending (the lower
+// position keeps the smaller key): the merge of blocks of kk first pairs q
+// with q ^ (kk - 1), the block reversed, then q with q ^ j for j = kk / 4
+// .. 1. Within a lane's keys the lower position is the lower h; across lanes
+// it is the lane whose bit j is clear, so each step is one shuffle and one
+// min-or-max per key.
 template <int H>
 __device__ __forceinline__ void bitonic_sort(uint32_t (&key)[H], int lane) {
 #pragma unroll
   for (int kk = 2; kk <= 32 * H; kk <<= 1) {
 #pragma unroll
     for (int j = kk >> 1; j > 0; j >>= 1) {
+      const bool flip = j == (kk >> 1);
       if (j >= 32) {
+        // partners in key h ^ dh: of the reversed lane (flip) or this lane
+        const int dh = flip ? (kk - 1) >> 5 : j >> 5;
+        uint32_t part[H];
 #pragma unroll
-        for (int h = 0; h < H; ++h) {
-          const int hp = h ^ (j >> 5);
-          if (hp > h) {
-            const bool asc = ((lane + 32 * h) & kk) == 0;
-            const uint32_t lo = min(key[h], key[hp]), hi = max(key[h], key[hp]);
-            key[h] = asc ? lo : hi;
-            key[hp] = asc ? hi : lo;
-          }
-        }
+        for (int h = 0; h < H; ++h)
+          part[h] = flip ? __shfl_xor_sync(kFull, key[h ^ dh], 31) : key[h ^ dh];
+#pragma unroll
+        for (int h = 0; h < H; ++h)
+          key[h] = h < (h ^ dh) ? min(key[h], part[h]) : max(key[h], part[h]);
       } else {
+        const bool lower = (lane & j) == 0;
 #pragma unroll
         for (int h = 0; h < H; ++h) {
-          const uint32_t pk = __shfl_xor_sync(kFull, key[h], j);
-          const bool low = (lane & j) == 0;
-          const bool up = ((lane + 32 * h) & kk) == 0;
-          key[h] = low == up ? min(key[h], pk) : max(key[h], pk);
+          const uint32_t pk = __shfl_xor_sync(kFull, key[h], flip ? kk - 1 : j);
+          key[h] = lower ? min(key[h], pk) : max(key[h], pk);
         }
       }
     }

@@ -47,8 +47,12 @@ cudaError_t mlp_adam(float *params, const float *grad, float *m, float *v, int s
 // Proposed shell per cell (tcgen05 inference over 128-cell tiles of four
 // 32-cell row segments, the first layer as a 5x5x5 convolution of the
 // occupancy grid), then per sorted source.
-cudaError_t mlp_propose(const float *params, const BatchBuffers &b, int8_t *cell_prop,
+cudaError_t mlp_propose(const void *image, const BatchBuffers &b, int8_t *cell_prop,
                         int8_t *source_prop, float tau, cudaStream_t s);
+// The inference kernel's operand image of a parameter vector (mlp_image_bytes
+// of device memory, 16-byte aligned), written once per model.
+size_t mlp_image_bytes();
+cudaError_t mlp_pack(const float *params, void *image, cudaStream_t s);
 // Training rows from a logged search: features of the cell of every
 // stride-th sorted source and its settled shell class (min(R*, 8) - 1).
 cudaError_t mlp_training_rows(const BatchBuffers &b, const int8_t *stop_log, long long stride,

@@ -284,14 +284,23 @@ constexpr bool kA1Split = true;
 constexpr int kAChunks = kA1Split ? 8 : 16;  // 16-byte K chunks the A buffer holds
 constexpr int kUmmaCtas = kA1Split ? 4 : 3;  // resident CTAs per SM
 
-struct UmmaShared {
-  __half a[128 * 8 * kAChunks];  // A1 (or its halves), then A2 and A3: chunk c at c * 2048 B, row m at m * 16 B
+// The network as the kernel holds it in shared memory, packed once per
+// model (mlp_pack) and copied whole by every CTA: FP16 K-major B operands,
+// the hidden layers' weights and biases halved (exact), so that their
+// accumulators hold z / 2 for the SiLU.
+struct UmmaWeights {
   __half w1[64 * 128];  // chunk c at c * 1024 B, row n at n * 16 B
   __half w2[64 * 64];   // chunk c at c * 1024 B
   __half w3[16 * 64];   // rows 8..15 zero; chunk c at c * 256 B
-  __half halo[kHaloRows * kHaloW];
   float b1[64], b2[64], b3[16];
   float lg1p[64];       // log(1 + c) for occupancies c < 64
+};
+static_assert(sizeof(UmmaWeights) % 16 == 0, "copied in 16-byte pieces");
+
+struct UmmaShared {
+  UmmaWeights wt;
+  __half a[128 * 8 * kAChunks];  // A1 (or its halves), then A2 and A3: chunk c at c * 2048 B, row m at m * 16 B
+  __half halo[kHaloRows * kHaloW];
   unsigned long long mbar;
   uint32_t tmem_base;
 };
@@ -532,17 +541,17 @@ __device__ __forceinline__ void issue_layer(int layer, const UmmaShared &sh, con
     for (int s2 = 0; s2 < 8; ++s2)
       if (s2 >= s_lo && s2 < s_hi)
         umma_f16(tcol, umma_desc(a + (s2 % (kAChunks / 2)) * 2 * 1024, 2048, 128),
-                 umma_desc(sh.w1 + s2 * 2 * 512, 1024, 128), umma_idesc(128, 64), s2 > 0);
+                 umma_desc(sh.wt.w1 + s2 * 2 * 512, 1024, 128), umma_idesc(128, 64), s2 > 0);
   } else if (layer == 1) {
 #pragma unroll
     for (int s2 = 0; s2 < 4; ++s2)
       umma_f16(tcol, umma_desc(a + s2 * 2 * 1024, 2048, 128),
-               umma_desc(sh.w2 + s2 * 2 * 512, 1024, 128), umma_idesc(128, 64), s2 > 0);
+               umma_desc(sh.wt.w2 + s2 * 2 * 512, 1024, 128), umma_idesc(128, 64), s2 > 0);
   } else {
 #pragma unroll
     for (int s2 = 0; s2 < 4; ++s2)
       umma_f16(tcol, umma_desc(a + s2 * 2 * 1024, 2048, 128),
-               umma_desc(sh.w3 + s2 * 2 * 128, 256, 128), umma_idesc(128, 16), s2 > 0);
+               umma_desc(sh.wt.w3 + s2 * 2 * 128, 256, 128), umma_idesc(128, 16), s2 > 0);
   }
   umma_commit(mbar);
 }
@@ -578,43 +587,51 @@ __device__ __forceinline__ void write_proposal(uint32_t taddr, const float *b3, 
   cell_prop[cell] = int8_t(prop >= kMlpOut ? 0 : prop);
 }
 
+// The network's shared-memory image (UmmaWeights) from its FP32 parameters.
+__global__ void k_pack_weights(const float *__restrict__ params, UmmaWeights *__restrict__ out) {
+  const float *W1 = params, *B1 = W1 + kMlpHidden * kMlpIn;
+  const float *W2 = B1 + kMlpHidden, *B2 = W2 + kMlpHidden * kMlpHidden;
+  const float *W3 = B2 + kMlpHidden, *B3 = W3 + kMlpOut * kMlpHidden;
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x, step = gridDim.x * blockDim.x;
+  for (int t = t0; t < 64 * 128; t += step) {
+    const int n = t >> 7, k = t & 127;
+    out->w1[(k >> 3) * 512 + n * 8 + (k & 7)] =
+        __float2half_rn(k < kMlpIn ? 0.5f * W1[n * kMlpIn + k] : 0.f);
+  }
+  for (int t = t0; t < 64 * 64; t += step) {
+    const int n = t >> 6, k = t & 63;
+    out->w2[(k >> 3) * 512 + n * 8 + (k & 7)] = __float2half_rn(0.5f * W2[n * kMlpHidden + k]);
+  }
+  for (int t = t0; t < 16 * 64; t += step) {
+    const int n = t >> 6, k = t & 63;
+    out->w3[(k >> 3) * 128 + n * 8 + (k & 7)] =
+        __float2half_rn(n < kMlpOut ? W3[n * kMlpHidden + k] : 0.f);
+  }
+  for (int t = t0; t < 64; t += step) {
+    out->b1[t] = 0.5f * B1[t];
+    out->b2[t] = 0.5f * B2[t];
+    out->lg1p[t] = log1pf(float(t));
+    if (t < 16) out->b3[t] = t < kMlpOut ? B3[t] : 0.f;
+  }
+}
+
 // Eight warps per CTA: warps w and w + 4 share lane quarter w of tensor
 // memory (rows 32 w .. 32 w + 31, one 32-cell row segment): each stages half
 // of the segment's halo and features, and takes half of the accumulator
 // columns in the epilogues.
 __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
-    const float *__restrict__ params, const FrameDesc *__restrict__ frames, int nframes,
+    const UmmaWeights *__restrict__ image, const FrameDesc *__restrict__ frames, int nframes,
     const uint32_t *__restrict__ count, float tau, int8_t *__restrict__ cell_prop,
     int *__restrict__ status) {
   extern __shared__ __align__(1024) unsigned char umma_smem[];
   UmmaShared &sh = *reinterpret_cast<UmmaShared *>(umma_smem);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int quarter = warp & 3, half = warp >> 2;
-  const float *W1 = params, *B1 = W1 + kMlpHidden * kMlpIn;
-  const float *W2 = B1 + kMlpHidden, *B2 = W2 + kMlpHidden * kMlpHidden;
-  const float *W3 = B2 + kMlpHidden, *B3 = W3 + kMlpOut * kMlpHidden;
-  // weights as FP16 K-major operands; the hidden layers' weights and biases
-  // halved (exact), so that their accumulators hold z / 2 for the SiLU
-  for (int t = threadIdx.x; t < 64 * 128; t += kUmmaThreads) {
-    const int n = t >> 7, k = t & 127;
-    sh.w1[(k >> 3) * 512 + n * 8 + (k & 7)] =
-        __float2half_rn(k < kMlpIn ? 0.5f * W1[n * kMlpIn + k] : 0.f);
+  {
+    const uint4 *src = reinterpret_cast<const uint4 *>(image);
+    uint4 *dst = reinterpret_cast<uint4 *>(&sh.wt);
+    for (int i = threadIdx.x; i < int(sizeof(UmmaWeights) / 16); i += kUmmaThreads) dst[i] = src[i];
   }
-  for (int t = threadIdx.x; t < 64 * 64; t += kUmmaThreads) {
-    const int n = t >> 6, k = t & 63;
-    sh.w2[(k >> 3) * 512 + n * 8 + (k & 7)] = __float2half_rn(0.5f * W2[n * kMlpHidden + k]);
-  }
-  for (int t = threadIdx.x; t < 16 * 64; t += kUmmaThreads) {
-    const int n = t >> 6, k = t & 63;
-    sh.w3[(k >> 3) * 128 + n * 8 + (k & 7)] =
-        __float2half_rn(n < kMlpOut ? W3[n * kMlpHidden + k] : 0.f);
-  }
-  if (threadIdx.x < 64) {
-    sh.b1[threadIdx.x] = 0.5f * B1[threadIdx.x];
-    sh.b2[threadIdx.x] = 0.5f * B2[threadIdx.x];
-    sh.lg1p[threadIdx.x] = log1pf(float(threadIdx.x));
-  }
-  if (threadIdx.x < 16) sh.b3[threadIdx.x] = threadIdx.x < kMlpOut ? B3[threadIdx.x] : 0.f;
   const uint32_t mbar = smem_u32(&sh.mbar);
   if (threadIdx.x == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1u) : "memory");
@@ -659,7 +676,7 @@ __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
       last.tile_base + (long long)((last.nx + 31) / 32) * ((last.ny + 3) / 4) * last.nz;
   for (long long ct = blockIdx.x; ct < tiles; ct += gridDim.x) {
     const TileInfo g = tile_info(frames, nframes, ct, tiles);
-    stage_halo(g, count, sh.lg1p, sh.halo);
+    stage_halo(g, count, sh.wt.lg1p, sh.halo);
     __syncthreads();  // the halo is in place
     const unsigned short kfeat = __half_as_ushort(__float2half_rn(float(g.fr->k) / 64.0f));
     if (kA1Split) {
@@ -682,10 +699,10 @@ __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
       sync_issue(0);
     }
     if (!(ok = wait_products())) break;
-    hidden_to_a(tlane, sh.b1, sh.a, m, half);
+    hidden_to_a(tlane, sh.wt.b1, sh.a, m, half);
     sync_issue(1);
     if (!(ok = wait_products())) break;
-    hidden_to_a(tlane, sh.b2, sh.a, m, half);
+    hidden_to_a(tlane, sh.wt.b2, sh.a, m, half);
     sync_issue(2);
     if (!(ok = wait_products())) break;
     if (half == 0) {
@@ -694,7 +711,7 @@ __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
       const bool valid = lane < g.ncl && y < tf.ny;
       const long long cell =
           tf.cell_base + ((long long)g.z0 * tf.ny + (valid ? y : 0)) * tf.nx + g.x0 + lane;
-      write_proposal(tlane, sh.b3, tau, cell_prop, cell, valid);
+      write_proposal(tlane, sh.wt.b3, tau, cell_prop, cell, valid);
     }
     // the next tile rewrites the halos, A and the accumulators
     tmem_fence_before();
@@ -797,7 +814,14 @@ cudaError_t mlp_training_rows(const BatchBuffers &b, const int8_t *stop_log, lon
   return cudaGetLastError();
 }
 
-cudaError_t mlp_propose(const float *params, const BatchBuffers &b, int8_t *cell_prop,
+size_t mlp_image_bytes() { return sizeof(UmmaWeights); }
+
+cudaError_t mlp_pack(const float *params, void *image, cudaStream_t s) {
+  k_pack_weights<<<32, 256, 0, s>>>(params, static_cast<UmmaWeights *>(image));
+  return cudaGetLastError();
+}
+
+cudaError_t mlp_propose(const void *image, const BatchBuffers &b, int8_t *cell_prop,
                         int8_t *source_prop, float tau, cudaStream_t s) {
   if (b.nframes <= 0 || b.ncells <= 0) return cudaSuccess;
   const size_t sm = sizeof(UmmaShared);  // operands without swizzle need 16-byte alignment only
@@ -811,8 +835,9 @@ cudaError_t mlp_propose(const float *params, const BatchBuffers &b, int8_t *cell
   // resident CTAs: shared memory (1 KB of it reserved per CTA) and the
   // kTmemCols each CTA holds of the SM's 512 tensor-memory columns
   const int per_sm = std::max(1, std::min(smem_sm / int(sm + 1024), int(512 / kTmemCols)));
-  k_cell_proposal_tc<<<sms * per_sm, kUmmaThreads, sm, s>>>(params, b.frames, b.nframes, b.count,
-                                                            tau, cell_prop, b.status);
+  k_cell_proposal_tc<<<sms * per_sm, kUmmaThreads, sm, s>>>(
+      static_cast<const UmmaWeights *>(image), b.frames, b.nframes, b.count, tau, cell_prop,
+      b.status);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_source_proposal<<<grid_of(b.npts, 256), 256, 0, s>>>(b.frames, b.nframes, b.off, b.ncells,
                                                          b.scell, cell_prop, source_prop);

@@ -163,7 +163,7 @@ void WorkspaceImpl::release_all() {
   rel(h_mask_); rel(h_nn_); rel(active_); rel(proposal_); rel(cell_prop_); rel(stop_log_);
   rel(order_); rel(csr_counts_); rel(csr_off_); rel(live_); rel(part_cnt_); rel(part_off_);
   rel(part_tiles_); rel(shard_cut_);
-  rel(model_); rel(shell_table_);
+  rel(model_); rel(model_image_); rel(shell_table_);
   shell_table_ready_ = false;
 }
 
@@ -551,7 +551,7 @@ Code WorkspaceImpl::enqueue(BatchBuffers &b, const WalkLaunch &wl, int nf, size_
     if (opts.fixed_proposal > 0) {
       LC_TRY(cudaMemsetAsync(proposal_.p, std::min(opts.fixed_proposal, 127), P, s));
     } else if (has_model_) {
-      LC_TRY(mlp_propose(model_.p, b, cell_prop_.p, proposal_.p, tau_, s));
+      LC_TRY(mlp_propose(model_image_.p, b, cell_prop_.p, proposal_.p, tau_, s));
     } else {
       LC_TRY(cudaMemsetAsync(proposal_.p, 0, P, s));
     }
@@ -604,7 +604,9 @@ Code WorkspaceImpl::set_model(const float *params, size_t n, float tau, std::str
     return Code::DeviceStatus;
   }
   LC_TRY(grow(model_, n));
+  LC_TRY(grow(model_image_, (mlp_image_bytes() + 15) / 16));
   LC_TRY(cudaMemcpyAsync(model_.p, params, n * sizeof(float), cudaMemcpyHostToDevice, stream()));
+  LC_TRY(mlp_pack(model_.p, model_image_.p, stream()));
   LC_TRY(cudaStreamSynchronize(stream()));
   has_model_ = true;
   tau_ = tau;

@@ -266,6 +266,7 @@ class WorkspaceImpl {
   Buf<long long> counters_;
   Buf<int8_t> proposal_, cell_prop_, stop_log_;
   Buf<float> model_;
+  Buf<uint4> model_image_;  // the inference kernel's operand image of model_
   Buf<uint32_t> shell_table_;
   bool shell_table_ready_ = false;
   bool has_model_ = false;
