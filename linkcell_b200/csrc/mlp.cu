@@ -275,14 +275,20 @@ __global__ void k_training_rows(BatchBuffers b, const int8_t *__restrict__ stop_
 constexpr int kUmmaThreads = 256;   // two warps per lane quarter of tensor memory
 constexpr int kHaloW = 40;          // halves per halo row (36 used: x0 - 2 .. x0 + 33)
 constexpr int kHaloRows = 40;       // halo rows of a tile: 8 y x 5 z
-constexpr uint32_t kTmemCols = 64;  // D1, D2 and D3 share the same columns
 constexpr int kMbarSpin = 1 << 22;  // bounded wait for the tensor cores
+// A CTA runs kGroups groups of four warps (one per lane quarter of tensor
+// memory), each on its own tile with its own operand buffer, halo, 64
+// accumulator columns (D1, D2 and D3 share them), barrier and mbarrier, so
+// that one group's waits for the tensor cores overlap the other's work.
+constexpr int kGroups = 2;
+constexpr int kGroupThreads = kUmmaThreads / kGroups;
+constexpr int kGroupWarps = kGroupThreads / 32;
+constexpr uint32_t kTmemCols = 64 * kGroups;
 // Layer 1's A operand (128 x 128) built and multiplied in two K halves in
-// one 16 KB buffer: shared memory for four CTAs per SM, for one more round
-// trip to the tensor cores per tile.
+// one 16 KB buffer per group: shared memory for more tiles in flight, for
+// one more round trip to the tensor cores per tile.
 constexpr bool kA1Split = true;
 constexpr int kAChunks = kA1Split ? 8 : 16;  // 16-byte K chunks the A buffer holds
-constexpr int kUmmaCtas = kA1Split ? 4 : 3;  // resident CTAs per SM
 
 // The network as the kernel holds it in shared memory, packed once per
 // model (mlp_pack) and copied whole by every CTA: FP16 K-major B operands,
@@ -297,13 +303,23 @@ struct UmmaWeights {
 };
 static_assert(sizeof(UmmaWeights) % 16 == 0, "copied in 16-byte pieces");
 
-struct UmmaShared {
-  UmmaWeights wt;
+struct __align__(16) UmmaGroup {
   __half a[128 * 8 * kAChunks];  // A1 (or its halves), then A2 and A3: chunk c at c * 2048 B, row m at m * 16 B
   __half halo[kHaloRows * kHaloW];
   unsigned long long mbar;
+};
+
+struct UmmaShared {
+  UmmaWeights wt;
+  UmmaGroup grp[kGroups];
   uint32_t tmem_base;
 };
+
+// Resident CTAs per SM: shared memory (1 KB of it reserved per CTA) and
+// tensor-memory columns.
+constexpr int kUmmaCtas = (228 * 1024) / (int(sizeof(UmmaShared)) + 1024) < int(512 / kTmemCols)
+                              ? (228 * 1024) / (int(sizeof(UmmaShared)) + 1024)
+                              : int(512 / kTmemCols);
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -382,10 +398,33 @@ __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// Periodic coordinate c for |c - [0, n)| <= 2.
-__device__ __forceinline__ int wrap_near(int c, int n) {
-  if (n < 3) return rem_euclid(c, n);
-  return c < 0 ? c + n : (c >= n ? c - n : c);
+// Barrier of warp group g (named barrier g + 1; 0 is __syncthreads), and
+// the same with an AND of every thread's predicate.
+// (Immediate barrier numbers: the kernel reserves three of the CTA's 16.)
+template <int ID>
+__device__ __forceinline__ void bar_sync_n() {
+  asm volatile("bar.sync %0, %1;" ::"n"(ID), "n"(kGroupThreads) : "memory");
+}
+template <int ID>
+__device__ __forceinline__ bool bar_and_n(bool p) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred a, b;\n\tsetp.ne.u32 a, %1, 0;\n\t"
+      "bar.red.and.pred b, %2, %3, a;\n\tselp.u32 %0, 1, 0, b;\n\t}\n"
+      : "=r"(r)
+      : "r"(uint32_t(p)), "n"(ID), "n"(kGroupThreads)
+      : "memory");
+  return r != 0u;
+}
+__device__ __forceinline__ void group_sync(int g) {
+  static_assert(kGroups <= 2, "one named barrier per group");
+  if (g == 0)
+    bar_sync_n<1>();
+  else
+    bar_sync_n<2>();
+}
+__device__ __forceinline__ bool group_sync_and(int g, bool p) {
+  return g == 0 ? bar_and_n<1>(p) : bar_and_n<2>(p);
 }
 
 // SiLU of two values from their halves u = z / 2 (the hidden layers' weights
@@ -399,12 +438,11 @@ __device__ __forceinline__ uint32_t silu_h2(float ulo, float uhi) {
   return *reinterpret_cast<const uint32_t *>(&y);
 }
 
-// Hidden layer epilogue: 32 of row m's 64 accumulators (columns
-// [32 h, 32 h + 32)) + bias, SiLU, as FP16 into the next A operand.
-__device__ __forceinline__ void hidden_to_a(uint32_t taddr, const float *bias, __half *a, int m,
-                                            int half) {
+// Hidden layer epilogue: row m's 64 accumulators + bias, SiLU, as FP16 into
+// the next A operand.
+__device__ __forceinline__ void hidden_to_a(uint32_t taddr, const float *bias, __half *a, int m) {
 #pragma unroll
-  for (int q = 2 * half; q < 2 * half + 2; ++q) {
+  for (int q = 0; q < 4; ++q) {
     float v[16];
     tmem_ld16(taddr + 16 * q, v);
     tmem_wait_ld();
@@ -473,34 +511,39 @@ __device__ __forceinline__ int wrap_cell(int c, int n) {
 
 // The tile's halo of log(1 + count): 36 columns x0 - 2 .. x0 + 33 of the
 // 8 x 5 rows (y0 - 2 .. y0 + 5, z0 - 2 .. z0 + 2), row (yi, zi) at halo row
-// yi * 5 + zi. Warp w stages the five rows of yi = w: lane l column l, and
-// lanes 0-3 columns 32-35, all ten loads in flight before the first store.
+// yi * 5 + zi. Warp w of the group stages the rows of yi = 2 w and 2 w + 1,
+// five at a time: lane l column l, and lanes 0-3 columns 32-35, the ten
+// loads in flight before the first store.
 __device__ __forceinline__ void stage_halo(const TileInfo &g, const uint32_t *__restrict__ count,
-                                           const float *lg1p, __half *halo) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t c[10];
+                                           const float *lg1p, __half *halo, int w) {
+  const int lane = threadIdx.x & 31;
+  auto feat = [&](uint32_t v) { return __float2half_rn(v < 64u ? lg1p[v] : log1pf(float(v))); };
 #pragma unroll
-  for (int i = 0; i < 10; ++i) c[i] = 0u;
-  if (g.ncl > 0) {
-    const FrameDesc &fr = *g.fr;
-    const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
-    const int jy = wrap_cell(g.y0 + warp - 2, ny);
-    const int jx0 = wrap_cell(g.x0 + lane - 2, nx);
-    const int jx1 = wrap_cell(g.x0 + lane + 30, nx);
+  for (int t = 0; t < 8 / kGroupWarps; ++t) {
+    const int yi = (8 / kGroupWarps) * w + t;
+    uint32_t c[10];
+#pragma unroll
+    for (int i = 0; i < 10; ++i) c[i] = 0u;
+    if (g.ncl > 0) {
+      const FrameDesc &fr = *g.fr;
+      const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
+      const int jy = wrap_cell(g.y0 + yi - 2, ny);
+      const int jx0 = wrap_cell(g.x0 + lane - 2, nx);
+      const int jx1 = wrap_cell(g.x0 + lane + 30, nx);
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        const int jz = wrap_cell(g.z0 + j - 2, nz);
+        const uint32_t *row = count + fr.cell_base + ((long long)jz * ny + jy) * (long long)nx;
+        c[j] = row[jx0];
+        if (lane < 4) c[5 + j] = row[jx1];
+      }
+    }
+    __half *h = halo + yi * 5 * kHaloW + lane;
 #pragma unroll
     for (int j = 0; j < 5; ++j) {
-      const int jz = wrap_cell(g.z0 + j - 2, nz);
-      const uint32_t *row = count + fr.cell_base + ((long long)jz * ny + jy) * (long long)nx;
-      c[j] = row[jx0];
-      if (lane < 4) c[5 + j] = row[jx1];
+      h[j * kHaloW] = feat(c[j]);
+      if (lane < 4) h[j * kHaloW + 32] = feat(c[5 + j]);
     }
-  }
-  auto feat = [&](uint32_t v) { return __float2half_rn(v < 64u ? lg1p[v] : log1pf(float(v))); };
-  __half *h = halo + warp * 5 * kHaloW + lane;
-#pragma unroll
-  for (int j = 0; j < 5; ++j) {
-    h[j * kHaloW] = feat(c[j]);
-    if (lane < 4) h[j * kHaloW + 32] = feat(c[5 + j]);
   }
 }
 
@@ -615,10 +658,11 @@ __global__ void k_pack_weights(const float *__restrict__ params, UmmaWeights *__
   }
 }
 
-// Eight warps per CTA: warps w and w + 4 share lane quarter w of tensor
-// memory (rows 32 w .. 32 w + 31, one 32-cell row segment): each stages half
-// of the segment's halo and features, and takes half of the accumulator
-// columns in the epilogues.
+// kGroups groups of four warps per CTA. Warp q of a group owns lane
+// quarter q of tensor memory (rows 32 q .. 32 q + 31: one 32-cell row
+// segment of the tile): it stages two y rows of the group's halo, builds the
+// features of its rows, and runs the epilogues of all 64 accumulator
+// columns of its rows. The group's first thread issues its products.
 __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
     const UmmaWeights *__restrict__ image, const FrameDesc *__restrict__ frames, int nframes,
     const uint32_t *__restrict__ count, float tau, int8_t *__restrict__ cell_prop,
@@ -626,14 +670,15 @@ __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
   extern __shared__ __align__(1024) unsigned char umma_smem[];
   UmmaShared &sh = *reinterpret_cast<UmmaShared *>(umma_smem);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int quarter = warp & 3, half = warp >> 2;
+  const int gi = warp / kGroupWarps, quarter = warp % kGroupWarps;
+  UmmaGroup &G = sh.grp[gi];
   {
     const uint4 *src = reinterpret_cast<const uint4 *>(image);
     uint4 *dst = reinterpret_cast<uint4 *>(&sh.wt);
     for (int i = threadIdx.x; i < int(sizeof(UmmaWeights) / 16); i += kUmmaThreads) dst[i] = src[i];
   }
-  const uint32_t mbar = smem_u32(&sh.mbar);
-  if (threadIdx.x == 0) {
+  const uint32_t mbar = smem_u32(&G.mbar);
+  if (threadIdx.x % kGroupThreads == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1u) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -648,25 +693,26 @@ __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
   tmem_fence_before();
   __syncthreads();
   tmem_fence_after();
-  const uint32_t tmem = sh.tmem_base;
+  const uint32_t tmem = sh.tmem_base + uint32_t(64 * gi);        // the group's columns
   const uint32_t tlane = tmem + (uint32_t(quarter * 32) << 16);  // this warp's lane quarter
   const int m = quarter * 32 + lane;                              // A row = accumulator lane
   // this quarter's row y0 + quarter reads halo rows (quarter + dy + 2) 5 + dz + 2
-  const __half *halo = sh.halo + quarter * 5 * kHaloW;
+  const __half *halo = G.halo + quarter * 5 * kHaloW;
+  const bool issuer = threadIdx.x % kGroupThreads == 0;
   uint32_t phase = 0;
   bool ok = true;
   auto sync_issue = [&](int layer) {
     async_proxy_fence();
     tmem_fence_before();
-    __syncthreads();
-    if (threadIdx.x == 0) issue_layer(layer, sh, sh.a, tmem, mbar);
+    group_sync(gi);
+    if (issuer) issue_layer(layer, sh, G.a, tmem, mbar);
   };
-  // one thread polls the barrier; the others wait at the CTA barrier
+  // one thread polls the mbarrier; the others wait at the group barrier
   auto wait_products = [&]() -> bool {
     bool w = true;
-    if (threadIdx.x == 0) w = mbar_wait(mbar, phase);
+    if (issuer) w = mbar_wait(mbar, phase);
     phase ^= 1u;
-    const bool all = __syncthreads_and(w);
+    const bool all = group_sync_and(gi, w);
     tmem_fence_after();
     return all;
   };
@@ -674,38 +720,30 @@ __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
   const FrameDesc &last = frames[nframes - 1];
   const long long tiles =
       last.tile_base + (long long)((last.nx + 31) / 32) * ((last.ny + 3) / 4) * last.nz;
-  for (long long ct = blockIdx.x; ct < tiles; ct += gridDim.x) {
+  for (long long ct = (long long)blockIdx.x * kGroups + gi; ct < tiles;
+       ct += (long long)gridDim.x * kGroups) {
     const TileInfo g = tile_info(frames, nframes, ct, tiles);
-    stage_halo(g, count, sh.wt.lg1p, sh.halo);
-    __syncthreads();  // the halo is in place
+    stage_halo(g, count, sh.wt.lg1p, G.halo, quarter);
+    group_sync(gi);  // the halo is in place
     const unsigned short kfeat = __half_as_ushort(__float2half_rn(float(g.fr->k) / 64.0f));
     if (kA1Split) {
-      if (half)
-        build_a1<4, 8>(halo, sh.a, m, lane, kfeat);
-      else
-        build_a1<0, 4>(halo, sh.a, m, lane, kfeat);
+      build_a1<0, 8>(halo, G.a, m, lane, kfeat);
       sync_issue(0);
       if (!(ok = wait_products())) break;
-      if (half)
-        build_a1<12, 16>(halo, sh.a, m, lane, kfeat);
-      else
-        build_a1<8, 12>(halo, sh.a, m, lane, kfeat);
+      build_a1<8, 16>(halo, G.a, m, lane, kfeat);
       sync_issue(3);
     } else {
-      if (half)
-        build_a1<8, 16>(halo, sh.a, m, lane, kfeat);
-      else
-        build_a1<0, 8>(halo, sh.a, m, lane, kfeat);
+      build_a1<0, 16>(halo, G.a, m, lane, kfeat);
       sync_issue(0);
     }
     if (!(ok = wait_products())) break;
-    hidden_to_a(tlane, sh.wt.b1, sh.a, m, half);
+    hidden_to_a(tlane, sh.wt.b1, G.a, m);
     sync_issue(1);
     if (!(ok = wait_products())) break;
-    hidden_to_a(tlane, sh.wt.b2, sh.a, m, half);
+    hidden_to_a(tlane, sh.wt.b2, G.a, m);
     sync_issue(2);
     if (!(ok = wait_products())) break;
-    if (half == 0) {
+    {
       const int y = g.y0 + quarter;
       const FrameDesc &tf = *g.fr;
       const bool valid = lane < g.ncl && y < tf.ny;
@@ -713,18 +751,18 @@ __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
           tf.cell_base + ((long long)g.z0 * tf.ny + (valid ? y : 0)) * tf.nx + g.x0 + lane;
       write_proposal(tlane, sh.wt.b3, tau, cell_prop, cell, valid);
     }
-    // the next tile rewrites the halos, A and the accumulators
+    // the group's next tile rewrites its halo, A and accumulators
     tmem_fence_before();
-    __syncthreads();
+    group_sync(gi);
     tmem_fence_after();
   }
-  if (!ok && threadIdx.x == 0) {
+  if (!ok && issuer) {
     atomicOr(status, kStatusMmaTimeout);
     mbar_wait(mbar, phase ^ 1u);  // give the products in flight a last bounded wait
   }
   __syncthreads();
   if (warp == 0) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sh.tmem_base),
                  "r"(kTmemCols)
                  : "memory");
   }
