@@ -63,6 +63,9 @@ def parse():
                         "autotuner pick")
     p.add_argument("--plain-tpp", type=int, default=0,
                    help="the same for the plain FP64 walk timed beside it")
+    p.add_argument("--walk-shape", default="",
+                   help="W,G: force the select walk's warps per block and work grab "
+                        "(the autotuner's choice otherwise); for profiling one shape")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-sweep", action="store_true",
                    help="skip the network-vs-constant-proposal sweep")
@@ -508,6 +511,9 @@ def run_ours(args):
         one untimed search that counts the walk statistics."""
         assert L.lc_gpu_set_mode(ws, mode) == 0
         assert L.lc_gpu_set_tpp(ws, tpp) == 0  # 0: the autotuner's choice
+        if args.walk_shape:
+            wwarps, wgrab = (int(v) for v in args.walk_shape.split(","))
+            assert L.lc_gpu_set_walk_shape(ws, wwarps, wgrab) == 0
         assert L.lc_gpu_set_proposal(ws, shell) == 0
         for _ in range(warmup):
             step()

@@ -253,26 +253,26 @@ __global__ void k_training_rows(BatchBuffers b, const int8_t *__restrict__ stop_
 }
 
 // ---------------------------------------------------------------------
-// Tensor-core inference on the 5th-generation tensor cores (tcgen05). A CTA
-// of eight warps evaluates 128 cells at a time -- four 32-cell row segments,
-// two warps per segment and lane quarter of tensor memory -- as the M = 128
-// rows of the three layers:
+// Tensor-core inference on the 5th-generation tensor cores (tcgen05). A
+// group of four warps evaluates 128 cells at a time -- four 32-cell row
+// segments, one warp per segment and lane quarter of tensor memory -- as
+// the M = 128 rows of the three layers:
 //   D1 = A1 W1^T  (A1: [128 x 128] occupancy features, 126 used),
 //   D2 = SiLU(D1 + b1) W2^T,  D3 = SiLU(D2 + b2) W3^T  (N = 64, 64, 16 with 8 used).
-// One thread issues tcgen05.mma (kind::f16: FP16 operands that the tensor
-// cores read from shared memory through matrix descriptors, FP32
-// accumulators in tensor memory) and tcgen05.commit, which arrives on an
-// mbarrier once the products are done; every warp then reads its 32
+// The group's first thread issues tcgen05.mma (kind::f16: FP16 operands that
+// the tensor cores read from shared memory through matrix descriptors, FP32
+// accumulators in tensor memory) and tcgen05.commit, which arrives on the
+// group's mbarrier once the products are done; every warp then reads its 32
 // accumulator lanes with tcgen05.ld, adds the bias, applies SiLU and writes
 // the next layer's A operand. Layer 1 is a 5x5x5 convolution of the
-// occupancy grid: the two warps of a segment stage its 36 x 5 x 5 halo of
-// log(1 + count) (13 and 12 of the 25 rows) and each of their lanes writes
-// half of its cell's 128 features (16-byte chunks 0-7 or 8-15) from it.
+// occupancy grid: the group stages the tile's 36 x 8 x 5 halo of
+// log(1 + count), and each lane writes its cell's 128 features (16-byte
+// chunks) from it, in two K halves.
 //
 // Operand layout (K-major, no swizzle): 8-row x 16-byte core matrices; the 8
 // rows of a core matrix are 16 B apart, 8-row groups SBO = 128 B apart, and
 // the 16-byte K chunks LBO apart (LBO = rows x 16 B).
-constexpr int kUmmaThreads = 256;   // two warps per lane quarter of tensor memory
+constexpr int kUmmaThreads = 256;   // two groups of four warps
 constexpr int kHaloW = 40;          // halves per halo row (36 used: x0 - 2 .. x0 + 33)
 constexpr int kHaloRows = 40;       // halo rows of a tile: 8 y x 5 z
 constexpr int kMbarSpin = 1 << 22;  // bounded wait for the tensor cores
