@@ -464,6 +464,22 @@ def walk_roofline(ref_pairs, walk_ms, f_sm_mhz, sms):
             "f_sm_mhz": f_sm_mhz, "sms": sms}
 
 
+def step_roofline(sources_per_s, prep_bytes_per_point, k, ref_pairs_per_source, peak_gbs, f_sm_mhz,
+                  sms):
+    """The whole search in sources/s against the slower of two bounds: HBM
+    for the prep's minimum plus the output row ((57.2 + 12 k) B per source on
+    this workload) and the FP32 issue bound for the reference's mean pairs per
+    source (SMs x 128 lanes x f_SM / 8 pair-evaluations/s)."""
+    hbm = peak_gbs * 1e9 / (prep_bytes_per_point + 12.0 * k)
+    walk = sms * 128 * f_sm_mhz * 1e6 / 8.0 / ref_pairs_per_source
+    peak = min(hbm, walk)
+    return {"bound": "hbm" if hbm <= walk else "fp32_issue", "unit": "sources/s",
+            "achieved": sources_per_s, "peak": peak, "frac": sources_per_s / peak,
+            "hbm_bound": hbm, "walk_bound": walk,
+            "bytes_per_source": prep_bytes_per_point + 12.0 * k,
+            "ref_pairs_per_source": ref_pairs_per_source}
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_env()
@@ -597,6 +613,8 @@ def run_ours(args):
                 # counter equals the oracle's heap pushes: 348.65 per source here)
                 "walk": walk_roofline(float(plain["counters"]["pairs"]), walk_avg_ms, f_sm, sms),
                 "prep": prep_roofline(w["cell"], n, head["prep_ms"], peak)}
+    roofline["step"] = step_roofline(value, roofline["prep"]["bytes_per_point"], k,
+                                     float(plain["counters"]["pairs"]) / n, peak, f_sm, sms)
 
     # the network against one constant shell for every source, same select walk
     lvc = None
