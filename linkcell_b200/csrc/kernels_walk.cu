@@ -1560,10 +1560,11 @@ __device__ bool sel_finish(const BatchBuffers &b, long long p, int lane, SelShar
 
 // One source; false: the source must go to the literal replay. STATS: count
 // the walk statistics (lc_gpu_set_stats; they cost about 3 % of the walk).
-template <int SN, bool STATS>
-__device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelShared<SN> &sh) {
-  const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
-  const FrameDesc &fr = b.frames[f];
+template <int SN, bool STATS, bool ONE>
+__device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelShared<SN> &sh,
+                              const FrameDesc &fr1) {
+  const int f = ONE || b.nframes == 1 ? 0 : frame_of_sorted(b, p);
+  const FrameDesc &fr = ONE ? fr1 : b.frames[f];
   const int Rp = b.proposal[p];
   const int k = fr.k;
   const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
@@ -1779,9 +1780,11 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
 
 // grab: consecutive sources a warp takes from the work queue at a time
 // (they share most candidates, which then stay in L1).
-template <int SN, bool STATS, int WARPS>
+// ONE: a single frame, passed as fr1 (read from the constant bank) instead
+// of b.frames[0].
+template <int SN, bool STATS, int WARPS, bool ONE>
 __global__ void __launch_bounds__(WARPS * 32, sel_warps_per_sm<SN>() / WARPS)
-    k_select_walk(BatchBuffers b, int grab) {
+    k_select_walk(BatchBuffers b, int grab, const __grid_constant__ FrameDesc fr1) {
   extern __shared__ __align__(16) unsigned char sel_smem[];
   SelShared<SN> &sh = reinterpret_cast<SelShared<SN> *>(sel_smem)[threadIdx.x >> 5];
   const long long total = walk_sources(b);
@@ -1798,7 +1801,7 @@ __global__ void __launch_bounds__(WARPS * 32, sel_warps_per_sm<SN>() / WARPS)
       const long long p = walk_source_at(b, src);
       if (p < 0) continue;
       const unsigned long long tie = STATS ? sh.wc[kWcReplays] : 0ull;
-      if (!select_source<SN, STATS>(b, p, lane, sh)) {
+      if (!select_source<SN, STATS, ONE>(b, p, lane, sh, fr1)) {
         if (STATS && lane == 0 && sh.wc[kWcReplays] == tie) ++sh.wc[kWcFallback];
         if (lane == 0) push_replay(b, p);
       }
@@ -1823,26 +1826,30 @@ __global__ void __launch_bounds__(WARPS * 32, sel_warps_per_sm<SN>() / WARPS)
 
 int sm_count();
 
-template <int SN, bool STATS, int WARPS>
+template <int SN, bool STATS, int WARPS, bool ONE>
 cudaError_t launch_select_as(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
   const size_t smem = sizeof(SelShared<SN>) * WARPS;
-  cudaError_t e = cudaFuncSetAttribute(k_select_walk<SN, STATS, WARPS>,
+  cudaError_t e = cudaFuncSetAttribute(k_select_walk<SN, STATS, WARPS, ONE>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk<SN, STATS, WARPS>,
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_walk<SN, STATS, WARPS, ONE>,
                                                 WARPS * 32, smem);
   if (per_sm < 1) per_sm = 1;
   const int grid = w.grid > 0 ? w.grid : sm_count() * per_sm;
   const int grab = w.grab == 8 || w.grab == 32 ? w.grab : 16;
-  k_select_walk<SN, STATS, WARPS><<<grid, WARPS * 32, smem, s>>>(b, grab);
+  k_select_walk<SN, STATS, WARPS, ONE><<<grid, WARPS * 32, smem, s>>>(b, grab, w.frame1);
   return cudaGetLastError();
 }
 
 template <int SN, int WARPS>
 cudaError_t launch_select_w(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s) {
-  return w.stats ? launch_select_as<SN, true, WARPS>(b, w, s)
-                 : launch_select_as<SN, false, WARPS>(b, w, s);
+  const bool one = w.one && b.nframes == 1;
+  if (w.stats)
+    return one ? launch_select_as<SN, true, WARPS, true>(b, w, s)
+               : launch_select_as<SN, true, WARPS, false>(b, w, s);
+  return one ? launch_select_as<SN, false, WARPS, true>(b, w, s)
+             : launch_select_as<SN, false, WARPS, false>(b, w, s);
 }
 
 // The select walk in the block shape w.warps asks for (one of the two its S

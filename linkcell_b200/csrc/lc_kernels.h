@@ -128,6 +128,11 @@ struct WalkLaunch {
   // 0 = the default) and sources per work grab (8, 16 or 32; 0 = 16)
   int warps = 0;
   int grab = 0;
+  // A single frame whose description the host holds (not device-planned, no
+  // CUDA graph, which would replay the launch with this copy): the select
+  // walk takes it as a kernel parameter and reads it from the constant bank.
+  bool one = false;
+  FrameDesc frame1{};
 };
 
 // Walk shapes the autotuner times for the select walk of k <= kmax.

@@ -318,6 +318,10 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   wl.kmax = kmax;
   wl.prune = opts.prune;
   wl.stats = opts.stats;
+  // a single host-planned frame goes to the select walk as a kernel
+  // parameter (not under a graph: its replays would keep the captured copy)
+  wl.one = nf == 1 && !dcell_.on && !opts.graph;
+  if (wl.one) wl.frame1 = frames[0];
   const int kclass = kmax <= 32 ? 0 : (kmax <= 64 ? 1 : (kmax <= 128 ? 2 : 3));
   const int tkey = (wl.mode * 4 + kclass) * 2 + (nf > 1 ? 1 : 0);
   const bool select = wl.mode == kModeLearned && kmax <= 64 && learned;  // the cube select walk
