@@ -30,12 +30,15 @@ __device__ __forceinline__ int frame_of_point(const FrameDesc *__restrict__ fr, 
 }
 
 // fold + bin + histogram: grid-stride over points, two per thread per trip
-// (their coordinate loads and histogram atomics in flight together).
+// (their coordinate loads and histogram atomics in flight together). ONE: a
+// single frame, passed as fr1 (read from the constant bank).
+template <bool ONE>
 __global__ void __launch_bounds__(256)
     k_fold_bin(const double *__restrict__ xyz, const int *__restrict__ mask,
                const FrameDesc *__restrict__ frames, int nframes, long long npts,
                uint32_t *__restrict__ cell_of, uint32_t *__restrict__ arank,
-               uint32_t *__restrict__ count, int *__restrict__ frame_flags) {
+               uint32_t *__restrict__ count, int *__restrict__ frame_flags,
+               const __grid_constant__ FrameDesc fr1) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long g0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; g0 < npts;
        g0 += 2 * stride) {
@@ -49,8 +52,8 @@ __global__ void __launch_bounds__(256)
       act[u] = g < npts;
       fi[u] = 0;
       if (!act[u]) continue;
-      fi[u] = nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
-      const FrameDesc &fr = frames[fi[u]];
+      fi[u] = ONE || nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
+      const FrameDesc &fr = ONE ? fr1 : frames[fi[u]];
       if (fr.dead || (fr.has_mask && mask[fr.mask_base + (g - fr.pt_base)] == 0)) {
         cell_of[g] = kInactive;
         act[u] = false;
@@ -65,7 +68,7 @@ __global__ void __launch_bounds__(256)
     for (int u = 0; u < 2; ++u) {
       c[u] = 0;
       if (!act[u]) continue;
-      const FrameDesc &fr = frames[fi[u]];
+      const FrameDesc &fr = ONE ? fr1 : frames[fi[u]];
       double s0, s1, s2;
       fractional(fr, r[u][0], r[u][1], r[u][2], s0, s1, s2);
       if (s0 != s0 || s1 != s1 || s2 != s2) atomicOr(&frame_flags[fi[u]], kFrameNaN);
@@ -298,14 +301,15 @@ __global__ void __launch_bounds__(256)
 // coalesced. Two slots per thread and the coordinate gathers issued first
 // keep more loads in flight (the kernel is bound by the latency of its
 // dependent gathers).
-__global__ void __launch_bounds__(256, 3)
+template <bool ONE>
+__global__ void __launch_bounds__(256, ONE ? 4 : 3)
     k_place_records(const double *__restrict__ xyz, const FrameDesc *__restrict__ frames,
                     int nframes, long long npts, long long ncells,
                     const uint32_t *__restrict__ off, const uint2 *__restrict__ tmp,
                     double *__restrict__ sx,
                     double *__restrict__ sy, double *__restrict__ sz, int *__restrict__ sidx,
                     uint32_t *__restrict__ scell, float4 *__restrict__ rec,
-                    int *__restrict__ status) {
+                    int *__restrict__ status, const __grid_constant__ FrameDesc fr1) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long total = off[ncells];
   for (long long p0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; p0 < total;
@@ -345,8 +349,8 @@ __global__ void __launch_bounds__(256, 3)
         atomicOr(status, kStatusBadIndex);
         continue;
       }
-      const int f = nframes == 1 ? 0 : frame_of_point(frames, nframes, g[u]);
-      const FrameDesc &fr = frames[f];
+      const int f = ONE || nframes == 1 ? 0 : frame_of_point(frames, nframes, g[u]);
+      const FrameDesc &fr = ONE ? fr1 : frames[f];
       double s0, s1, s2, q0, q1, q2;
       fractional(fr, r[u][0], r[u][1], r[u][2], s0, s1, s2);
       cartesian(fr, s0, s1, s2, q0, q1, q2);
@@ -414,10 +418,15 @@ int grid_for(long long n, int block) {
 
 long long scan_tiles(long long ncells) { return (ncells + kScanTile - 1) / kScanTile; }
 
-cudaError_t launch_fold_bin(const BatchBuffers &b, cudaStream_t s) {
+cudaError_t launch_fold_bin(const BatchBuffers &b, cudaStream_t s, const FrameDesc *one) {
   if (b.npts <= 0) return cudaSuccess;
-  k_fold_bin<<<grid_for(b.npts, 256), 256, 0, s>>>(b.xyz, b.mask, b.frames, b.nframes, b.npts,
-                                                     b.cell_of, b.arank, b.count, b.frame_flags);
+  const int grid = grid_for(b.npts, 256);
+  if (one && b.nframes == 1)
+    k_fold_bin<true><<<grid, 256, 0, s>>>(b.xyz, b.mask, b.frames, b.nframes, b.npts, b.cell_of,
+                                          b.arank, b.count, b.frame_flags, *one);
+  else
+    k_fold_bin<false><<<grid, 256, 0, s>>>(b.xyz, b.mask, b.frames, b.nframes, b.npts, b.cell_of,
+                                           b.arank, b.count, b.frame_flags, FrameDesc{});
   return cudaGetLastError();
 }
 
@@ -441,15 +450,21 @@ cudaError_t launch_zero_live(const BatchBuffers &b, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_place(const BatchBuffers &b, cudaStream_t s) {
+cudaError_t launch_place(const BatchBuffers &b, cudaStream_t s, const FrameDesc *one) {
   if (b.npts <= 0) return cudaSuccess;
   const int g = grid_for(b.npts, 256);
   k_place_slots<<<g, 256, 0, s>>>(b.frames, b.nframes, b.cell_of, b.arank, b.off, b.tmp, b.npts,
                                   b.ncells, b.out_nn, b.out_d2, b.status);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_place_records<<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.npts, b.ncells, b.off, b.tmp,
-                                    b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec, b.status);
+  if (one && b.nframes == 1)
+    k_place_records<true><<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.npts, b.ncells, b.off,
+                                            b.tmp, b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec,
+                                            b.status, *one);
+  else
+    k_place_records<false><<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.npts, b.ncells, b.off,
+                                             b.tmp, b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec,
+                                             b.status, FrameDesc{});
   return cudaGetLastError();
 }
 

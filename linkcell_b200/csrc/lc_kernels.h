@@ -99,13 +99,15 @@ constexpr int kScanTile = kScanBlock * kScanItems;
 long long scan_tiles(long long ncells);
 
 // fold + bin + cell histogram (one pass over the points).
-cudaError_t launch_fold_bin(const BatchBuffers &b, cudaStream_t s);
+// one: the batch's single frame as the host holds it (read by the kernel from
+// its parameters), or nullptr to read the frames from device memory.
+cudaError_t launch_fold_bin(const BatchBuffers &b, cudaStream_t s, const FrameDesc *one = nullptr);
 // exclusive scan of the histogram (single-pass decoupled look-back).
 cudaError_t launch_scan(const BatchBuffers &b, cudaStream_t s);
 // Zeroes counts and scan tile states of the live cells (device-planned batches).
 cudaError_t launch_zero_live(const BatchBuffers &b, cudaStream_t s);
 // stable cell-sorted placement: arrival slots, then in-cell rank by point id.
-cudaError_t launch_place(const BatchBuffers &b, cudaStream_t s);
+cudaError_t launch_place(const BatchBuffers &b, cudaStream_t s, const FrameDesc *one = nullptr);
 
 // Walk modes.
 enum WalkMode : int {

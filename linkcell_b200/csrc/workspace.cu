@@ -545,9 +545,10 @@ Code WorkspaceImpl::enqueue(BatchBuffers &b, const WalkLaunch &wl, int nf, size_
                                    dcell_.hint, b.mask, frames_.p, live_.p, status_.p, s));
     LC_TRY(launch_zero_live(b, s));
   }
-  LC_TRY(launch_fold_bin(b, s));
+  const FrameDesc *one = wl.one ? &wl.frame1 : nullptr;
+  LC_TRY(launch_fold_bin(b, s, one));
   LC_TRY(launch_scan(b, s));
-  LC_TRY(launch_place(b, s));
+  LC_TRY(launch_place(b, s, one));
   if (timed) LC_TRY(cudaEventRecord(ev_[1], s));
   if (b.proposal) {
     // shell proposals per sorted source (part of the walk phase)
