@@ -2153,8 +2153,10 @@ __device__ void warp_replay(const BatchBuffers &b, const FrameDesc &fr, long lon
   }
 }
 
-template <int KPL>
-__global__ void __launch_bounds__(64, 11) k_replay_warp(BatchBuffers b) {
+// ONE: a single frame, passed as fr1 (read from the constant bank).
+template <int KPL, bool ONE>
+__global__ void __launch_bounds__(64, 11)
+    k_replay_warp(BatchBuffers b, const __grid_constant__ FrameDesc fr1) {
   long long cnt = *b.replay_count;
   if (cnt > b.replay_cap) cnt = b.replay_cap;
   const int lane = threadIdx.x & 31;
@@ -2162,8 +2164,8 @@ __global__ void __launch_bounds__(64, 11) k_replay_warp(BatchBuffers b) {
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long q = warp; q < cnt; q += nwarps) {
     const long long p = b.replay_list[q];
-    const int f = b.nframes == 1 ? 0 : frame_of_sorted(b, p);
-    const FrameDesc &fr = b.frames[f];
+    const int f = ONE || b.nframes == 1 ? 0 : frame_of_sorted(b, p);
+    const FrameDesc &fr = ONE ? fr1 : b.frames[f];
     if ((b.frame_flags[f] & kFrameNaN) || fr.k > 32 * KPL) {
       // NaN comparisons follow the reference's sequential scans: one thread
       if (lane == 0 && warp < b.replay_threads) {
@@ -2461,7 +2463,15 @@ cudaError_t launch_range_partition(const BatchBuffers &b, const RowCuts &cuts, u
   return cudaGetLastError();
 }
 
-cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s) {
+template <int KPL>
+void launch_replay_kpl(const BatchBuffers &b, int grid, const FrameDesc *one, cudaStream_t s) {
+  if (one && b.nframes == 1)
+    k_replay_warp<KPL, true><<<grid, 64, 0, s>>>(b, *one);
+  else
+    k_replay_warp<KPL, false><<<grid, 64, 0, s>>>(b, FrameDesc{});
+}
+
+cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s, const FrameDesc *one) {
   if (b.replay_threads <= 0) return cudaSuccess;
   if (b.kmax <= 256) {
     // one warp per queued source; NaN frames take one thread of the warp
@@ -2469,13 +2479,13 @@ cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s) {
     const int warps = std::max(1, std::min(b.replay_threads, sm_count() * 22));
     const int grid = (warps + 1) / 2;
     if (b.kmax <= 32)
-      k_replay_warp<1><<<grid, 64, 0, s>>>(b);
+      launch_replay_kpl<1>(b, grid, one, s);
     else if (b.kmax <= 64)
-      k_replay_warp<2><<<grid, 64, 0, s>>>(b);
+      launch_replay_kpl<2>(b, grid, one, s);
     else if (b.kmax <= 128)
-      k_replay_warp<4><<<grid, 64, 0, s>>>(b);
+      launch_replay_kpl<4>(b, grid, one, s);
     else
-      k_replay_warp<8><<<grid, 64, 0, s>>>(b);
+      launch_replay_kpl<8>(b, grid, one, s);
     return cudaGetLastError();
   }
   const int block = 128;

@@ -142,7 +142,7 @@ constexpr int kSelGrabs[3] = {8, 16, 32};
 inline int sel_warps_for(int kmax, int i) { return kmax <= 32 ? (i ? 4 : 8) : (i ? 2 : 4); }
 
 cudaError_t launch_walk(const BatchBuffers &b, const WalkLaunch &w, cudaStream_t s);
-cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s);
+cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s, const FrameDesc *one = nullptr);
 // order[pt_base + index] = sorted position of each active source (order is
 // pre-filled with -1 for masked points).
 // Output-row ranges of a host-pointer search: row cuts cut[0] = 0 <

@@ -498,7 +498,7 @@ Code WorkspaceImpl::walk_shard(BatchBuffers &b, const WalkLaunch &wl, cudaStream
   br.src_hi = shard_cut_.p + 1;
   LC_TRY(launch_walk(br, wl, s));
   if (timed) LC_TRY(cudaEventRecord(ev_[2], s));
-  LC_TRY(launch_replay(br, s));
+  LC_TRY(launch_replay(br, s, wl.one ? &wl.frame1 : nullptr));
   LC_TRY(launch_shard_owned(b, shard_cut_.p, shard_.rank, shard_.owned, s));
   if (timed) LC_TRY(cudaEventRecord(ev_[3], s));
   return Code::Ok;
@@ -566,7 +566,7 @@ Code WorkspaceImpl::enqueue(BatchBuffers &b, const WalkLaunch &wl, int nf, size_
   if (timed) LC_TRY(cudaEventRecord(ev_[4], s));
   LC_TRY(launch_walk(b, wl, s));
   if (timed) LC_TRY(cudaEventRecord(ev_[2], s));
-  LC_TRY(launch_replay(b, s));
+  LC_TRY(launch_replay(b, s, wl.one ? &wl.frame1 : nullptr));
   if (timed) LC_TRY(cudaEventRecord(ev_[3], s));
   return Code::Ok;
 }
@@ -824,7 +824,7 @@ Code WorkspaceImpl::walk_in_row_ranges(BatchBuffers &b, const WalkLaunch &wl, cu
     LC_TRY(cudaMemsetAsync(work_.p, 0, sizeof(uint32_t), s));
     LC_TRY(cudaMemsetAsync(replay_count_.p, 0, sizeof(uint32_t), s));
     LC_TRY(launch_walk(br, wl, s));
-    LC_TRY(launch_replay(br, s));
+    LC_TRY(launch_replay(br, s, wl.one ? &wl.frame1 : nullptr));
     LC_TRY(cudaEventRecord(range_ev_[r], s));
     LC_TRY(cudaStreamWaitEvent(copy_stream_, range_ev_[r], 0));
     const size_t e0 = elem_at(r0), ne = elem_at(r1) - e0;
