@@ -1037,12 +1037,6 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
-// Gap (cell units) between a source at fraction f of its cell and the cell
-// at offset d along one axis.
-__device__ __forceinline__ float axis_gap(int d, float f) {
-  return d > 0 ? float(d) - f : (d < 0 ? f + float(-d - 1) : 0.f);
-}
-
 // Ascending bitonic sort of 32 H unsigned keys held H per lane: position q
 // is lane q % 32's key[q / 32]. Every comparator is ascending (the lower
 // position keeps the smaller key): the merge of blocks of kk first pairs q
@@ -1388,7 +1382,6 @@ template <int SN, bool STATS>
 __device__ bool sel_finish(const BatchBuffers &b, long long p, int lane, SelShared<SN> &sh,
                            const FrameDesc &fr, int o, int total, int Rs, int Rp, bool partial) {
   const int k = fr.k;
-  const double cell_min = fr.cell_min;
   // exact distance of buffer entry i (absolute index)
   auto exact = [&](int i) -> double {
     const int t = sh.t[i];
@@ -1565,7 +1558,7 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
                               const FrameDesc &fr1) {
   const int f = ONE || b.nframes == 1 ? 0 : frame_of_sorted(b, p);
   const FrameDesc &fr = ONE ? fr1 : b.frames[f];
-  const int Rp = b.proposal[p];
+  int Rp = b.proposal[p];
   const int k = fr.k;
   const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
   if ((b.frame_flags[f] & kFrameNaN) || Rp <= 0 || Rp > 8 || Rp > fr.max_reach || k > 16 * SN ||
@@ -1588,9 +1581,12 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   // candidate of the reaches below R_p, and usually the k nearest. It
   // settles R* = R_p when at least k candidates lie within rho2 (their
   // distances are then at most rho2, and everything within rho2 is here);
-  // otherwise the whole ball B(R_p) is gathered again.
+  // otherwise the whole ball B(R_p) is gathered again. A gather that
+  // overflows the buffer starts over at R_p - 1 (any proposal gives the same
+  // rows; a long one in a dense region holds more candidates than the buffer).
   int total = 0, Rs = 0;
   bool partial = false;
+retry:
   for (int pass = fr.sel_rho_thr[Rp] < fr.sel_thr[Rp] ? 0 : 1; pass < 2; ++pass) {
   partial = pass == 0;
   const float thr = partial ? fr.sel_rho_thr[Rp] : fr.sel_thr[Rp];
@@ -1753,7 +1749,13 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
         }
         const unsigned km = __ballot_sync(kFull, keep);
         const int nk = __popc(km);
-        if (total + nk > kSelCap) return false;
+        if (total + nk > kSelCap) {
+          if (Rp <= 1) return false;
+          --Rp;
+          if (STATS && lane == 0) ++sh.wc[kWcRegather];
+          __syncwarp();
+          goto retry;
+        }
         if (keep) {
           const int pos = total + __popc(km & lt);
           sh.d[pos] = d32;
