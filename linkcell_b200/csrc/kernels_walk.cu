@@ -1080,6 +1080,14 @@ enum SelWarpCounter {
   kWcPairs, kWcPruned, kWcRerank, kWcSlots
 };
 
+// Square root from the hardware approximation (relative error below 2^-22),
+// for bounds that carry a wider margin than that.
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Exact quotient of x by n from a double reciprocal estimate (x < 2^32).
 __device__ __forceinline__ uint32_t quot(uint32_t x, uint32_t n, double inv) {
   uint32_t q = uint32_t(__double2uint_rz(double(x) * inv));
@@ -1318,7 +1326,9 @@ __device__ int sel_reach(const BatchBuffers &b, long long p, int lane, SelShared
     const float d32 = sh.d[o + i];
     if (use_hist && d32 <= spec_hi) atomicAdd(&sh.hist[min(31, int(d32 * spec_scale))], 1);
     const int s = int(sh.m[o + i] & 255u);
-    const float rr = sqrtf(d32) * inv_c;
+    // sqrt error 2^-22 rr: inside the 16 u (R + 2) of eps_r beside the rest of
+    // the FP32 evaluation (about 1.5 u rr)
+    const float rr = sqrt_approx(d32) * inv_c;
     const float rc = ceilf(rr);
     int bR;
     double dex = -1.0;
@@ -1614,7 +1624,7 @@ retry:
         const float r01 = fr.sel_r01, r02 = fr.sel_r02;
         const float cmin = -(fmaxf(r01 * lo1, r01 * hi1) + fmaxf(r02 * lo2, r02 * hi2));
         const float cmax = -(fminf(r01 * lo1, r01 * hi1) + fminf(r02 * lo2, r02 * hi2));
-        const float hm = sqrtf(fr.sel_ls00 * Q) * 1.0001f + 1e-4f;
+        const float hm = sqrt_approx(fr.sel_ls00 * Q) * 1.0001f + 1e-4f;
         // cells dx with [dx - fa, dx + 1 - fa] meeting [cmin - hm, cmax + hm]:
         // dx <= cmax + hm + fa and dx >= cmin - hm + fa - 1 (with margins)
         const int dxh = int(floorf(fminf(cmax + hm + fa + 1e-4f, float(Rp))));
