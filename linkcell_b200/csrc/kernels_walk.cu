@@ -1044,7 +1044,10 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 // .. 1. Within a lane's keys the lower position is the lower h; across lanes
 // it is the lane whose bit j is clear, so each step is one shuffle and one
 // min-or-max per key.
-template <int H>
+// LOWER: the last merge sorts only the lower half (positions 0 .. 31, key[0]):
+// after its mirror step they hold the 32 smallest keys; the upper ones are
+// left for bitonic_upper.
+template <int H, bool LOWER = false>
 __device__ __forceinline__ void bitonic_sort(uint32_t (&key)[H], int lane) {
 #pragma unroll
   for (int kk = 2; kk <= 32 * H; kk <<= 1) {
@@ -1065,11 +1068,22 @@ __device__ __forceinline__ void bitonic_sort(uint32_t (&key)[H], int lane) {
         const bool lower = (lane & j) == 0;
 #pragma unroll
         for (int h = 0; h < H; ++h) {
+          if (LOWER && kk == 32 * H && h > 0) continue;
           const uint32_t pk = __shfl_xor_sync(kFull, key[h], flip ? kk - 1 : j);
           key[h] = lower ? min(key[h], pk) : max(key[h], pk);
         }
       }
     }
+  }
+}
+
+// The rest of bitonic_sort<2, true>: sorts the upper half (positions 32 ..
+// 63, key[1]), a bitonic sequence after the last merge's mirror step.
+__device__ __forceinline__ void bitonic_upper(uint32_t &k1, int lane) {
+#pragma unroll
+  for (int j = 16; j > 0; j >>= 1) {
+    const uint32_t pk = __shfl_xor_sync(kFull, k1, j);
+    k1 = (lane & j) == 0 ? min(k1, pk) : max(k1, pk);
   }
 }
 
@@ -1145,7 +1159,10 @@ __device__ bool select_sorted(const BatchBuffers &b, long long p, int lane, SelS
         key[h] = (__float_as_uint(d) & ~kSlotMask) | uint32_t(idx);
     }
   }
-  bitonic_sort<H>(key, lane);
+  // k <= 32 (SN = 2): the k-th key is among the 32 smallest, so the upper
+  // half is sorted only when S reaches into it
+  constexpr bool kLower = H == 2 && SN == 2;
+  bitonic_sort<H, kLower>(key, lane);
   uint32_t kv = key[0];
 #pragma unroll
   for (int h = 1; h < H; ++h)
@@ -1156,6 +1173,7 @@ __device__ bool select_sorted(const BatchBuffers &b, long long p, int lane, SelS
   const float TSk =
       __fmul_ru(__fadd_ru(Tup, __fmul_ru(3.f, __fmaf_ru(Tup, 8.f * kU32, beta_s))), 1.f + kRel);
   const uint32_t tsb = __float_as_uint(TSk);
+  if (kLower && __any_sync(kFull, key[H - 1] <= tsb)) bitonic_upper(key[H - 1], lane);
   bool in[H];
   int nS = 0;
 #pragma unroll
