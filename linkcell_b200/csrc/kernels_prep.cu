@@ -309,7 +309,8 @@ __global__ void __launch_bounds__(256, ONE ? 4 : 3)
                     double *__restrict__ sx,
                     double *__restrict__ sy, double *__restrict__ sz, int *__restrict__ sidx,
                     uint32_t *__restrict__ scell, float4 *__restrict__ rec,
-                    int *__restrict__ status, const __grid_constant__ FrameDesc fr1) {
+                    uint32_t *__restrict__ syz, int *__restrict__ status,
+                    const __grid_constant__ FrameDesc fr1) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long total = off[ncells];
   for (long long p0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; p0 < total;
@@ -370,6 +371,8 @@ __global__ void __launch_bounds__(256, ONE ? 4 : 3)
       const double c1 = fr.h[1] * f0 + fr.h[4] * f1 + fr.h[7] * f2 + fr.origin[1];
       const double c2 = fr.h[2] * f0 + fr.h[5] * f1 + fr.h[8] * f2 + fr.origin[2];
       rec[dst] = make_float4(float(q0 - c0), float(q1 - c1), float(q2 - c2), __int_as_float(cx));
+      if (syz)
+        syz[dst] = fr.ny <= 0xFFFF && fr.nz <= 0xFFFF ? uint32_t(cy) | (uint32_t(cz) << 16) : kNoYZ;
     }
   }
 }
@@ -460,11 +463,11 @@ cudaError_t launch_place(const BatchBuffers &b, cudaStream_t s, const FrameDesc 
   if (one && b.nframes == 1)
     k_place_records<true><<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.npts, b.ncells, b.off,
                                             b.tmp, b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec,
-                                            b.status, *one);
+                                            b.syz, b.status, *one);
   else
     k_place_records<false><<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.npts, b.ncells, b.off,
                                              b.tmp, b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec,
-                                             b.status, FrameDesc{});
+                                             b.syz, b.status, FrameDesc{});
   return cudaGetLastError();
 }
 

@@ -1592,14 +1592,21 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   if ((b.frame_flags[f] & kFrameNaN) || Rp <= 0 || Rp > 8 || Rp > fr.max_reach || k > 16 * SN ||
       2 * Rp + 1 > nx || 2 * Rp + 1 > ny || 2 * Rp + 1 > nz)
     return false;
-  const uint32_t lc = b.scell[p];
-  const uint32_t qy = quot(lc, uint32_t(nx), fr.inv_nx);
-  const uint32_t iz_ = quot(lc, uint32_t(nx) * uint32_t(ny), fr.inv_nxy);
-  const int ix = int(lc - qy * uint32_t(nx));
-  const int iy = int(qy - iz_ * uint32_t(ny));
-  const int iz = int(iz_);
-  const long long cb = fr.cell_base;
   const float4 r = b.rec[p];
+  const int ix = __float_as_int(r.w);
+  int iy, iz;
+  const uint32_t yz = b.syz ? b.syz[p] : kNoYZ;
+  if (yz != kNoYZ) {
+    iy = int(yz & 0xFFFFu);
+    iz = int(yz >> 16);
+  } else {
+    const uint32_t lc = b.scell[p];
+    const uint32_t qy = quot(lc, uint32_t(nx), fr.inv_nx);
+    const uint32_t iz_ = quot(lc, uint32_t(nx) * uint32_t(ny), fr.inv_nxy);
+    iy = int(qy - iz_ * uint32_t(ny));
+    iz = int(iz_);
+  }
+  const long long cb = fr.cell_base;
   const float plx = r.x, ply = r.y, plz = r.z;
   const float fa = fr.nhinv[0] * plx + fr.nhinv[1] * ply + fr.nhinv[2] * plz;
   const float fb = fr.nhinv[3] * plx + fr.nhinv[4] * ply + fr.nhinv[5] * plz;

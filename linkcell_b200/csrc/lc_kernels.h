@@ -12,6 +12,8 @@ namespace lc {
 
 // Device buffers of one batch. Sizes: P = points in the batch, C = cells
 // in the batch, F = frames.
+constexpr uint32_t kNoYZ = 0xFFFFFFFFu;
+
 struct BatchBuffers {
   const double *xyz = nullptr;   // P*3, frame-major, caller's
   const int *mask = nullptr;     // caller's; frames index it with mask_base
@@ -35,6 +37,9 @@ struct BatchBuffers {
   int *sidx = nullptr;           // index of the point inside its frame
   uint32_t *scell = nullptr;     // cell id inside the frame
   float4 *rec = nullptr;         // FP32 offset from the cell corner; w: the cell's x index (int bits)
+  // optional: the cell's y | z << 16 (kNoYZ where the frame has more than
+  // 65535 cells along y or z), read by the select walk instead of dividing scell
+  uint32_t *syz = nullptr;
   // outputs (caller's)
   int *out_nn = nullptr;
   double *out_d2 = nullptr;

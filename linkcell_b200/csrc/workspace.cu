@@ -163,7 +163,7 @@ void WorkspaceImpl::release_all() {
   rel(h_mask_); rel(h_nn_); rel(active_); rel(proposal_); rel(cell_prop_); rel(stop_log_);
   rel(order_); rel(csr_counts_); rel(csr_off_); rel(live_); rel(part_cnt_); rel(part_off_);
   rel(part_tiles_); rel(shard_cut_);
-  rel(model_); rel(model_image_); rel(shell_table_);
+  rel(model_); rel(model_image_); rel(shell_table_); rel(syz_);
   shell_table_ready_ = false;
 }
 
@@ -232,6 +232,7 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
       opts.mode == kModeLearned && kmax <= 256 && (opts.fixed_proposal > 0 || has_model_);
   if (learned) {
     LC_TRY(grow(proposal_, P));
+    LC_TRY(grow(syz_, P));
     if (opts.fixed_proposal <= 0 && has_model_) LC_TRY(grow(cell_prop_, C));
   }
   if (!shell_table_ready_) {
@@ -294,6 +295,7 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
   b.sidx = sidx_.p;
   b.scell = scell_.p;
   b.rec = rec_.p;
+  b.syz = learned ? syz_.p : nullptr;
   b.out_nn = out_nn;
   b.out_d2 = out_d2;
   b.work = work_.p;

@@ -262,6 +262,7 @@ class WorkspaceImpl {
   Buf<uint32_t> scell_;
   Buf<double> sx_, sy_, sz_, replay_d_;
   Buf<float4> rec_;
+  Buf<uint32_t> syz_;  // learned walk: the cell's y | z << 16 per sorted point
   Buf<FrameDesc> frames_;
   Buf<long long> counters_;
   Buf<int8_t> proposal_, cell_prop_, stop_log_;
