@@ -1011,7 +1011,7 @@ struct __align__(16) SelSeg {
   int excl;        // first candidate position of the run
   int start;       // its first sorted position
   int xoff;        // dx = candidate cell x + xoff
-  uint32_t meta;   // wrap counts of its candidates in SelShared::m layout
+  uint32_t meta;   // wrap index of its candidates in SelShared::tm layout
   float Dx, Dy, Dz;  // dy e_b + dz e_c (FP32)
   int syz;           // max(1, |dy|, |dz|)
 };
@@ -1020,8 +1020,9 @@ struct __align__(16) SelSeg {
 template <int SN>
 struct SelShared {
   float d[kSelCap];
-  int t[kSelCap];
-  uint32_t m[kSelCap];  // shell | wa + 1 << 8 | wb + 1 << 10 | wc + 1 << 12
+  // x: sorted position; y: shell | ((wa + 1) 9 + (wb + 1) 3 + (wc + 1)) << 8,
+  // the wrap triple as its index into FrameDesc::shift27
+  uint2 tm[kSelCap];
   SelSeg segs[64];
   double sd[32 * SN];
   int sj[32 * SN];
@@ -1155,7 +1156,7 @@ __device__ bool select_sorted(const BatchBuffers &b, long long p, int lane, SelS
     key[h] = 0xffffffffu;
     if (idx < total) {
       const float d = sh.d[o + idx];
-      if (int(sh.m[o + idx] & 255u) <= Rs && d <= Bs_hi)
+      if (int(sh.tm[o + idx].y & 255u) <= Rs && d <= Bs_hi)
         key[h] = (__float_as_uint(d) & ~kSlotMask) | uint32_t(idx);
     }
   }
@@ -1192,10 +1193,9 @@ __device__ bool select_sorted(const BatchBuffers &b, long long p, int lane, SelS
     jj[h] = 0x7fffffff;
     if (32 * h < nS && in[h]) {
       const int i = o + int(key[h] & kSlotMask);
-      const int t = sh.t[i];
-      const uint32_t m = sh.m[i];
-      const double *sh3 =
-          fr.shift27[((m >> 8) & 3u) * 9 + ((m >> 10) & 3u) * 3 + ((m >> 12) & 3u)];
+      const uint2 tm = sh.tm[i];
+      const int t = int(tm.x);
+      const double *sh3 = fr.shift27[tm.y >> 8];
       dd[h] = dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], sh3[0], sh3[1],
                             sh3[2]);
       jj[h] = b.sidx[t];
@@ -1321,9 +1321,9 @@ __device__ int sel_reach(const BatchBuffers &b, long long p, int lane, SelShared
   const double cell_min = fr.cell_min;
   // exact distance of buffer entry i (absolute index)
   auto exact = [&](int i) -> double {
-    const int t = sh.t[i];
-    const uint32_t m = sh.m[i];
-    const double *sh3 = fr.shift27[((m >> 8) & 3u) * 9 + ((m >> 10) & 3u) * 3 + ((m >> 12) & 3u)];
+    const uint2 tm = sh.tm[i];
+    const int t = int(tm.x);
+    const double *sh3 = fr.shift27[tm.y >> 8];
     return dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], sh3[0], sh3[1],
                          sh3[2]);
   };
@@ -1343,7 +1343,7 @@ __device__ int sel_reach(const BatchBuffers &b, long long p, int lane, SelShared
   for (int i = lane; i < total; i += 32) {
     const float d32 = sh.d[o + i];
     if (use_hist && d32 <= spec_hi) atomicAdd(&sh.hist[min(31, int(d32 * spec_scale))], 1);
-    const int s = int(sh.m[o + i] & 255u);
+    const int s = int(sh.tm[o + i].y & 255u);
     // sqrt error 2^-22 rr: inside the 16 u (R + 2) of eps_r beside the rest of
     // the FP32 evaluation (about 1.5 u rr)
     const float rr = sqrt_approx(d32) * inv_c;
@@ -1412,9 +1412,9 @@ __device__ bool sel_finish(const BatchBuffers &b, long long p, int lane, SelShar
   const int k = fr.k;
   // exact distance of buffer entry i (absolute index)
   auto exact = [&](int i) -> double {
-    const int t = sh.t[i];
-    const uint32_t m = sh.m[i];
-    const double *sh3 = fr.shift27[((m >> 8) & 3u) * 9 + ((m >> 10) & 3u) * 3 + ((m >> 12) & 3u)];
+    const uint2 tm = sh.tm[i];
+    const int t = int(tm.x);
+    const double *sh3 = fr.shift27[tm.y >> 8];
     return dist2_shifted(b.sx[p], b.sy[p], b.sz[p], b.sx[t], b.sy[t], b.sz[t], sh3[0], sh3[1],
                          sh3[2]);
   };
@@ -1438,7 +1438,7 @@ __device__ bool sel_finish(const BatchBuffers &b, long long p, int lane, SelShar
     __syncwarp();
     for (int i = lane; i < total; i += 32) {
       const float d32 = sh.d[o + i];
-      if (int(sh.m[o + i] & 255u) <= Rs && d32 <= Bs_hi)
+      if (int(sh.tm[o + i].y & 255u) <= Rs && d32 <= Bs_hi)
         atomicAdd(&sh.hist[min(31, int(d32 * scale))], 1);
     }
     __syncwarp();
@@ -1462,7 +1462,7 @@ __device__ bool sel_finish(const BatchBuffers &b, long long p, int lane, SelShar
   __syncwarp();
   for (int i = lane; i < total; i += 32) {
     const float d32 = sh.d[o + i];
-    if (int(sh.m[o + i] & 255u) > Rs || !(d32 <= Bs_hi)) continue;
+    if (int(sh.tm[o + i].y & 255u) > Rs || !(d32 <= Bs_hi)) continue;
     const float x = d32 * scale;
     if (min(31, int(x)) != bstar) continue;
     const int sub = min(31, int((x - float(bstar)) * 32.f));
@@ -1492,7 +1492,7 @@ __device__ bool sel_finish(const BatchBuffers &b, long long p, int lane, SelShar
   int nS = 0;
   for (int i0 = 0; i0 < total; i0 += 32) {
     const int i = i0 + lane;
-    const bool in = i < total && int(sh.m[o + i] & 255u) <= Rs && sh.d[o + i] <= TS;
+    const bool in = i < total && int(sh.tm[o + i].y & 255u) <= Rs && sh.d[o + i] <= TS;
     const unsigned m = __ballot_sync(kFull, in);
     if (nS + __popc(m) > 32 * SN) return false;  // S larger than the row buffer
     if (in) sh.si[nS + __popc(m & lanemask_lt())] = o + i;
@@ -1511,7 +1511,7 @@ __device__ bool sel_finish(const BatchBuffers &b, long long p, int lane, SelShar
     if (q < nS) {
       const int i = sh.si[q];
       ed[h] = exact(i);
-      ej[h] = b.sidx[sh.t[i]];
+      ej[h] = b.sidx[sh.tm[i].x];
       sh.sd[q] = ed[h];
       sh.sj[q] = ej[h];
     }
@@ -1679,7 +1679,7 @@ retry:
           lenB = int(o[xh - nx + 1]) - sB;
           wrapB = 1;
         }
-        wbc = ((wb + 1) << 10) | ((wc + 1) << 12);
+        wbc = (wb + 1) * 3 + (wc + 1);
         const float fdy = float(dy), fdz = float(dz);
         Dx = fdy * fr.ev[3] + fdz * fr.ev[6];
         Dy = fdy * fr.ev[4] + fdz * fr.ev[7];
@@ -1715,7 +1715,7 @@ retry:
         sg.excl = excl;
         sg.start = startA;
         sg.xoff = -ix;
-        sg.meta = (1u << 8) | uint32_t(wbc);
+        sg.meta = uint32_t(9 + wbc) << 8;
         sg.Dx = Dx, sg.Dy = Dy, sg.Dz = Dz, sg.syz = syz;
         sh.segs[si] = sg;
       }
@@ -1724,7 +1724,7 @@ retry:
         sg.excl = exclB;
         sg.start = sB;
         sg.xoff = -ix + wrapB * nx;
-        sg.meta = (uint32_t(wrapB + 1) << 8) | uint32_t(wbc);
+        sg.meta = uint32_t((wrapB + 1) * 9 + wbc) << 8;
         sg.Dx = Dx, sg.Dy = Dy, sg.Dz = Dz, sg.syz = syz;
         sh.segs[si + (lenA > 0 ? 1 : 0)] = sg;
       }
@@ -1794,8 +1794,7 @@ retry:
         if (keep) {
           const int pos = total + __popc(km & lt);
           sh.d[pos] = d32;
-          sh.t[pos] = t[w];
-          sh.m[pos] = mm;
+          sh.tm[pos] = make_uint2(uint32_t(t[w]), mm);
         }
         total += nk;
       }
