@@ -1095,6 +1095,25 @@ enum SelWarpCounter {
   kWcPairs, kWcPruned, kWcRerank, kWcSlots
 };
 
+// Packed FP32 pairs (Blackwell's f32x2 instructions round each component as
+// the scalar instruction does).
+__device__ __forceinline__ unsigned long long f2_pack(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+
+// (q - p) + fma(f, e, D) for the x and y components at once.
+__device__ __forceinline__ void offset_xy(float qx, float qy, unsigned long long pxy, float f,
+                                          unsigned long long exy, float Dx, float Dy, float &ox,
+                                          float &oy) {
+  unsigned long long a, c, r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(a) : "l"(f2_pack(qx, qy)), "l"(pxy));
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(c) : "l"(f2_pack(f, f)), "l"(exy), "l"(f2_pack(Dx, Dy)));
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(c));
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(ox), "=f"(oy) : "l"(r));
+}
+
 // Square root from the hardware approximation (relative error below 2^-22),
 // for bounds that carry a wider margin than that.
 __device__ __forceinline__ float sqrt_approx(float x) {
@@ -1612,6 +1631,8 @@ __device__ bool select_source(const BatchBuffers &b, long long p, int lane, SelS
   const float fb = fr.nhinv[3] * plx + fr.nhinv[4] * ply + fr.nhinv[5] * plz;
   const float fc = fr.nhinv[6] * plx + fr.nhinv[7] * ply + fr.nhinv[8] * plz;
   const float ev0 = fr.ev[0], ev1 = fr.ev[1], ev2 = fr.ev[2];
+  const unsigned long long pxy = f2_pack(plx, ply), exy = f2_pack(ev0, ev1);
+  const int p32 = p <= 0x7fffffffLL ? int(p) : -1;  // candidate positions are ints
   // The first gather covers only rho2 = max(B(R_p - 1), q B(R_p)): every
   // candidate of the reaches below R_p, and usually the k nearest. It
   // settles R* = R_p when at least k candidates lie within rho2 (their
@@ -1759,7 +1780,7 @@ retry:
         if (live[w]) {
           const SelSeg &S = sh.segs[owner[w]];
           t[w] = S.start + (g - S.excl);
-          live[w] = (long long)t[w] != p;
+          live[w] = t[w] != p32;
         }
       }
       float4 q[kSelWin];
@@ -1775,8 +1796,8 @@ retry:
           const SelSeg &S = sh.segs[owner[w]];
           const int dx = __float_as_int(q[w].w) + S.xoff;  // the candidate cell's x offset
           const float fdx = float(dx);
-          const float ex = (q[w].x - plx) + fmaf(fdx, ev0, S.Dx);
-          const float ey = (q[w].y - ply) + fmaf(fdx, ev1, S.Dy);
+          float ex, ey;  // (q.x - plx) + fmaf(fdx, ev0, S.Dx), and y likewise
+          offset_xy(q[w].x, q[w].y, pxy, fdx, exy, S.Dx, S.Dy, ex, ey);
           const float ez = (q[w].z - plz) + fmaf(fdx, ev2, S.Dz);
           d32 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
           keep = !(d32 > thr);
