@@ -258,7 +258,7 @@ int lc_knearest_batch(const double *xyz, const lc_frame *frames, size_t n_frames
  * reference). For callers that cannot call cudaMalloc: hosts whose own pool
  * allocator owns all device memory, real-time loops that must not allocate,
  * plug-ins inside frameworks that own the allocator. Every scratch buffer
- * lives in one fixed static device array (about 5.1 MB on each GPU that
+ * lives in one fixed static device array (about 6.7 MB on each GPU that
  * loads the library, held until exit); the caller passes device xyz, mask
  * (n ints or NULL), out_nn and out_d2 (n * k each, out_d2 may be NULL) and
  * a host lc_cell. Limits: n <= 65536 points, at most 65536 linked cells,

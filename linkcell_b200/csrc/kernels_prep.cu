@@ -140,9 +140,11 @@ __global__ void __launch_bounds__(kScanBlock)
     uint32_t v[kScanItems];
     if (base + kScanItems <= nlive) {
       const uint4 *src = reinterpret_cast<const uint4 *>(count + base);
-      const uint4 a = src[0], b = src[1];
-      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-      v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+#pragma unroll
+      for (int m = 0; m < kScanItems / 4; ++m) {
+        const uint4 a = src[m];
+        v[4 * m + 0] = a.x; v[4 * m + 1] = a.y; v[4 * m + 2] = a.z; v[4 * m + 3] = a.w;
+      }
     } else {
 #pragma unroll
       for (int m = 0; m < kScanItems; ++m) v[m] = (base + m < nlive) ? count[base + m] : 0u;
@@ -229,8 +231,9 @@ __global__ void __launch_bounds__(kScanBlock)
         run += v[m];
       }
       uint4 *dst = reinterpret_cast<uint4 *>(off + base);
-      dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
-      dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+#pragma unroll
+      for (int m = 0; m < kScanItems / 4; ++m)
+        dst[m] = make_uint4(o[4 * m + 0], o[4 * m + 1], o[4 * m + 2], o[4 * m + 3]);
     } else {
 #pragma unroll
       for (int m = 0; m < kScanItems; ++m) {
@@ -258,55 +261,92 @@ __global__ void k_zero_live(uint32_t *__restrict__ count, unsigned long long *__
     tile_state[t] = 0ull;
 }
 
-// Arrival slots: tmp[off[c] + arank[g]] = (g, c). The output rows of masked
-// points are filled here with -1 / NaN (src/knearest.rs:293-296).
+// Arrival slots: tmp[off[c] + arank[g]] = (g, c, folded coordinates of g).
+// The coordinates are read here in point order (coalesced) and folded
+// again (the same fractional / cartesian expressions as the bin), so the
+// stable placement after this reads its slots as one stream and gathers
+// nothing by point id. The output rows of masked points are filled here
+// with -1 / NaN (src/knearest.rs:293-296). Two points per thread per trip:
+// their loads, and then their dependent cell-offset loads, are in flight
+// together. ONE: a single frame, passed as fr1.
+template <bool ONE>
 __global__ void __launch_bounds__(256)
-    k_place_slots(const FrameDesc *__restrict__ frames, int nframes,
-                  const uint32_t *__restrict__ cell_of, const uint32_t *__restrict__ arank,
-                  const uint32_t *__restrict__ off, uint2 *__restrict__ tmp, long long npts,
-                  long long ncells, int *__restrict__ out_nn, double *__restrict__ out_d2,
-                  int *__restrict__ status) {
+    k_place_slots(const double *__restrict__ xyz, const FrameDesc *__restrict__ frames,
+                  int nframes, const uint32_t *__restrict__ cell_of,
+                  const uint32_t *__restrict__ arank, const uint32_t *__restrict__ off,
+                  PlaceSlot *__restrict__ tmp, long long npts, long long ncells,
+                  int *__restrict__ out_nn, double *__restrict__ out_d2, int *__restrict__ status,
+                  const __grid_constant__ FrameDesc fr1) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long total = off[ncells];
-  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += stride) {
-    const uint32_t c = cell_of[g];
-    if (c == kInactive) {
-      const int f = nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
-      const FrameDesc &fr = frames[f];
-      const long long i = g - fr.pt_base;
-      int *row = out_nn + fr.out_base + i * fr.k;
-      for (int s = 0; s < fr.k; ++s) row[s] = -1;
-      if (out_d2) {
-        double *drow = out_d2 + fr.out_base + i * fr.k;
-        const double nan = __longlong_as_double(0x7ff8000000000000ll);
-        for (int s = 0; s < fr.k; ++s) drow[s] = nan;
+  for (long long g0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; g0 < npts;
+       g0 += 2 * stride) {
+    const long long gg[2] = {g0, g0 + stride};
+    uint32_t c[2], rk[2];
+    double r[2][3];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const long long g = gg[u];
+      c[u] = g < npts ? cell_of[g] : kInactive;
+      rk[u] = 0u;
+      if (c[u] == kInactive) continue;
+      rk[u] = arank[g];
+      r[u][0] = xyz[3 * g + 0];
+      r[u][1] = xyz[3 * g + 1];
+      r[u][2] = xyz[3 * g + 2];
+    }
+    long long pos[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+      pos[u] = c[u] != kInactive && c[u] < ncells ? (long long)off[c[u]] + rk[u] : -1;
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const long long g = gg[u];
+      if (g >= npts) continue;
+      if (c[u] == kInactive) {
+        const int f = ONE || nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
+        const FrameDesc &fr = ONE ? fr1 : frames[f];
+        const long long i = g - fr.pt_base;
+        int *row = out_nn + fr.out_base + i * fr.k;
+        for (int s = 0; s < fr.k; ++s) row[s] = -1;
+        if (out_d2) {
+          double *drow = out_d2 + fr.out_base + i * fr.k;
+          const double nan = __longlong_as_double(0x7ff8000000000000ll);
+          for (int s = 0; s < fr.k; ++s) drow[s] = nan;
+        }
+        continue;
       }
-      continue;
+      if (pos[u] < 0 || pos[u] >= total) {
+        atomicOr(status, kStatusBadIndex);
+        continue;
+      }
+      const int f = ONE || nframes == 1 ? 0 : frame_of_point(frames, nframes, g);
+      const FrameDesc &fr = ONE ? fr1 : frames[f];
+      double s0, s1, s2, q0, q1, q2;
+      fractional(fr, r[u][0], r[u][1], r[u][2], s0, s1, s2);
+      cartesian(fr, s0, s1, s2, q0, q1, q2);
+      // two 16-byte stores: (g, c, q0) and (q1, q2)
+      double2 *w = reinterpret_cast<double2 *>(tmp + pos[u]);
+      const unsigned long long gc = (unsigned long long)c[u] << 32 | uint32_t(g);
+      w[0] = make_double2(__longlong_as_double((long long)gc), q0);
+      w[1] = make_double2(q1, q2);
     }
-    const long long pos = (long long)off[c] + arank[g];
-    if (pos >= total || c >= ncells) {
-      atomicOr(status, kStatusBadIndex);
-      continue;
-    }
-    tmp[pos] = make_uint2(uint32_t(g), c);
   }
 }
 
 // Stable placement, one thread per sorted slot: the point g arriving at
 // slot pos of cell c lands at off[c] + (number of points of c with a
 // smaller id), so the order inside a cell is by point id (the reference
-// bins points in id order). The slot holds the cell next to the point id,
-// so the only gather by id is g's coordinates; the writes of the sorted SoA
-// records stay within the cell's few slots, so a warp's stores remain
-// coalesced. Two slots per thread and the coordinate gathers issued first
-// keep more loads in flight (the kernel is bound by the latency of its
-// dependent gathers).
+// bins points in id order). The slot carries the point's cell and folded
+// coordinates, so the kernel reads its slots, the cell offsets and the
+// ids of the cell's other slots in sorted order, with no gather by id; the
+// writes of the sorted SoA records stay within the cell's few slots, so a
+// warp's stores remain coalesced.
 template <bool ONE>
 __global__ void __launch_bounds__(256, ONE ? 4 : 3)
-    k_place_records(const double *__restrict__ xyz, const FrameDesc *__restrict__ frames,
-                    int nframes, long long npts, long long ncells,
-                    const uint32_t *__restrict__ off, const uint2 *__restrict__ tmp,
-                    double *__restrict__ sx,
+    k_place_records(const FrameDesc *__restrict__ frames, int nframes, long long npts,
+                    long long ncells, const uint32_t *__restrict__ off,
+                    const PlaceSlot *__restrict__ tmp, double *__restrict__ sx,
                     double *__restrict__ sy, double *__restrict__ sz, int *__restrict__ sidx,
                     uint32_t *__restrict__ scell, float4 *__restrict__ rec,
                     uint32_t *__restrict__ syz, int *__restrict__ status,
@@ -318,33 +358,32 @@ __global__ void __launch_bounds__(256, ONE ? 4 : 3)
     long long pos[2] = {p0, p0 + stride};
     bool live[2];
     uint32_t g[2], c[2];
-    double r[2][3];
+    double q[2][3];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
       live[u] = pos[u] < total;
-      const uint2 gc = live[u] ? tmp[pos[u]] : make_uint2(0u, kInactive);
-      g[u] = gc.x;
-      c[u] = gc.y;
-    }
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const bool ok = live[u] && (long long)g[u] < npts;
-      const long long b3 = 3 * (long long)g[u];
-      r[u][0] = ok ? xyz[b3 + 0] : 0.0;
-      r[u][1] = ok ? xyz[b3 + 1] : 0.0;
-      r[u][2] = ok ? xyz[b3 + 2] : 0.0;
-      if (!ok) c[u] = kInactive;
+      g[u] = 0u;
+      c[u] = kInactive;
+      if (!live[u]) continue;
+      const double2 *w = reinterpret_cast<const double2 *>(tmp + pos[u]);
+      const double2 w0 = w[0], w1 = w[1];
+      const unsigned long long gc = (unsigned long long)__double_as_longlong(w0.x);
+      g[u] = uint32_t(gc);
+      c[u] = uint32_t(gc >> 32);
+      q[u][0] = w0.y;
+      q[u][1] = w1.x;
+      q[u][2] = w1.y;
     }
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
       if (!live[u]) continue;
-      if (c[u] >= ncells) {
+      if (c[u] >= ncells || (long long)g[u] >= npts) {
         atomicOr(status, kStatusBadIndex);
         continue;
       }
       const uint32_t a = off[c[u]], e = off[c[u] + 1];
       uint32_t rk = 0;
-      for (uint32_t q = a; q < e; ++q) rk += tmp[q].x < g[u] ? 1u : 0u;
+      for (uint32_t t = a; t < e; ++t) rk += tmp[t].g < g[u] ? 1u : 0u;
       const long long dst = (long long)a + rk;
       if (dst >= (long long)e) {
         atomicOr(status, kStatusBadIndex);
@@ -352,9 +391,7 @@ __global__ void __launch_bounds__(256, ONE ? 4 : 3)
       }
       const int f = ONE || nframes == 1 ? 0 : frame_of_point(frames, nframes, g[u]);
       const FrameDesc &fr = ONE ? fr1 : frames[f];
-      double s0, s1, s2, q0, q1, q2;
-      fractional(fr, r[u][0], r[u][1], r[u][2], s0, s1, s2);
-      cartesian(fr, s0, s1, s2, q0, q1, q2);
+      const double q0 = q[u][0], q1 = q[u][1], q2 = q[u][2];
       sx[dst] = q0;
       sy[dst] = q1;
       sz[dst] = q2;
@@ -456,18 +493,26 @@ cudaError_t launch_zero_live(const BatchBuffers &b, cudaStream_t s) {
 cudaError_t launch_place(const BatchBuffers &b, cudaStream_t s, const FrameDesc *one) {
   if (b.npts <= 0) return cudaSuccess;
   const int g = grid_for(b.npts, 256);
-  k_place_slots<<<g, 256, 0, s>>>(b.frames, b.nframes, b.cell_of, b.arank, b.off, b.tmp, b.npts,
-                                  b.ncells, b.out_nn, b.out_d2, b.status);
+  const bool single = one && b.nframes == 1;
+  const FrameDesc fr1 = single ? *one : FrameDesc{};
+  if (single)
+    k_place_slots<true><<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.cell_of, b.arank, b.off,
+                                          b.tmp, b.npts, b.ncells, b.out_nn, b.out_d2, b.status,
+                                          fr1);
+  else
+    k_place_slots<false><<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.cell_of, b.arank, b.off,
+                                           b.tmp, b.npts, b.ncells, b.out_nn, b.out_d2, b.status,
+                                           fr1);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  if (one && b.nframes == 1)
-    k_place_records<true><<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.npts, b.ncells, b.off,
-                                            b.tmp, b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec,
-                                            b.syz, b.status, *one);
+  if (single)
+    k_place_records<true><<<g, 256, 0, s>>>(b.frames, b.nframes, b.npts, b.ncells, b.off, b.tmp,
+                                            b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec, b.syz,
+                                            b.status, fr1);
   else
-    k_place_records<false><<<g, 256, 0, s>>>(b.xyz, b.frames, b.nframes, b.npts, b.ncells, b.off,
-                                             b.tmp, b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec,
-                                             b.syz, b.status, FrameDesc{});
+    k_place_records<false><<<g, 256, 0, s>>>(b.frames, b.nframes, b.npts, b.ncells, b.off, b.tmp,
+                                             b.sx, b.sy, b.sz, b.sidx, b.scell, b.rec, b.syz,
+                                             b.status, fr1);
   return cudaGetLastError();
 }
 

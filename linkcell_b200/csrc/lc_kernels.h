@@ -14,6 +14,14 @@ namespace lc {
 // in the batch, F = frames.
 constexpr uint32_t kNoYZ = 0xFFFFFFFFu;
 
+// A point at its arrival slot inside its cell: the point id, the batch cell
+// and the folded FP64 coordinates, 32 bytes (two 16-byte words).
+struct __align__(16) PlaceSlot {
+  uint32_t g, c;
+  double q0, q1, q2;
+};
+static_assert(sizeof(PlaceSlot) == 32, "PlaceSlot is two 16-byte words");
+
 struct BatchBuffers {
   const double *xyz = nullptr;   // P*3, frame-major, caller's
   const int *mask = nullptr;     // caller's; frames index it with mask_base
@@ -25,7 +33,7 @@ struct BatchBuffers {
   const long long *live_cells = nullptr;
   uint32_t *cell_of = nullptr;   // P: batch cell id or kInactive
   uint32_t *arank = nullptr;     // P: arrival rank inside the cell (atomics)
-  uint2 *tmp = nullptr;          // P: (point id, cell) at the point's arrival slot
+  PlaceSlot *tmp = nullptr;      // P: the point at its arrival slot
   uint32_t *count = nullptr;     // C
   uint32_t *off = nullptr;       // C+1: exclusive scan of count
   unsigned long long *tile_state = nullptr;  // scan tiles
@@ -98,7 +106,7 @@ enum WalkCounters : int {
 constexpr int kShellTableRmax = 16;
 
 constexpr int kScanBlock = 256;
-constexpr int kScanItems = 8;
+constexpr int kScanItems = 16;  // a multiple of 4 (16-byte loads and stores)
 constexpr int kScanTile = kScanBlock * kScanItems;
 
 long long scan_tiles(long long ncells);

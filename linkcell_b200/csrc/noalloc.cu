@@ -66,7 +66,7 @@ constexpr Layout make_layout() {
   l.small = o; o += align256(8 * sizeof(uint32_t));
   l.cell_of = o; o += align256(P * 4);
   l.arank = o; o += align256(P * 4);
-  l.tmp = o; o += align256(P * 8);
+  l.tmp = o; o += align256(P * sizeof(lc::PlaceSlot));
   l.count = o; o += align256(C * 4);
   l.off = o; o += align256((C + 1) * 4);
   l.tile_state = o; o += align256(tiles * 8);
@@ -85,7 +85,7 @@ constexpr Layout make_layout() {
 
 constexpr Layout kLayout = make_layout();
 
-// About 5.1 MB per device.
+// About 6.7 MB per device.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kLayout.total];
 
 // Device address of the scratch array in the current device's context.
@@ -171,7 +171,7 @@ extern "C" int lc_gpu_knearest_noalloc(const double *xyz, size_t n, const struct
   b.ncells = ncells;
   b.cell_of = reinterpret_cast<uint32_t *>(base + L.cell_of);
   b.arank = reinterpret_cast<uint32_t *>(base + L.arank);
-  b.tmp = reinterpret_cast<uint2 *>(base + L.tmp);
+  b.tmp = reinterpret_cast<lc::PlaceSlot *>(base + L.tmp);
   b.count = reinterpret_cast<uint32_t *>(base + L.count);
   b.off = reinterpret_cast<uint32_t *>(base + L.off);
   b.tile_state = reinterpret_cast<unsigned long long *>(base + L.tile_state);

@@ -256,7 +256,7 @@ class WorkspaceImpl {
   cudaStream_t last_stream_ = nullptr;  // stream of the last batch
 
   Buf<uint32_t> cell_of_, arank_, count_, off_, tile_counter_, work_, replay_count_;
-  Buf<uint2> tmp_;
+  Buf<PlaceSlot> tmp_;
   Buf<unsigned long long> tile_state_;
   Buf<int> status_, frame_flags_, sidx_, replay_list_, replay_i_;
   Buf<uint32_t> scell_;

@@ -36,8 +36,8 @@ def test_scan_wait_runs_out_and_is_reported(gpu, lib, oracle_mod, mode):
     import torch
     from gpu_helpers import assert_same, lc_cell_of
     from linkcell_b200 import _capi
-    box = [60.0, 60.0, 60.0]  # 20^3 = 8,000 cells: four scan tiles of 2,048
-    xyz = np.random.default_rng(8).random((20000, 3)) * 60.0
+    box = [90.0, 90.0, 90.0]  # 30^3 = 27,000 cells: seven scan tiles of 4,096
+    xyz = np.random.default_rng(8).random((20000, 3)) * 90.0
     want = oracle_mod.knearest(xyz, box, 12, cell_hint=3.0)
     cell = lc_cell_of(box)
     x = torch.as_tensor(xyz, device="cuda")
