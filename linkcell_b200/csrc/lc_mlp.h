@@ -44,8 +44,8 @@ cudaError_t mlp_grad(const float *params, const float *X, const int *y, int B, M
                      float *grad, float *loss, cudaStream_t s);
 cudaError_t mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr,
                      cudaStream_t s);
-// Proposed shell per cell (tcgen05 inference over 128-cell tiles of four
-// 32-cell row segments, the first layer as a 5x5x5 convolution of the
+// Proposed shell per cell (tcgen05 inference over 16 x 8-cell tiles of 128
+// cells, the first layer as a 5x5x5 convolution of the
 // occupancy grid), then per sorted source.
 cudaError_t mlp_propose(const void *image, const BatchBuffers &b, int8_t *cell_prop,
                         int8_t *source_prop, float tau, cudaStream_t s);

@@ -65,7 +65,7 @@ struct FrameDesc {
   long long cell_base;  // first cell of the frame in the batch
   long long out_base;   // first output element (row 0, slot 0)
   long long mask_base;  // offset of the frame's mask (shared masks repeat 0)
-  long long tile_base;  // first 32 x 4-cell tile of the frame (shell proposals)
+  long long tile_base;  // first 16 x 8-cell tile of the frame (shell proposals)
   // Cube select walk, per reach R = 1..8 (index R): the FP32 filter at
   // B(R) = (R cell_min)^2, the row-trimming limit thr / (0.99 lam_min), the
   // FP32 error offset beta (rounded up), B(R) + 2 band(B(R)) rounded up,
@@ -88,6 +88,14 @@ struct FrameDesc {
   // at index (na + 1) 9 + (nb + 1) 3 + (nc + 1), in the reference expression
   double shift27[27][3];
 };
+
+// Shell-proposal tiles: kPropTileX x kPropTileY cells of one z plane of one
+// frame, numbered x fastest, then y, then z (the network's M = 128 rows).
+constexpr int kPropTileX = 16, kPropTileY = 8;
+LC_HD long long proposal_tiles(int nx, int ny, int nz) {
+  return (long long)((nx + kPropTileX - 1) / kPropTileX) * ((ny + kPropTileY - 1) / kPropTileY) *
+         nz;
+}
 
 // ------------------------------------------------------------ exact FP64
 LC_HD double xadd(double a, double b) {

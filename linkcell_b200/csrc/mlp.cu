@@ -254,8 +254,8 @@ __global__ void k_training_rows(BatchBuffers b, const int8_t *__restrict__ stop_
 
 // ---------------------------------------------------------------------
 // Tensor-core inference on the 5th-generation tensor cores (tcgen05). A
-// group of four warps evaluates 128 cells at a time -- four 32-cell row
-// segments, one warp per segment and lane quarter of tensor memory -- as
+// group of four warps evaluates 128 cells at a time -- a 16 x 8-cell tile,
+// two 16-cell rows per warp and lane quarter of tensor memory -- as
 // the M = 128 rows of the three layers:
 //   D1 = A1 W1^T  (A1: [128 x 128] occupancy features, 126 used),
 //   D2 = SiLU(D1 + b1) W2^T,  D3 = SiLU(D2 + b2) W3^T  (N = 64, 64, 16 with 8 used).
@@ -265,7 +265,7 @@ __global__ void k_training_rows(BatchBuffers b, const int8_t *__restrict__ stop_
 // group's mbarrier once the products are done; every warp then reads its 32
 // accumulator lanes with tcgen05.ld, adds the bias, applies SiLU and writes
 // the next layer's A operand. Layer 1 is a 5x5x5 convolution of the
-// occupancy grid: the group stages the tile's 36 x 8 x 5 halo of
+// occupancy grid: the group stages the tile's 20 x 12 x 5 halo of
 // log(1 + count), and each lane writes its cell's 128 features (16-byte
 // chunks) from it, in two K halves.
 //
@@ -273,8 +273,10 @@ __global__ void k_training_rows(BatchBuffers b, const int8_t *__restrict__ stop_
 // rows of a core matrix are 16 B apart, 8-row groups SBO = 128 B apart, and
 // the 16-byte K chunks LBO apart (LBO = rows x 16 B).
 constexpr int kUmmaThreads = 256;   // two groups of four warps
-constexpr int kHaloW = 40;          // halves per halo row (36 used: x0 - 2 .. x0 + 33)
-constexpr int kHaloRows = 40;       // halo rows of a tile: 8 y x 5 z
+// halves per halo row: x0 - 2 .. x0 + 17. Lanes 16-31 read the halo five rows
+// (200 bytes) after lanes 0-15, which puts their 32-byte spans on other banks.
+constexpr int kHaloW = kPropTileX + 4;
+constexpr int kHaloRows = (kPropTileY + 4) * 5;  // halo rows of a tile: 12 y x 5 z
 constexpr int kMbarSpin = 1 << 22;  // bounded wait for the tensor cores
 // A CTA runs kGroups groups of four warps (one per lane quarter of tensor
 // memory), each on its own tile with its own operand buffer, halo, 64
@@ -460,10 +462,13 @@ __device__ __forceinline__ void hidden_to_a(uint32_t taddr, const float *bias, _
   }
 }
 
-// A tile of the shell-proposal network: 32 cells along x (x0 .. x0 + 31)
-// in each of 4 rows y0 .. y0 + 3 of one z plane of one frame (quarter q of
-// the 128 matrix rows = row y0 + q). Tiles are numbered frame by frame
-// (FrameDesc::tile_base), x fastest, then y in steps of 4, then z.
+// A tile of the shell-proposal network: 16 cells along x (x0 .. x0 + 15)
+// in each of 8 rows y0 .. y0 + 7 of one z plane of one frame. Matrix row
+// m = 32 q + lane is cell (x0 + lane % 16, y0 + 2 q + lane / 16). Tiles are
+// numbered frame by frame (FrameDesc::tile_base), x fastest, then y in
+// steps of 8, then z. 16 x 8 pads a mesh less than 32 x 4 does along x,
+// where most meshes are not a multiple of 32 (138 x 135 x 140 cells: 5 %
+// padding against 17 %).
 struct TileInfo {
   const FrameDesc *fr;
   int ncl, x0, y0, z0;  // ncl: cells of each row inside the frame (0 past the last tile)
@@ -491,14 +496,15 @@ __device__ __forceinline__ TileInfo tile_info(const FrameDesc *__restrict__ fram
   g.fr = &frames[f];
   const FrameDesc &fr = *g.fr;
   // a frame has fewer than 2^31 cells, so its tile numbers fit 32 bits
-  const uint32_t per_x = uint32_t(fr.nx + 31) / 32u, per_y = uint32_t(fr.ny + 3) / 4u;
+  const uint32_t per_x = uint32_t(fr.nx + kPropTileX - 1) / uint32_t(kPropTileX);
+  const uint32_t per_y = uint32_t(fr.ny + kPropTileY - 1) / uint32_t(kPropTileY);
   const uint32_t lt = uint32_t(tile - fr.tile_base);
-  const uint32_t row = lt / per_x;  // (z, y / 4)
+  const uint32_t row = lt / per_x;  // (z, y / kPropTileY)
   const uint32_t zq = row / per_y;
-  g.x0 = int(lt - row * per_x) * 32;
-  g.y0 = int(row - zq * per_y) * 4;
+  g.x0 = int(lt - row * per_x) * kPropTileX;
+  g.y0 = int(row - zq * per_y) * kPropTileY;
   g.z0 = int(zq);
-  g.ncl = min(32, fr.nx - g.x0);
+  g.ncl = min(kPropTileX, fr.nx - g.x0);
   return g;
 }
 
@@ -509,51 +515,49 @@ __device__ __forceinline__ int wrap_cell(int c, int n) {
   return unsigned(c) < unsigned(n) ? c : rem_euclid(c, n);
 }
 
-// The tile's halo of log(1 + count): 36 columns x0 - 2 .. x0 + 33 of the
-// 8 x 5 rows (y0 - 2 .. y0 + 5, z0 - 2 .. z0 + 2), row (yi, zi) at halo row
-// yi * 5 + zi. Warp w of the group stages the rows of yi = 2 w and 2 w + 1,
-// five at a time: lane l column l, and lanes 0-3 columns 32-35, the ten
-// loads in flight before the first store.
+// The tile's halo of log(1 + count): the 20 columns x0 - 2 .. x0 + 17 of
+// the 12 x 5 rows (y0 - 2 .. y0 + 9, z0 - 2 .. z0 + 2), row (yi, zi) at halo
+// row yi * 5 + zi. Warp w of the group stages the 300 cells of yi = 3 w ..
+// 3 w + 2, about ten per lane, all ten loads in flight before the first store.
 __device__ __forceinline__ void stage_halo(const TileInfo &g, const uint32_t *__restrict__ count,
                                            const float *lg1p, __half *halo, int w) {
+  static_assert(kPropTileY + 4 == 3 * kGroupWarps, "three halo y rows per warp");
+  constexpr int kPerWarp = 3 * 5 * kHaloW;  // 300 cells
+  constexpr int kLoads = (kPerWarp + 31) / 32;
   const int lane = threadIdx.x & 31;
   auto feat = [&](uint32_t v) { return __float2half_rn(v < 64u ? lg1p[v] : log1pf(float(v))); };
+  uint32_t c[kLoads];
 #pragma unroll
-  for (int t = 0; t < 8 / kGroupWarps; ++t) {
-    const int yi = (8 / kGroupWarps) * w + t;
-    uint32_t c[10];
-#pragma unroll
-    for (int i = 0; i < 10; ++i) c[i] = 0u;
-    if (g.ncl > 0) {
+  for (int i = 0; i < kLoads; ++i) {
+    c[i] = 0u;
+    const int t = 32 * i + lane;
+    if (g.ncl > 0 && t < kPerWarp) {
       const FrameDesc &fr = *g.fr;
       const int nx = fr.nx, ny = fr.ny, nz = fr.nz;
+      const int yi = 3 * w + t / (5 * kHaloW), r = t % (5 * kHaloW);
+      const int zi = r / kHaloW, col = r % kHaloW;
       const int jy = wrap_cell(g.y0 + yi - 2, ny);
-      const int jx0 = wrap_cell(g.x0 + lane - 2, nx);
-      const int jx1 = wrap_cell(g.x0 + lane + 30, nx);
-#pragma unroll
-      for (int j = 0; j < 5; ++j) {
-        const int jz = wrap_cell(g.z0 + j - 2, nz);
-        const uint32_t *row = count + fr.cell_base + ((long long)jz * ny + jy) * (long long)nx;
-        c[j] = row[jx0];
-        if (lane < 4) c[5 + j] = row[jx1];
-      }
+      const int jz = wrap_cell(g.z0 + zi - 2, nz);
+      const int jx = wrap_cell(g.x0 + col - 2, nx);
+      c[i] = count[fr.cell_base + ((long long)jz * ny + jy) * (long long)nx + jx];
     }
-    __half *h = halo + yi * 5 * kHaloW + lane;
+  }
+  __half *h = halo + 3 * w * 5 * kHaloW;  // the warp's 15 halo rows, contiguous
 #pragma unroll
-    for (int j = 0; j < 5; ++j) {
-      h[j * kHaloW] = feat(c[j]);
-      if (lane < 4) h[j * kHaloW + 32] = feat(c[5 + j]);
-    }
+  for (int i = 0; i < kLoads; ++i) {
+    const int t = 32 * i + lane;
+    if (t < kPerWarp) h[t] = feat(c[i]);
   }
 }
 
 // Feature chunks [c0, c1) (8 features each) of row m = the lane's cell:
-// f = (dx + 2) * 25 + (dy + 2) * 5 + (dz + 2) is halo row f % 25, column
-// lane + f / 25; then k / 64 and two zeros.
+// f = (dx + 2) * 25 + (dy + 2) * 5 + (dz + 2) is halo row f % 25 after the
+// lane's y row, column lane % 16 + f / 25; then k / 64 and two zeros. halo
+// points at the lane's y row.
 template <int C0, int C1>
 __device__ __forceinline__ void build_a1(const __half *halo, __half *a, int m, int lane,
                                          unsigned short kfeat) {
-  const unsigned short *hs = reinterpret_cast<const unsigned short *>(halo) + lane;
+  const unsigned short *hs = reinterpret_cast<const unsigned short *>(halo) + (lane & 15);
 #pragma unroll
   for (int c = C0; c < C1; ++c) {
     uint32_t v[8];
@@ -659,8 +663,8 @@ __global__ void k_pack_weights(const float *__restrict__ params, UmmaWeights *__
 }
 
 // kGroups groups of four warps per CTA. Warp q of a group owns lane
-// quarter q of tensor memory (rows 32 q .. 32 q + 31: one 32-cell row
-// segment of the tile): it stages two y rows of the group's halo, builds the
+// quarter q of tensor memory (rows 32 q .. 32 q + 31: the tile's y rows
+// 2 q and 2 q + 1): it stages three y rows of the group's halo, builds the
 // features of its rows, and runs the epilogues of all 64 accumulator
 // columns of its rows. The group's first thread issues its products.
 __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
@@ -696,8 +700,9 @@ __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
   const uint32_t tmem = sh.tmem_base + uint32_t(64 * gi);        // the group's columns
   const uint32_t tlane = tmem + (uint32_t(quarter * 32) << 16);  // this warp's lane quarter
   const int m = quarter * 32 + lane;                              // A row = accumulator lane
-  // this quarter's row y0 + quarter reads halo rows (quarter + dy + 2) 5 + dz + 2
-  const __half *halo = G.halo + quarter * 5 * kHaloW;
+  // the lane's row y0 + yl reads halo rows (yl + dy + 2) 5 + dz + 2
+  const int yl = 2 * quarter + (lane >> 4), xl = lane & 15;
+  const __half *halo = G.halo + yl * 5 * kHaloW;
   const bool issuer = threadIdx.x % kGroupThreads == 0;
   uint32_t phase = 0;
   bool ok = true;
@@ -718,8 +723,7 @@ __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
   };
 
   const FrameDesc &last = frames[nframes - 1];
-  const long long tiles =
-      last.tile_base + (long long)((last.nx + 31) / 32) * ((last.ny + 3) / 4) * last.nz;
+  const long long tiles = last.tile_base + proposal_tiles(last.nx, last.ny, last.nz);
   for (long long ct = (long long)blockIdx.x * kGroups + gi; ct < tiles;
        ct += (long long)gridDim.x * kGroups) {
     const TileInfo g = tile_info(frames, nframes, ct, tiles);
@@ -744,11 +748,11 @@ __global__ void __launch_bounds__(kUmmaThreads, kUmmaCtas) k_cell_proposal_tc(
     sync_issue(2);
     if (!(ok = wait_products())) break;
     {
-      const int y = g.y0 + quarter;
+      const int y = g.y0 + yl;
       const FrameDesc &tf = *g.fr;
-      const bool valid = lane < g.ncl && y < tf.ny;
+      const bool valid = xl < g.ncl && y < tf.ny;
       const long long cell =
-          tf.cell_base + ((long long)g.z0 * tf.ny + (valid ? y : 0)) * tf.nx + g.x0 + lane;
+          tf.cell_base + ((long long)g.z0 * tf.ny + (valid ? y : 0)) * tf.nx + g.x0 + xl;
       write_proposal(tlane, sh.wt.b3, tau, cell_prop, cell, valid);
     }
     // the group's next tile rewrites its halo, A and accumulators

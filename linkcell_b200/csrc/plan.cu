@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(256)
   }
   __syncthreads();
   const long long ncell = (long long)s_fd.nx * s_fd.ny * s_fd.nz;
-  const long long tiles = (long long)((s_fd.nx + 31) / 32) * ((s_fd.ny + 3) / 4) * s_fd.nz;
+  const long long tiles = proposal_tiles(s_fd.nx, s_fd.ny, s_fd.nz);
   for (int f = threadIdx.x; f < nframes; f += blockDim.x) {
     FrameDesc fd = s_fd;
     fd.pt_base = (long long)f * n;

@@ -185,7 +185,7 @@ Code WorkspaceImpl::run(std::vector<FrameDesc> &frames, const double *xyz, const
     fd.pt_base = npts;
     fd.cell_base = ncells;
     fd.tile_base = ptiles;  // shell-proposal tiles
-    ptiles += (long long)((fd.nx + 31) / 32) * ((fd.ny + 3) / 4) * fd.nz;
+    ptiles += proposal_tiles(fd.nx, fd.ny, fd.nz);
     npts += fd.n;
     ncells += (long long)fd.nx * fd.ny * fd.nz;
     kmax = std::max(kmax, fd.k);
