@@ -2212,7 +2212,7 @@ __device__ void warp_replay(const BatchBuffers &b, const FrameDesc &fr, long lon
 
 // ONE: a single frame, passed as fr1 (read from the constant bank).
 template <int KPL, bool ONE>
-__global__ void __launch_bounds__(64, 11)
+__global__ void __launch_bounds__(64, 16)
     k_replay_warp(BatchBuffers b, const __grid_constant__ FrameDesc fr1) {
   long long cnt = *b.replay_count;
   if (cnt > b.replay_cap) cnt = b.replay_cap;
@@ -2532,8 +2532,10 @@ cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s, const FrameDesc
   if (b.replay_threads <= 0) return cudaSuccess;
   if (b.kmax <= 256) {
     // one warp per queued source; NaN frames take one thread of the warp
-    // 2-warp blocks, 11 per SM (the replay is bound by latency: more warps)
-    const int warps = std::max(1, std::min(b.replay_threads, sm_count() * 22));
+    // 2-warp blocks, 16 per SM at 64 registers: the replay is bound by
+    // latency, so more warps (4M: 0.29 -> 0.25 ms at k = 32 against 11 per SM
+    // at 80 registers, 0.69 -> 0.58 ms at k = 64)
+    const int warps = std::max(1, std::min(b.replay_threads, sm_count() * 32));
     const int grid = (warps + 1) / 2;
     if (b.kmax <= 32)
       launch_replay_kpl<1>(b, grid, one, s);
