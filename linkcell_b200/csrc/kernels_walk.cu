@@ -2211,8 +2211,13 @@ __device__ void warp_replay(const BatchBuffers &b, const FrameDesc &fr, long lon
 }
 
 // ONE: a single frame, passed as fr1 (read from the constant bank).
+// Blocks per SM of the literal replay: 16 at 64 registers; 11 at 80 for
+// k-lists past 128 (KPL = 8), which would spill more at 64.
+template <int KPL>
+constexpr int replay_blocks_per_sm() { return KPL >= 8 ? 11 : 16; }
+
 template <int KPL, bool ONE>
-__global__ void __launch_bounds__(64, 16)
+__global__ void __launch_bounds__(64, replay_blocks_per_sm<KPL>())
     k_replay_warp(BatchBuffers b, const __grid_constant__ FrameDesc fr1) {
   long long cnt = *b.replay_count;
   if (cnt > b.replay_cap) cnt = b.replay_cap;
@@ -2535,7 +2540,8 @@ cudaError_t launch_replay(const BatchBuffers &b, cudaStream_t s, const FrameDesc
     // 2-warp blocks, 16 per SM at 64 registers: the replay is bound by
     // latency, so more warps (4M: 0.29 -> 0.25 ms at k = 32 against 11 per SM
     // at 80 registers, 0.69 -> 0.58 ms at k = 64)
-    const int warps = std::max(1, std::min(b.replay_threads, sm_count() * 32));
+    const int per_sm = b.kmax <= 128 ? replay_blocks_per_sm<4>() : replay_blocks_per_sm<8>();
+    const int warps = std::max(1, std::min(b.replay_threads, sm_count() * 2 * per_sm));
     const int grid = (warps + 1) / 2;
     if (b.kmax <= 32)
       launch_replay_kpl<1>(b, grid, one, s);
